@@ -1,0 +1,256 @@
+"""ctypes bindings of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Loaded only by tests/, by ``__graft_entry__.smoke()`` and by the CPU-baseline leg of
+bench.py, as the checker. Two libraries:
+
+* ``liboracle.so``: our plain-C restatement of the reference path (wacomm_oracle.c);
+* ``_ref/libwacomm_ref.so``: the reference's own ``Particle::move`` and helpers compiled from
+  its sources (present only where it was built; ``ref_available()`` tells).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from wacommplusplus_b200.types import PARTICLE_DTYPE, config_data
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libwacomm_ref.so")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libwacomm_ref_cuda.so")
+
+SEMANTICS_HOST = 0
+SEMANTICS_DEVICE = 1
+
+_c_double_p = ctypes.POINTER(ctypes.c_double)
+_c_float_p = ctypes.POINTER(ctypes.c_float)
+
+
+class _Window(ctypes.Structure):
+    _fields_ = [
+        ("T", ctypes.c_int), ("sW", ctypes.c_int), ("sRho", ctypes.c_int),
+        ("eta", ctypes.c_int), ("xi", ctypes.c_int),
+        ("times", _c_double_p), ("mask", _c_double_p), ("lonRad", _c_double_p),
+        ("latRad", _c_double_p), ("depthIntervals", _c_double_p), ("h", _c_double_p),
+        ("zeta", _c_float_p), ("u", _c_float_p), ("v", _c_float_p), ("w", _c_float_p),
+        ("akt", _c_float_p),
+        ("windU10", _c_float_p), ("windV10", _c_float_p),
+        ("stokesU", _c_float_p), ("stokesV", _c_float_p),
+    ]
+
+
+def _dptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_c_double_p)
+
+
+def _fptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_c_float_p)
+
+
+def _window_struct(win):
+    s = _Window()
+    s.T, s.sW, s.sRho, s.eta, s.xi = win.T, win.sW, win.sRho, win.eta, win.xi
+    s.times, s.mask = _dptr(win.times), _dptr(win.mask)
+    s.lonRad, s.latRad = _dptr(win.lonRad), _dptr(win.latRad)
+    s.depthIntervals, s.h = _dptr(win.depthIntervals), _dptr(win.h)
+    s.zeta, s.u, s.v = _fptr(win.zeta), _fptr(win.u), _fptr(win.v)
+    s.w, s.akt = _fptr(win.w), _fptr(win.akt)
+    s.windU10, s.windV10 = _fptr(win.windU10), _fptr(win.windV10)
+    s.stokesU, s.stokesV = _fptr(win.stokesU), _fptr(win.stokesV)
+    return s
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError(f"oracle library missing: {ORACLE_SO} (run make -C oracle)")
+        lib = ctypes.CDLL(ORACLE_SO)
+        u64, i64, d = ctypes.c_uint64, ctypes.c_int64, ctypes.c_double
+        lib.wo_uniform.restype = d
+        lib.wo_uniform.argtypes = [u64, u64, i64, u64, u64]
+        lib.wo_normal.restype = d
+        lib.wo_normal.argtypes = [u64, u64, i64, u64, u64]
+        lib.wo_mix.restype = u64
+        lib.wo_mix.argtypes = [u64]
+        lib.wo_forcing_error_normal.restype = d
+        lib.wo_forcing_error_normal.argtypes = [u64, u64, i64, u64, u64, d, d, d, d, d]
+        lib.wo_jibe_step_probability.restype = d
+        lib.wo_jibe_step_probability.argtypes = [d, d]
+        lib.wo_correlated_normal.restype = d
+        lib.wo_correlated_normal.argtypes = [d, d, d]
+        lib.wo_drift_coefficients.restype = ctypes.c_int
+        lib.wo_drift_coefficients.argtypes = [ctypes.c_int, _c_double_p]
+        lib.wo_compute_leeway.restype = None
+        lib.wo_compute_leeway.argtypes = [_c_double_p, d, d, ctypes.c_int, d, d, _c_double_p]
+        lib.wo_sample_drift_side.restype = ctypes.c_int
+        lib.wo_sample_drift_side.argtypes = [u64, u64, d]
+        lib.wo_restart_elapsed.restype = d
+        lib.wo_restart_elapsed.argtypes = [d, d, d]
+        lib.wo_reflect_cell.restype = d
+        lib.wo_reflect_cell.argtypes = [d, ctypes.c_int, d, ctypes.c_int]
+        lib.wo_reflect_domain.restype = d
+        lib.wo_reflect_domain.argtypes = [d, d]
+        lib.wo_move_batch.restype = ctypes.c_int
+        lib.wo_move_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long,
+                                      ctypes.POINTER(_Window), ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int]
+        lib.wo_concentration.restype = None
+        lib.wo_concentration.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_void_p]
+        lib.wo_source_emission_times.restype = ctypes.c_long
+        lib.wo_source_emission_times.argtypes = [ctypes.c_int, d, d, d, d, d, _c_double_p,
+                                                 ctypes.c_long]
+        lib.wo_source_position_offset.restype = d
+        lib.wo_source_position_offset.argtypes = [u64, u64, u64]
+        geo = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_double_p, _c_double_p, _c_double_p,
+               _c_double_p, d, d, d, _c_double_p, _c_double_p, _c_double_p]
+        lib.wo_kji2deplatlon.restype = ctypes.c_int
+        lib.wo_kji2deplatlon.argtypes = geo
+        lib.wo_deplatlon2kji.restype = ctypes.c_int
+        lib.wo_deplatlon2kji.argtypes = geo
+        _oracle = lib
+    return _oracle
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        if not ref_available():
+            raise RuntimeError(f"reference build missing: {REF_SO}")
+        lib = ctypes.CDLL(REF_SO)
+        u64, i64, d = ctypes.c_uint64, ctypes.c_int64, ctypes.c_double
+        vp, i32, lng = ctypes.c_void_p, ctypes.c_int, ctypes.c_long
+        lib.ref_move_batch.restype = i32
+        lib.ref_move_batch.argtypes = [vp, vp, lng, i32, i32, i32, i32, i32, i32] + [vp] * 16 + [i32]
+        lib.ref_concentration.restype = i32
+        lib.ref_concentration.argtypes = [vp, lng, i32, i32, i32, i32, i32, vp, i32]
+        lib.ref_remove_dead.restype = lng
+        lib.ref_remove_dead.argtypes = [vp, lng]
+        for name in ("ref_uniform", "ref_normal"):
+            getattr(lib, name).restype = d
+            getattr(lib, name).argtypes = [u64, u64, i64, u64, u64]
+        lib.ref_forcing_error_normal.restype = d
+        lib.ref_forcing_error_normal.argtypes = [u64, u64, i64, u64, u64, d, d, d, d, d]
+        lib.ref_drift_coefficients.restype = None
+        lib.ref_drift_coefficients.argtypes = [i32, _c_double_p]
+        lib.ref_compute_leeway.restype = None
+        lib.ref_compute_leeway.argtypes = [_c_double_p, d, d, i32, d, d, _c_double_p]
+        lib.ref_jibe_step_probability.restype = d
+        lib.ref_jibe_step_probability.argtypes = [d, d]
+        lib.ref_sample_drift_side.restype = i32
+        lib.ref_sample_drift_side.argtypes = [u64, u64, d]
+        lib.ref_source_position_offset.restype = d
+        lib.ref_source_position_offset.argtypes = [u64, u64, u64]
+        lib.ref_source_emission_times.restype = lng
+        lib.ref_source_emission_times.argtypes = [i32, d, d, d, d, d, _c_double_p, lng]
+        lib.ref_reflect_domain.restype = d
+        lib.ref_reflect_domain.argtypes = [d, d]
+        lib.ref_reflect_cell.restype = d
+        lib.ref_reflect_cell.argtypes = [d, i32, d, i32]
+        lib.ref_restart_elapsed.restype = d
+        lib.ref_restart_elapsed.argtypes = [d, d, d]
+        lib.ref_max_threads.restype = i32
+        _ref = lib
+    return _ref
+
+
+def _cfg_ptr(cfg):
+    assert isinstance(cfg, config_data)
+    return ctypes.cast(ctypes.pointer(cfg), ctypes.c_void_p)
+
+
+def oracle_move(cfg, particles, win, time_index, semantics=SEMANTICS_HOST, threads=0):
+    """Moves ``particles`` (PARTICLE_DTYPE array, updated in place) over one interval with the
+    C restatement. Raises on a drift object outside the catalogue in host semantics."""
+    assert particles.dtype == PARTICLE_DTYPE and particles.flags.c_contiguous
+    ws = _window_struct(win)
+    status = oracle_lib().wo_move_batch(_cfg_ptr(cfg), particles.ctypes.data, len(particles),
+                                        ctypes.byref(ws), time_index, semantics, threads)
+    if status != 0:
+        raise RuntimeError("oracle: drift object outside the catalogue")
+    return particles
+
+
+def ref_move(cfg, particles, win, time_index, threads=0):
+    """Moves ``particles`` in place with the reference Particle::move (OpenMP dynamic,64)."""
+    assert particles.dtype == PARTICLE_DTYPE and particles.flags.c_contiguous
+    lib = ref_lib()
+    ptr = lambda a: None if a is None else a.ctypes.data
+    lib.ref_move_batch(_cfg_ptr(cfg), particles.ctypes.data, len(particles), time_index,
+                       win.T, win.sW, win.sRho, win.eta, win.xi,
+                       ptr(win.times), ptr(win.mask), ptr(win.lonRad), ptr(win.latRad),
+                       ptr(win.sWValues), ptr(win.depthIntervals), ptr(win.h), ptr(win.zeta),
+                       ptr(win.u), ptr(win.v), ptr(win.w), ptr(win.akt),
+                       ptr(win.windU10), ptr(win.windV10), ptr(win.stokesU), ptr(win.stokesV),
+                       threads)
+    return particles
+
+
+def oracle_concentration(particles, conc_time_index, n_times, win):
+    """uint32 counts [n_times][sRho][eta][xi] of the alive particles at conc_time_index."""
+    conc = np.zeros((n_times, win.sRho, win.eta, win.xi), dtype=np.uint32)
+    oracle_lib().wo_concentration(particles.ctypes.data, len(particles), conc_time_index,
+                                  n_times, win.sRho, win.eta, win.xi, conc.ctypes.data)
+    return conc
+
+
+def ref_concentration(particles, conc_time_index, n_times, win, threads=0):
+    """Float counts from the reference Concentration::evaluate."""
+    conc = np.zeros((n_times, win.sRho, win.eta, win.xi), dtype=np.float32)
+    ref_lib().ref_concentration(particles.ctypes.data, len(particles), conc_time_index, n_times,
+                                win.sRho, win.eta, win.xi, conc.ctypes.data, threads)
+    return conc
+
+
+def emission_times(lib_kind, mode, value, source_start, source_end, interval_start,
+                   interval_end):
+    """sourceEmissionTimes through the oracle ("oracle") or the reference ("ref")."""
+    cap = 1 << 20
+    out = np.zeros(cap, dtype=np.float64)
+    if lib_kind == "oracle":
+        count = oracle_lib().wo_source_emission_times(mode, value, source_start, source_end,
+                                                      interval_start, interval_end,
+                                                      _dptr(out), cap)
+    else:
+        count = ref_lib().ref_source_emission_times(mode, value, source_start, source_end,
+                                                    interval_start, interval_end, _dptr(out), cap)
+    if count < 0:
+        return None
+    return out[:min(count, cap)].copy()
+
+
+def kji2deplatlon(grid, k, j, i):
+    """(dep, lat, lon) of an index position on ``grid`` (lon/lat in degrees)."""
+    dep, lat, lon = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    oracle_lib().wo_kji2deplatlon(grid.eta, grid.xi, grid.sW, _dptr(grid.lon), _dptr(grid.lat),
+                                  _dptr(grid.h), _dptr(grid.sWValues), k, j, i,
+                                  ctypes.byref(dep), ctypes.byref(lat), ctypes.byref(lon))
+    return dep.value, lat.value, lon.value
+
+
+def deplatlon2kji(grid, dep, lat, lon):
+    """(k, j, i) of a geographic position, or None off the grid."""
+    k, j, i = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    status = oracle_lib().wo_deplatlon2kji(grid.eta, grid.xi, grid.sW, _dptr(grid.lon),
+                                           _dptr(grid.lat), _dptr(grid.h), _dptr(grid.sWValues),
+                                           dep, lat, lon, ctypes.byref(k), ctypes.byref(j),
+                                           ctypes.byref(i))
+    if status != 0:
+        return None
+    return k.value, j.value, i.value

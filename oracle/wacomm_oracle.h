@@ -1,0 +1,134 @@
+/*
+ * CPU oracle of the WaComM++ particle-move path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of the reference algorithm, used by tests/, by
+ * __graft_entry__.smoke() and by the cpu_baseline leg of bench.py as the checker. The
+ * product library never links, loads or calls it. Each function cites the reference
+ * file:line it restates. Parity is pinned two ways (tests/test_oracle_*.py): against the
+ * reference's own known-answer tests (pinned RNG values, leeway catalogue, analytic
+ * interval, integrator order ratios, concentration count preservation), and record-for-
+ * record against the reference Particle::move compiled from its own sources
+ * (oracle/_ref, built by oracle/Makefile when the reference tree is present).
+ */
+#ifndef WACOMM_ORACLE_H
+#define WACOMM_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same binary layout as the reference's particle_data (Particle.hpp:31-41), 64 bytes. */
+typedef struct wo_particle {
+    uint64_t id;
+    double k, j, i;
+    double health, age, time;
+    uint16_t driftObjectType;
+    int8_t driftSide;
+} wo_particle;
+
+typedef struct wo_region {
+    double west, south, east, north;
+    double windErrorStdDev, windErrorComponentCorrelation;
+    double windErrorSpatialScale, windErrorTemporalScale;
+} wo_region;
+
+/* Same binary layout as the reference's config_data (Config.hpp:36-72), 1248 bytes. */
+typedef struct wo_config {
+    _Bool random;
+    _Bool randomSources;
+    double deltat, dti, survprob, tau0, sv, crid, sigma, shoreLimit;
+    int upperClosure, lowerClosure, horizontalClosure;
+    uint64_t randomSeed;
+    int trackingDirection, backwardDiffusion, integrator;
+    double restartCheckpoint;
+    int driftModel;
+    _Bool leewayCoefficientEnsemble;
+    double leewayResidualCorrelation;
+    _Bool leewayRandomSide;
+    double leewayRightSideProbability, leewayJibeProbabilityHourly;
+    double windErrorStdDev, windErrorComponentCorrelation;
+    double windErrorSpatialScale, windErrorTemporalScale;
+    uint32_t observationalCalibrationRegionCount;
+    wo_region observationalCalibrationRegions[16];
+    uint16_t driftObjectType;
+    int8_t driftSide;
+    _Bool hasWind;
+    double windU10, windV10;
+} wo_config;
+
+/* A forcing window in the layout of the reference device contract (kernel.cu:63-69):
+ * zeta/wind/stokes [T][eta][xi]; u,v [T][sRho][eta][xi]; w,akt [T][sW][eta][xi] with storage
+ * level = logical k + levels - 1; depthIntervals[sW-1] indexed kI+sW-2; 2-D fields [eta][xi]. */
+typedef struct wo_window {
+    int T, sW, sRho, eta, xi;
+    const double *times, *mask, *lonRad, *latRad, *depthIntervals, *h;
+    const float *zeta, *u, *v, *w, *akt;
+    const float *windU10, *windV10, *stokesU, *stokesV; /* may be NULL */
+} wo_window;
+
+enum { WO_SEMANTICS_HOST = 0, WO_SEMANTICS_DEVICE = 1 };
+enum { WO_CLOSURE_CONSTRAINT = 1, WO_CLOSURE_KILL = 2, WO_CLOSURE_REFLECTION = 3 };
+enum { WO_EULER = 1, WO_MIDPOINT = 2 };
+
+/* NumericalHelpers.hpp:84-120 (scheme ordered-splitmix64-v2). */
+uint64_t wo_mix(uint64_t value);
+uint64_t wo_combine(uint64_t state, uint64_t coordinate);
+double wo_uniform(uint64_t seed, uint64_t particle, int64_t interval, uint64_t substep,
+                  uint64_t component);
+double wo_normal(uint64_t seed, uint64_t particle, int64_t interval, uint64_t substep,
+                 uint64_t component);
+/* DriftModel.hpp:118-160, 176-219. */
+double wo_forcing_error_normal(uint64_t seed, uint64_t particle, int64_t interval,
+                               uint64_t substep, uint64_t component, double longitude,
+                               double latitude, double physicalTime, double spatialScale,
+                               double temporalScale);
+double wo_correlated_normal(double first, double independent, double correlation);
+double wo_jibe_step_probability(double hourly, double seconds);
+int wo_drift_coefficients(int type, double out9[9]); /* returns 0 if type is in the catalogue */
+void wo_compute_leeway(const double c9[9], double windU, double windV, int side,
+                       double downwindNormal, double crosswindNormal, double outUV[2]);
+int wo_calibration_region(const wo_region *regions, uint32_t count, double lonRad,
+                          double latRad);
+int wo_sample_drift_side(uint64_t seed, uint64_t particle, double rightProbability);
+/* NumericalHelpers.hpp:45-74. */
+double wo_restart_elapsed(double intervalStart, double intervalEnd, double checkpoint);
+double wo_reflect_cell(double oldCoordinate, int oldCell, double candidate, int candidateCell);
+double wo_reflect_domain(double coordinate, double maximum);
+
+/* Moves n particles over the forcing interval starting at timeIndex.
+ * semantics = WO_SEMANTICS_HOST restates Particle::move (Particle.cpp:71-824);
+ * semantics = WO_SEMANTICS_DEVICE restates the reference kernel (kernel.cu:153-368).
+ * Returns 0, or -1 when a particle names a drift object outside the catalogue in host
+ * semantics (the reference throws there, DriftModel.cpp:51-54). threads<=0: all cores. */
+int wo_move_batch(const wo_config *config, wo_particle *particles, long n,
+                  const wo_window *window, int timeIndex, int semantics, int threads);
+
+/* Concentration::evaluate (Concentration.hpp:16-44) into uint32 counts
+ * conc[Tc][sRho][eta][xi] (accumulated, not cleared). */
+void wo_concentration(const wo_particle *particles, long n, int concTimeIdx, int Tc, int sRho,
+                      int eta, int xi, uint32_t *conc);
+
+/* sourceEmissionTimes (SourceEmission.hpp:38-79): mode 0 uniform_rate, 1 forcing_interval_batch,
+ * 2 single_pulse. Returns the count (writing at most cap values) or -1 on an invalid schedule. */
+long wo_source_emission_times(int mode, double value, double sourceStart, double sourceEnd,
+                              double intervalStart, double intervalEnd, double *out, long cap);
+double wo_source_position_offset(uint64_t seed, uint64_t particle, uint64_t component);
+
+/* kji2deplatlon / deplatlon2kji (OceanModelAdapter.cpp:271-442) on a grid with lon/lat in
+ * degrees [eta][xi], h [eta][xi] and sW[sW] (indexed k+sW-1). kji2deplatlon returns -1 and
+ * 1e37 outputs off the grid; deplatlon2kji returns -1 when the point is not on the grid. */
+int wo_kji2deplatlon(int eta, int xi, int sW, const double *lon, const double *lat,
+                     const double *h, const double *sWValues, double k, double j, double i,
+                     double *dep, double *latOut, double *lonOut);
+int wo_deplatlon2kji(int eta, int xi, int sW, const double *lon, const double *lat,
+                     const double *h, const double *sWValues, double dep, double latIn,
+                     double lonIn, double *k, double *j, double *i);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
