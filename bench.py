@@ -1,0 +1,335 @@
+"""Throughput of the particle-move hot path on B200 (particle-steps/s).
+
+Workload (the precision-form configuration, plain FP32 forcing): the analytic 128x128 grid with
+10 sigma levels over lon 14.00-14.20 E, lat 40.70-40.90 N, uniform current u=0.2, v=0.1 m/s,
+25 hourly FP32 records; 16,777,216 particles per GPU placed uniformly at 0-5 m depth;
+deterministic, explicit midpoint, dt=30 s (120 substeps per interval). One step = one forcing
+interval of every particle. Synthetic, seeded inputs stand in for the unavailable benchmark data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). `value` is device-timed with the particles resident in HBM;
+`e2e` moves the same particles through the public host-buffer entry point with the copies in the
+timed region; `cpu_baseline` times the reference's own CPU path on a bounded sample.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_ALG = 118.0  # algorithmic bytes per particle-step: one read + one write of the 59-byte state
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            data = json.load(fh)
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per particle-step of the move kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "move_kernel_config3.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_particle_step:"):
+            return float(line.split(":", 1)[1].strip().split()[0])
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def physical_gpu(local_rank):
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if visible:
+        ids = [x for x in visible.split(",") if x.strip()]
+        if local_rank < len(ids) and ids[local_rank].strip().isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+def workload(n_particles, rank, frames=25):
+    from wacommplusplus_b200 import synthetic as syn
+    from wacommplusplus_b200.types import default_config
+    win = syn.config1_window(n_frames=frames)
+    particles = syn.uniform_particles(n_particles, win.eta, win.xi, seed=1 + rank,
+                                      first_id=rank * n_particles)
+    cfg = default_config(random=False)
+    return win, particles, cfg
+
+
+def cpu_reference_rate(win, particles, cfg, threads, repeats=3, sample=262144):
+    """Particle-steps/s of the reference CPU path (Particle::move under OpenMP dynamic,64, or the
+    oracle port where the reference build is absent) on `sample` particles for one interval."""
+    from oracle import bindings as ob
+    kind = "reference" if ob.ref_available() else "port"
+    sample = min(sample, len(particles))
+    rates = []
+    for r in range(repeats + 1):
+        recs = particles[:sample].copy()
+        t0 = time.perf_counter()
+        if kind == "reference":
+            ob.ref_move(cfg, recs, win, r % (win.T - 1), threads=threads)
+        else:
+            ob.oracle_move(cfg, recs, win, r % (win.T - 1), threads=threads)
+        dt = time.perf_counter() - t0
+        steps = sample * int(round(3600.0 / cfg.dti))
+        if r > 0:  # first run warms caches and the thread pool
+            rates.append(steps / dt)
+    return statistics.median(rates), kind, sample
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = len(os.sched_getaffinity(0))
+    win, particles, cfg = workload(1 << 18, 0)
+    from oracle import bindings as ob
+    kind = "reference" if ob.ref_available() else "port"
+    sample = len(particles)
+    steps_per = sample * 120
+    for _ in range(args.warmup):
+        recs = particles.copy()
+        (ob.ref_move if kind == "reference" else ob.oracle_move)(cfg, recs, win, 0, threads=threads)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        recs = particles.copy()
+        (ob.ref_move if kind == "reference" else ob.oracle_move)(cfg, recs, win, s % (win.T - 1),
+                                                                 threads=threads)
+    dt = time.perf_counter() - t0
+    value = steps_per * args.steps / dt
+    line = {
+        "impl": "reference", "metric": "particle-steps/s", "value": value,
+        "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "precision-form analytic grid 128x128x10, plain FP32 forcing, "
+                               f"{sample} particles per step (bounded CPU sample), midpoint, dt=30 s",
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads,
+                         "kind": kind,
+                         "sample": f"{sample} particles x 120 substeps per step, OpenMP dynamic,64"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=10)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    parser.add_argument("--particles", type=int, default=1 << 24)
+    parser.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16"])
+    parser.add_argument("--arithmetic", default="fp32", choices=["fp32", "reference"])
+    parser.add_argument("--no-e2e", action="store_true")
+    parser.add_argument("--no-cpu", action="store_true")
+    args = parser.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+
+    from wacommplusplus_b200.engine import Engine
+
+    win, particles, cfg = workload(args.particles, rank)
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = len(os.sched_getaffinity(0))
+        rate, kind, sample = cpu_reference_rate(win, particles, cfg, threads)
+        rate1, _, sample1 = cpu_reference_rate(win, particles, cfg, 1, repeats=1, sample=16384)
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": kind,
+               "sample": f"{sample} particles x 120 substeps, one interval, OpenMP dynamic,64, "
+                         f"median of 3 after a warm-up",
+               "value_1core": rate1}
+
+    engine = Engine(local_rank, arithmetic=args.arithmetic, storage=args.storage)
+    engine.load_window(win)
+    engine.set_config(cfg)
+    engine.set_particles(particles)
+    n_intervals = win.T - 1
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for s in range(args.warmup):
+        engine.move_interval(s % n_intervals)
+        engine.stats()
+    ext = torch.cuda.ExternalStream(engine.stream)
+    sampler = ClockSampler(physical_gpu(local_rank))
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(ext)
+    steps_total, launches, move_ms, move_steps = 0.0, 0, [], []
+    for s in range(args.steps):
+        engine.move_interval((args.warmup + s) % n_intervals)
+        st = engine.stats()
+        steps_total += st["particle_steps"]
+        launches += st["launches"]
+        move_ms.append(st["move_ms"])
+        move_steps.append(st["particle_steps"])
+    end.record(ext)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    elapsed_ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([elapsed_ms, steps_total], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        elapsed_ms, steps_total = float(mx[0]), float(t[1])
+    value = steps_total / (elapsed_ms / 1000.0)
+
+    kernel_ms = statistics.mean(move_ms)
+    per_launch_steps = statistics.mean(move_steps)
+    achieved = per_launch_steps * B_ALG / (kernel_ms / 1000.0) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic_per_step = profile_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": None if traffic_per_step is None else traffic_per_step * per_launch_steps,
+                "kernel": "move_soa_kernel (fp32 interpolation)", "kernel_ms": kernel_ms,
+                "algorithmic_bytes_per_particle_step": B_ALG}
+
+    e2e = None
+    if not args.no_e2e:
+        n = len(particles)
+        host = torch.empty(n * 64, dtype=torch.uint8, pin_memory=True)
+        host.numpy()[:] = particles.view(np.uint8).reshape(-1)
+        frame_bytes = win.nbytes_frame
+        for s in range(2):
+            engine.move_interval_host_ptr(s % n_intervals, host.data_ptr(), n)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_steps = 0.0
+        for s in range(args.steps):
+            t = (args.warmup + s) % n_intervals
+            f = win.frame(t + 1)
+            engine.upload_frame(t + 1, f["zeta"], f["u"], f["v"], f["w"], f["akt"])
+            engine.move_interval_host_ptr(t, host.data_ptr(), n)
+            e2e_steps += engine.stats()["particle_steps"]
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([dt, e2e_steps], dtype=torch.float64, device="cuda")
+            mx = t.clone()
+            dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+            dt, e2e_steps = float(mx[0]), float(t[1])
+        e2e = {"value": e2e_steps / dt, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": n * 64 + frame_bytes, "d2h_bytes_per_step": n * 64,
+               "timing": "wall clock around K steps of upload_frame + move_interval_host"}
+
+    if rank == 0:
+        line = {
+            "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.arithmetic == "fp32" else "f64",
+            "data": "synthetic",
+            "config": {"workload": "precision-form analytic grid 128x128x10 (lon 14.00-14.20 E, "
+                                   "lat 40.70-40.90 N), 25 hourly records, u=0.2 v=0.1 m/s, "
+                                   f"{args.particles} particles per GPU, deterministic midpoint, "
+                                   f"dt=30 s, forcing storage {args.storage}, arithmetic "
+                                   f"{args.arithmetic}",
+                       "l2": "inputs larger than L2 (particle state 1 GiB per GPU)",
+                       "parallelism": f"particle shards x{world}, no data-path collective"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    engine.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,222 @@
+/*
+ * wacomm_b200 -- B200-native particle-move engine for WaComM++: the C ABI.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an int status
+ * (WACOMM_B200_OK = 0) and never exits the process; wacomm_b200_last_error() returns the
+ * message of the last failure on a context. Host pointers are owned by the caller; device
+ * memory is owned by the context. A context is bound to one CUDA device and is not
+ * re-entrant: calls from several host threads must be serialized by the caller.
+ *
+ * The reference interfaces replaced here:
+ *   - the CPU step Particle::move(config_data*, ...)            Particle.hpp:54-58, Particle.cpp:71-824
+ *   - the GPU launcher cudaMoveParticle(...)                   cuda/kernel.h:7, kernel.cu:370-382
+ *   - the per-interval device staging of Wacomm::run           Wacomm.cpp:386-610
+ *   - dead-particle removal                                     Wacomm.cpp:711-713
+ *   - Concentration::evaluate(...) and the land mask            Concentration.hpp:16-44, Wacomm.cpp:722-739
+ *   - sourceEmissionTimes / Source::emit / Sources::emit        SourceEmission.hpp:38-79, Source.cpp:25-45,
+ *                                                               Sources.cpp:233-249
+ *   - OceanModelAdapter::kji2deplatlon                          OceanModelAdapter.cpp:271-327
+ * The drop-in C++ launcher with the reference's exact signature is declared in
+ * include/wacomm_b200_kernel.h.
+ */
+#ifndef WACOMM_B200_H
+#define WACOMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define WACOMM_B200_BOOL bool
+extern "C" {
+#else
+#define WACOMM_B200_BOOL _Bool
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define WACOMM_B200_OK 0
+#define WACOMM_B200_ERR_ARGUMENT 1     /* a null pointer, a size or an option out of range */
+#define WACOMM_B200_ERR_CUDA 2         /* a CUDA runtime call failed */
+#define WACOMM_B200_ERR_STATE 3        /* a call out of order (no grid, frame missing ...) */
+#define WACOMM_B200_ERR_DRIFT_OBJECT 4 /* a particle names a drift object outside the catalogue */
+#define WACOMM_B200_ERR_CAPACITY 5     /* a size above a documented maximum */
+
+/* ------------------------------------------------------------------ records */
+
+/* Byte-for-byte the reference particle_data (Particle.hpp:31-41), 64 bytes. */
+typedef struct wacomm_b200_particle {
+    uint64_t id;
+    double k, j, i;
+    double health, age, time;
+    uint16_t driftObjectType;
+    int8_t driftSide;
+} wacomm_b200_particle;
+
+typedef struct wacomm_b200_calibration_region {
+    double west, south, east, north;
+    double windErrorStdDev, windErrorComponentCorrelation;
+    double windErrorSpatialScale, windErrorTemporalScale;
+} wacomm_b200_calibration_region;
+
+/* Byte-for-byte the reference config_data (Config.hpp:36-72), 1248 bytes. */
+typedef struct wacomm_b200_config {
+    WACOMM_B200_BOOL random;
+    WACOMM_B200_BOOL randomSources;
+    double deltat, dti, survprob, tau0, sv, crid, sigma, shoreLimit;
+    int upperClosure, lowerClosure, horizontalClosure;
+    uint64_t randomSeed;
+    int trackingDirection, backwardDiffusion, integrator;
+    double restartCheckpoint;
+    int driftModel;
+    WACOMM_B200_BOOL leewayCoefficientEnsemble;
+    double leewayResidualCorrelation;
+    WACOMM_B200_BOOL leewayRandomSide;
+    double leewayRightSideProbability, leewayJibeProbabilityHourly;
+    double windErrorStdDev, windErrorComponentCorrelation;
+    double windErrorSpatialScale, windErrorTemporalScale;
+    uint32_t observationalCalibrationRegionCount;
+    wacomm_b200_calibration_region observationalCalibrationRegions[16];
+    uint16_t driftObjectType;
+    int8_t driftSide;
+    WACOMM_B200_BOOL hasWind;
+    double windU10, windV10;
+} wacomm_b200_config;
+
+/* ------------------------------------------------------------------ engine options */
+
+#define WACOMM_B200_SEMANTICS_HOST 0   /* Particle::move rules (Particle.cpp:71-824), the default */
+#define WACOMM_B200_SEMANTICS_DEVICE 1 /* reference kernel rules (kernel.cu:153-368) */
+
+#define WACOMM_B200_ARITH_REFERENCE 0  /* FP64 with the reference's float roundings (parity mode) */
+#define WACOMM_B200_ARITH_FP32 1       /* FP32 interpolation, FP64 position and time weight */
+
+#define WACOMM_B200_STORAGE_FP32 0     /* forcing pair stored as float */
+#define WACOMM_B200_STORAGE_FP16 1     /* forcing pair stored as half (requires ARITH_FP32) */
+#define WACOMM_B200_STORAGE_BF16 2     /* forcing pair stored as bfloat16 (requires ARITH_FP32) */
+
+#define WACOMM_B200_RNG_REFERENCE 0    /* ordered-splitmix64-v2 draws, draw-for-draw with the reference */
+#define WACOMM_B200_RNG_PHILOX 1       /* Philox4x32-10 keyed on (particle id, interval, substep) */
+
+typedef struct wacomm_b200_options {
+    int semantics;            /* WACOMM_B200_SEMANTICS_* */
+    int arithmetic;           /* WACOMM_B200_ARITH_* */
+    int storage;              /* WACOMM_B200_STORAGE_* */
+    int rng;                  /* WACOMM_B200_RNG_* */
+    int block_size;           /* threads per block of the move kernel: 64..1024, multiple of 32 */
+    int substeps_per_launch;  /* 0: one launch per interval; else launches of this many dti */
+    int sort_by_cell;         /* 1: order the work by forcing cell before each launch */
+    int fuse_concentration;   /* 1: count the concentration in the move kernel's epilogue */
+} wacomm_b200_options;
+
+/* ------------------------------------------------------------------ context */
+
+typedef struct wacomm_b200_context wacomm_b200_context;
+
+/* Library version string; usable without a GPU. */
+const char *wacomm_b200_version(void);
+/* Number of CUDA devices visible (0 when none); never fails. */
+int wacomm_b200_device_count(void);
+
+int wacomm_b200_context_create(int device, wacomm_b200_context **out);
+int wacomm_b200_context_destroy(wacomm_b200_context *ctx);
+const char *wacomm_b200_last_error(const wacomm_b200_context *ctx);
+
+/* Fills *out with the defaults: host semantics, FP32 arithmetic and storage, reference RNG,
+ * 256 threads, one launch per interval, cell sort on, fused concentration on. */
+int wacomm_b200_default_options(wacomm_b200_options *out);
+int wacomm_b200_set_options(wacomm_b200_context *ctx, const wacomm_b200_options *options);
+int wacomm_b200_get_options(const wacomm_b200_context *ctx, wacomm_b200_options *out);
+
+/* Run parameters (the reference's config_data, copied). */
+int wacomm_b200_set_config(wacomm_b200_context *ctx, const wacomm_b200_config *config);
+
+/* Static grid (the oceanmodel_data fields, OceanModelAdapter.hpp:20-34), host arrays [eta][xi];
+ * depth_intervals has s_w-1 entries indexed kI+s_w-2 (WacommAdapter.cpp:101-103); s_w = s_rho+1.
+ * mask may be NULL (used only by the concentration land mask). */
+int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, int s_w,
+                         const double *mask, const double *lon_rad, const double *lat_rad,
+                         const double *h, const double *depth_intervals);
+
+/* Times of the forcing records (seconds; oceanTime). Allocates one device frame slot per time. */
+int wacomm_b200_set_times(wacomm_b200_context *ctx, int n_times, const double *ocean_time);
+
+/* Uploads forcing record t (host arrays in the reference layout: zeta [eta][xi],
+ * u,v [s_rho][eta][xi], w,akt [s_w][eta][xi], level 0 at the bottom). wind/stokes are optional
+ * [eta][xi] fields on the ocean grid and times (Wacomm.cpp:70-84); pass NULL when absent. Frames
+ * persist on the device until overwritten, so each record crosses PCIe once. */
+int wacomm_b200_upload_frame(wacomm_b200_context *ctx, int t, const float *zeta, const float *u,
+                             const float *v, const float *w, const float *akt,
+                             const float *wind_u10, const float *wind_v10, const float *stokes_u,
+                             const float *stokes_v);
+
+/* Particle records in and out (reference particle_data layout, host memory). set replaces the
+ * resident set, append adds after it, get copies the resident records (in their order) into
+ * out (capacity n), and count reports how many are resident. */
+int wacomm_b200_set_particles(wacomm_b200_context *ctx, const wacomm_b200_particle *host,
+                              size_t n);
+int wacomm_b200_append_particles(wacomm_b200_context *ctx, const wacomm_b200_particle *host,
+                                 size_t n);
+int wacomm_b200_get_particles(wacomm_b200_context *ctx, wacomm_b200_particle *out, size_t n);
+int wacomm_b200_particle_count(const wacomm_b200_context *ctx, size_t *out);
+
+/* Moves every resident particle over the forcing interval that starts at record time_index in
+ * the configured tracking direction (Particle.cpp:109-120), asynchronously on the context's
+ * stream. When fuse_concentration is on, alive particles are also counted into the
+ * concentration grid at time index time_index + direction (Wacomm.cpp:713-722). */
+int wacomm_b200_move_interval(wacomm_b200_context *ctx, int time_index);
+
+/* The same interval through host buffers: uploads n records from `particles` (pinned or
+ * pageable host memory), moves them, and writes them back in place. Copies are pipelined
+ * against the kernels in slabs; the resident set is replaced by these records. */
+int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
+                                   wacomm_b200_particle *particles, size_t n);
+
+/* Stable removal of records with health <= 0 (Wacomm.cpp:711-713). */
+int wacomm_b200_remove_dead(wacomm_b200_context *ctx);
+
+/* Concentration grid of n_conc_times records [n_conc_times][s_rho][eta][xi] as uint32 counts.
+ * reset zeroes it; count adds the resident alive particles at conc_time_index
+ * (Concentration.hpp:16-44); get copies it out (uint32) and get_float copies it as the reference
+ * float grid, writing 1e37 into land cells (mask != 1) of every level when mask_land is set
+ * (Wacomm.cpp:188-196,724-739). */
+int wacomm_b200_concentration_reset(wacomm_b200_context *ctx, int n_conc_times);
+int wacomm_b200_concentration_count(wacomm_b200_context *ctx, int conc_time_index);
+int wacomm_b200_concentration_get(wacomm_b200_context *ctx, uint32_t *out, size_t n);
+int wacomm_b200_concentration_get_float(wacomm_b200_context *ctx, float *out, size_t n,
+                                        int mask_land);
+
+int wacomm_b200_synchronize(wacomm_b200_context *ctx);
+
+/* Statistics of the last move_interval: device milliseconds of all its kernels (CUDA events on
+ * the context stream around pack, sort and move), of the move kernel launches alone, how many
+ * kernels it launched and how many particle-steps (substeps of active particles) it took. */
+int wacomm_b200_last_interval_stats(const wacomm_b200_context *ctx, float *device_ms,
+                                    float *move_ms, int *kernel_launches, double *particle_steps);
+
+/* The CUDA stream (cudaStream_t) the context launches on, for callers that order their own work
+ * or events against it. */
+int wacomm_b200_stream(const wacomm_b200_context *ctx, void **out);
+
+/* ------------------------------------------------------------------ device-pointer entry */
+
+/* The reference GPU launcher (kernel.cu:370-382) behind a C name: every pointer is a device
+ * pointer owned by the caller, particles (AoS particle_data) are updated in place,
+ * the call is asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream) and returns
+ * the CUDA error code of the launch (0 = cudaSuccess). mask, num_thread and num_gpu are ignored
+ * like the reference does; wind/stokes may be NULL. Device semantics, reference arithmetic. */
+int wacomm_b200_cuda_move_particle(const wacomm_b200_config *config_device,
+                                   wacomm_b200_particle *particles_device, int time_index,
+                                   int ocean_time, int s_w, int s_rho, int eta, int xi,
+                                   const double *times, const double *mask,
+                                   const double *lon_rad, const double *lat_rad,
+                                   const double *depth_intervals, const double *h,
+                                   const float *zeta, const float *u, const float *v,
+                                   const float *w, const float *akt, const float *wind_u10,
+                                   const float *wind_v10, const float *stokes_u,
+                                   const float *stokes_v, int particle_count, int num_thread,
+                                   int num_gpu, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WACOMM_B200_H */

@@ -345,12 +345,22 @@ static double depth_interval(const interval_state *s, int kI) {
 /* Velocity at a fractional position and forcing weight: ocean current plus leeway and Stokes
  * (Particle.cpp:352-475 host; kernel.cu:206-260 device). The vertical component is a float
  * sum in host semantics and a double blend of two float bilinears in device semantics. */
+/* Level used for memory access: valid levels are unchanged; an out-of-range level (reached only
+ * by a dead particle when survprob <= -1, or by a NaN position, where the reference reads out of
+ * bounds) is clamped into the grid so the oracle and the kernels read the same cells. */
+static int mem_level(int kI, int sW) {
+    if (kI > 0) return 0;
+    if (kI < -sW + 2) return -sW + 2;
+    return kI;
+}
+
 static int advective_velocity(const interval_state *s, int semantics, const wo_particle *p,
                               int kI, double kF, int jI, double jF, int iI, double iF,
                               double stageAlpha, double elapsed, double physicalTime,
                               double stepDt, float *uu, float *vv, double *ww) {
     const wo_config *cfg = s->cfg;
     const wo_window *win = s->win;
+    kI = mem_level(kI, win->sW);
     *uu = bilinear_t4(s, win->u, win->sRho, kI, jI, iI, jF, iF, stageAlpha);
     *vv = bilinear_t4(s, win->v, win->sRho, kI, jI, iI, jF, iF, stageAlpha);
     if (cfg->driftModel == 1 && p->driftObjectType != 0) {
@@ -561,11 +571,12 @@ static int move_one(const interval_state *base, int semantics, wo_particle *part
                                &vv, &ww) != 0)
             return -1;
         double aa;
+        int kA = mem_level(kI, sW);
         if (semantics == WO_SEMANTICS_HOST)
-            aa = trilinear_f(s, win->akt, sW, kI, kF, jI, iI, jF, iF, alpha);
+            aa = trilinear_f(s, win->akt, sW, kA, kF, jI, iI, jF, iF, alpha);
         else
-            aa = (double)bilinear_t4(s, win->akt, sW, kI, jI, iI, jF, iF, alpha) * (1.0 - kF) +
-                 (double)bilinear_t4(s, win->akt, sW, kI - 1, jI, iI, jF, iF, alpha) * kF;
+            aa = (double)bilinear_t4(s, win->akt, sW, kA, jI, iI, jF, iF, alpha) * (1.0 - kF) +
+                 (double)bilinear_t4(s, win->akt, sW, kA - 1, jI, iI, jF, iF, alpha) * kF;
 
         double dxleap = dir * uu * stepDt, dyleap = dir * vv * stepDt;
         double dzleap = dir * (cfg->sv + ww) * stepDt;

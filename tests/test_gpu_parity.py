@@ -1,0 +1,219 @@
+"""Parity of the B200 kernels with the oracle, through the C ABI.
+
+Reference arithmetic (ARITH_REFERENCE) must reproduce the oracle to round-off: positions within
+1e-9 grid-index units (about 0.1 mm here; the reference's own CPU/GPU bound is 1e-12 deterministic
+and 1e-9 stochastic, tests/CudaParticleParityTest.cu:141), health within 1e-15, drift sides and
+alive/dead status exactly, and concentration counts bit-exactly given the positions.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from helpers import load_move_cases, max_abs_diff, records_equal
+from kats import concentration_kat, particle_move_kats
+from oracle import bindings as ob
+from wacommplusplus_b200 import synthetic as syn
+from wacommplusplus_b200.engine import Engine
+from wacommplusplus_b200.types import default_config
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-9
+HEALTH_TOL = 1e-15
+
+
+class EngineMover:
+    """Runs one interval through the engine the way the reference calls Particle::move."""
+
+    def __init__(self, engine):
+        self.engine = engine
+        self.loaded = None
+
+    def __call__(self, cfg, records, window, time_index):
+        e = self.engine
+        if self.loaded is not window:
+            e.load_window(window)
+            self.loaded = window
+        e.set_config(cfg)
+        e.set_particles(records)
+        e.move_interval(time_index)
+        out = e.get_particles()
+        records[:] = out
+        return records
+
+
+@pytest.fixture(scope="module")
+def engine_host(cuda_device):
+    with Engine(cuda_device, semantics="host", arithmetic="reference") as e:
+        yield e
+
+
+@pytest.fixture(scope="module")
+def engine_device(cuda_device):
+    with Engine(cuda_device, semantics="device", arithmetic="reference") as e:
+        yield e
+
+
+def assert_close(got, want, tol=POS_TOL, what=""):
+    assert len(got) == len(want)
+    assert np.array_equal(got["id"], want["id"])
+    assert np.array_equal(got["health"] > 0, want["health"] > 0), what
+    assert np.array_equal(got["driftSide"], want["driftSide"]), what
+    d = max_abs_diff(got, want)
+    assert d["k"] <= tol and d["j"] <= tol and d["i"] <= tol, (what, d)
+    assert d["age"] <= 1e-9, (what, d)
+    rel = np.abs(got["health"] - want["health"]) / np.maximum(1.0, np.abs(want["health"]))
+    assert np.nanmax(rel) <= HEALTH_TOL * 8, (what, d)
+
+
+def test_known_answers_host_rules(engine_host):
+    assert particle_move_kats(EngineMover(engine_host)) > 40
+
+
+def test_known_answers_device_rules(engine_device):
+    assert particle_move_kats(EngineMover(engine_device)) > 40
+
+
+def test_concentration_known_answer(engine_host):
+    def count(records, t, n_times, s_rho, eta, xi):
+        e = engine_host
+        win = syn.config1_window(n_frames=1, eta=eta, xi=xi, s_rho=s_rho)
+        e.load_window(win)
+        e.set_config(default_config())
+        e.set_particles(records)
+        e.concentration_reset(n_times)
+        e.concentration_count(t)
+        return e.concentration()
+    assert concentration_kat(count) == 2
+
+
+@pytest.mark.parametrize("case", load_move_cases(), ids=lambda c: c["name"])
+@pytest.mark.parametrize("rules", ["host", "device"])
+def test_fixture_cases_reference_arithmetic(case, rules, engine_host, engine_device):
+    engine = engine_host if rules == "host" else engine_device
+    sem = ob.SEMANTICS_HOST if rules == "host" else ob.SEMANTICS_DEVICE
+    cfg = default_config(**case["overrides"])
+    win = case["window"]
+    engine.load_window(win)
+    engine.set_config(cfg)
+    engine.set_particles(case["start"])
+    want = case["start"].copy()
+    for t in (0, 1):
+        engine.move_interval(t)
+        ob.oracle_move(cfg, want, win, t, sem, threads=1)
+        assert_close(engine.get_particles(), want, what=f"{case['name']} t={t}")
+    if rules == "host":
+        assert_close(engine.get_particles(), case["after2"], what="vs reference fixture")
+    cfg.trackingDirection = -1
+    engine.set_config(cfg)
+    engine.move_interval(win.T - 1)
+    ob.oracle_move(cfg, want, win, win.T - 1, sem, threads=1)
+    assert_close(engine.get_particles(), want, what=f"{case['name']} backward")
+
+
+def _config1(n_particles=16384, frames=6):
+    win = syn.config1_window(n_frames=frames)
+    return win, syn.uniform_particles(n_particles, win.eta, win.xi, seed=1)
+
+
+@pytest.mark.parametrize("arithmetic", ["reference", "fp32"])
+def test_config1_forward_backward(cuda_device, arithmetic):
+    """Plain analytic case: 16,384 particles, 5 intervals forward then back, midpoint, no
+    diffusion; concentration counted in the move kernel equals the oracle's count of the
+    kernel's own positions."""
+    win, p0 = _config1()
+    cfg = default_config(random=False)
+    with Engine(cuda_device, arithmetic=arithmetic) as e:
+        e.load_window(win)
+        e.set_config(cfg)
+        e.set_particles(p0)
+        e.concentration_reset(win.T)
+        want = p0.copy()
+        for t in range(win.T - 1):
+            e.move_interval(t)
+            ob.oracle_move(cfg, want, win, t, threads=0)
+        got = e.get_particles()
+        tol = POS_TOL if arithmetic == "reference" else 1e-5
+        alive = want["health"] > 0
+        assert np.array_equal(got["health"] > 0, alive)
+        d = max_abs_diff(got, want)
+        assert d["i"] <= tol and d["j"] <= tol and d["k"] <= tol, d
+        conc = e.concentration()
+        assert np.array_equal(conc[win.T - 1], ob.oracle_concentration(got, win.T - 1, win.T, win)[win.T - 1])
+        # backward from the end state returns to the release points of the survivors
+        cfg.trackingDirection = -1
+        e.set_config(cfg)
+        back_want = want.copy()
+        for t in range(win.T - 1, 0, -1):
+            e.move_interval(t)
+            ob.oracle_move(cfg, back_want, win, t, threads=0)
+        back = e.get_particles()
+        d = max_abs_diff(back, back_want)
+        assert d["i"] <= tol and d["j"] <= tol, d
+        # 0.2 m/s east and 0.1 m/s north move a particle ~27 and ~14 cells in 5 h; those released
+        # far enough from the east and north edges never meet a closure
+        inside = (back_want["health"] > 0) & (p0["i"] < win.xi - 36) & (p0["j"] < win.eta - 20)
+        assert inside.sum() > 5000
+        assert np.abs(back["i"][inside] - p0["i"][inside]).max() < 1e-6
+        assert np.abs(back["j"][inside] - p0["j"][inside]).max() < 1e-6
+
+
+def test_chunked_and_unsorted_launches_are_identical(cuda_device):
+    cases = {c["name"]: c for c in load_move_cases()}
+    case = cases["drift_i2"]
+    cfg = default_config(**case["overrides"])
+    outs = []
+    for opts in (dict(), dict(substeps_per_launch=7), dict(sort_by_cell=0),
+                 dict(block_size=64, substeps_per_launch=50)):
+        with Engine(cuda_device, arithmetic="reference", **opts) as e:
+            e.load_window(case["window"])
+            e.set_config(cfg)
+            e.set_particles(case["start"])
+            e.move_interval(0)
+            e.move_interval(1)
+            outs.append(e.get_particles())
+    for o in outs[1:]:
+        assert records_equal(o, outs[0])
+
+
+def test_host_buffer_entry_matches_resident_path(cuda_device):
+    win, p0 = _config1(n_particles=50000, frames=3)
+    cfg = default_config(random=True)
+    with Engine(cuda_device, arithmetic="reference") as e:
+        e.load_window(win)
+        e.set_config(cfg)
+        e.set_particles(p0)
+        e.move_interval(0)
+        resident = e.get_particles()
+        host = p0.copy()
+        e.move_interval_host(0, host)
+        assert records_equal(host, resident)
+
+
+def test_remove_dead_keeps_order(cuda_device):
+    win = syn.config1_window(n_frames=2)
+    p = syn.uniform_particles(1000, win.eta, win.xi, seed=3)
+    p["health"][::3] = -1.0
+    with Engine(cuda_device) as e:
+        e.load_window(win)
+        e.set_config(default_config())
+        e.set_particles(p)
+        e.remove_dead()
+        got = e.get_particles()
+    assert np.array_equal(got, p[p["health"] > 0])
+
+
+def test_unknown_drift_object_is_an_error_under_host_rules(cuda_device):
+    win = syn.config1_window(n_frames=2)
+    p = syn.uniform_particles(64, win.eta, win.xi, seed=3)
+    p["driftObjectType"] = 40
+    p["driftSide"] = 1
+    cfg = default_config(driftModel=1, windU10=5.0)
+    with Engine(cuda_device, arithmetic="reference") as e:
+        e.load_window(win)
+        e.set_config(cfg)
+        e.set_particles(p)
+        e.move_interval(0)
+        with pytest.raises(RuntimeError, match="catalogue"):
+            e.synchronize()

@@ -1,0 +1,105 @@
+"""ctypes binding of libwacomm_b200.so (the C ABI of include/wacomm_b200.h).
+
+The library is built in-tree by ``wacommplusplus_b200/csrc/Makefile`` (``__graft_entry__.build()``).
+There is no fallback: when the library is missing, loading raises, and every engine call needs a
+CUDA device.
+"""
+import ctypes
+import os
+
+from .types import config_data
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwacomm_b200.so")
+
+OK = 0
+ERR_ARGUMENT = 1
+ERR_CUDA = 2
+ERR_STATE = 3
+ERR_DRIFT_OBJECT = 4
+ERR_CAPACITY = 5
+
+SEMANTICS_HOST, SEMANTICS_DEVICE = 0, 1
+ARITH_REFERENCE, ARITH_FP32 = 0, 1
+STORAGE_FP32, STORAGE_FP16, STORAGE_BF16 = 0, 1, 2
+RNG_REFERENCE, RNG_PHILOX = 0, 1
+
+
+class options_t(ctypes.Structure):
+    _fields_ = [
+        ("semantics", ctypes.c_int), ("arithmetic", ctypes.c_int), ("storage", ctypes.c_int),
+        ("rng", ctypes.c_int), ("block_size", ctypes.c_int),
+        ("substeps_per_launch", ctypes.c_int), ("sort_by_cell", ctypes.c_int),
+        ("fuse_concentration", ctypes.c_int),
+    ]
+
+
+# Every symbol include/wacomm_b200.h declares, with (restype, argtypes).
+_vp, _i, _sz, _d = ctypes.c_void_p, ctypes.c_int, ctypes.c_size_t, ctypes.c_double
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+SIGNATURES = {
+    "wacomm_b200_version": (ctypes.c_char_p, []),
+    "wacomm_b200_device_count": (_i, []),
+    "wacomm_b200_context_create": (_i, [_i, ctypes.POINTER(_vp)]),
+    "wacomm_b200_context_destroy": (_i, [_vp]),
+    "wacomm_b200_last_error": (ctypes.c_char_p, [_vp]),
+    "wacomm_b200_default_options": (_i, [ctypes.POINTER(options_t)]),
+    "wacomm_b200_set_options": (_i, [_vp, ctypes.POINTER(options_t)]),
+    "wacomm_b200_get_options": (_i, [_vp, ctypes.POINTER(options_t)]),
+    "wacomm_b200_set_config": (_i, [_vp, ctypes.POINTER(config_data)]),
+    "wacomm_b200_set_grid": (_i, [_vp, _i, _i, _i, _i, _dp, _dp, _dp, _dp, _dp]),
+    "wacomm_b200_set_times": (_i, [_vp, _i, _dp]),
+    "wacomm_b200_upload_frame": (_i, [_vp, _i] + [_fp] * 9),
+    "wacomm_b200_set_particles": (_i, [_vp, _vp, _sz]),
+    "wacomm_b200_append_particles": (_i, [_vp, _vp, _sz]),
+    "wacomm_b200_get_particles": (_i, [_vp, _vp, _sz]),
+    "wacomm_b200_particle_count": (_i, [_vp, ctypes.POINTER(_sz)]),
+    "wacomm_b200_move_interval": (_i, [_vp, _i]),
+    "wacomm_b200_move_interval_host": (_i, [_vp, _i, _vp, _sz]),
+    "wacomm_b200_remove_dead": (_i, [_vp]),
+    "wacomm_b200_concentration_reset": (_i, [_vp, _i]),
+    "wacomm_b200_concentration_count": (_i, [_vp, _i]),
+    "wacomm_b200_concentration_get": (_i, [_vp, _vp, _sz]),
+    "wacomm_b200_concentration_get_float": (_i, [_vp, _vp, _sz, _i]),
+    "wacomm_b200_synchronize": (_i, [_vp]),
+    "wacomm_b200_last_interval_stats": (_i, [_vp, _fp, _fp, ctypes.POINTER(_i), _dp]),
+    "wacomm_b200_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "wacomm_b200_cuda_move_particle": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i] + [_vp] * 15 +
+                                       [_i, _i, _i, _vp]),
+}
+
+_lib = None
+
+
+class WacommError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"wacomm_b200 error {code}: {message}")
+        self.code = code
+
+
+def lib():
+    """The loaded library; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `make -C wacommplusplus_b200/csrc` "
+                "(or __graft_entry__.build()); there is no CPU fallback")
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (restype, argtypes) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = restype
+            fn.argtypes = argtypes
+        _lib = handle
+    return _lib
+
+
+def device_count():
+    return lib().wacomm_b200_device_count()
+
+
+def default_options():
+    o = options_t()
+    lib().wacomm_b200_default_options(ctypes.byref(o))
+    return o

@@ -1,0 +1,879 @@
+// The engine context behind the C ABI (include/wacomm_b200.h).
+//
+// It replaces the per-interval staging of Wacomm::run (Wacomm.cpp:386-610): instead of
+// allocating, uploading the whole forcing window and the particles, launching and freeing on
+// every interval, the context keeps the grid, every forcing record and the particle set
+// resident in device memory, packs the bracketing pair once per interval, orders the work by
+// forcing cell and moves all particles in one launch (or a few chunk launches), counting the
+// concentration in the same kernel.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "move_kernels.cuh"
+
+using namespace wb;
+
+namespace {
+
+struct FrameSlot {
+    float *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *akt = nullptr;
+    float *windU = nullptr, *windV = nullptr, *stokesU = nullptr, *stokesV = nullptr;
+    bool loaded = false;
+};
+
+struct SoABuffers {
+    ParticleSoA s{};
+    size_t cap = 0;
+};
+
+constexpr size_t MAX_PARTICLES = (size_t)1 << 31;  // uint32 work indices
+
+}  // namespace
+
+struct wacomm_b200_context {
+    int device = 0;
+    cudaStream_t stream = nullptr, h2d = nullptr, d2h = nullptr;
+    std::string error;
+    wacomm_b200_options opt{};
+    wacomm_b200_config cfg{};
+    bool hasConfig = false;
+
+    int eta = 0, xi = 0, sRho = 0, sW = 0;
+    bool hasGrid = false;
+    double *dMask = nullptr, *dLon = nullptr, *dLat = nullptr, *dH = nullptr, *dDepth = nullptr;
+    bool hasMask = false;
+    double2 *dMetric = nullptr;
+    int metricSemantics = -1;
+
+    std::vector<double> times;
+    std::vector<FrameSlot> slots;
+
+    void *dNodes = nullptr;
+    size_t nodesBytes = 0;
+    SurfPair *dSurf = nullptr;
+    EnvPair *dEnv = nullptr;
+    int pairT0 = -1, pairT1 = -1, pairStorage = -1;
+    bool pairEnv = false;
+
+    size_t n = 0;
+    SoABuffers S, T;
+    uint32_t *dKeys = nullptr, *dOrder = nullptr, *dFlags = nullptr, *dPositions = nullptr;
+    size_t workCap = 0;
+    uint32_t *dHist = nullptr, *dOffsets = nullptr;
+    size_t binsCap = 0;
+    uint32_t *dScanTemp = nullptr;
+    size_t scanTempCap = 0;
+    uint32_t *dCount = nullptr;  // scratch word (compaction result)
+
+    wacomm_b200_particle *dAos = nullptr;
+    size_t aosCap = 0;
+
+    uint32_t *dConc = nullptr;
+    int concTimes = 0;
+
+    unsigned long long *dSteps = nullptr;
+    int *dErr = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evMove0 = nullptr, evMove1 = nullptr;
+    bool moveTimed = false;
+    float lastMs = 0;
+    int lastLaunches = 0;
+    double lastSteps = 0;
+};
+
+namespace {
+
+int fail(wacomm_b200_context *ctx, int code, const char *fmt, ...) {
+    char buffer[512];
+    va_list args;
+    va_start(args, fmt);
+    vsnprintf(buffer, sizeof(buffer), fmt, args);
+    va_end(args);
+    if (ctx) ctx->error = buffer;
+    return code;
+}
+
+#define CUDA_TRY(ctx, expr)                                                                  \
+    do {                                                                                     \
+        cudaError_t _e = (expr);                                                             \
+        if (_e != cudaSuccess)                                                               \
+            return fail(ctx, WACOMM_B200_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(_e)); \
+    } while (0)
+
+template <class T>
+int grow(wacomm_b200_context *ctx, T *&ptr, size_t &cap, size_t need) {
+    if (need <= cap && ptr) return WACOMM_B200_OK;
+    size_t bytes = std::max<size_t>(need, 1) * sizeof(T);
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    CUDA_TRY(ctx, cudaMalloc((void **)&ptr, bytes));
+    cap = std::max<size_t>(need, 1);
+    return WACOMM_B200_OK;
+}
+
+void free_soa(SoABuffers &b) {
+    cudaFree(b.s.id);
+    cudaFree(b.s.k);
+    cudaFree(b.s.j);
+    cudaFree(b.s.i);
+    cudaFree(b.s.health);
+    cudaFree(b.s.age);
+    cudaFree(b.s.time);
+    cudaFree(b.s.type);
+    cudaFree(b.s.side);
+    cudaFree(b.s.elapsed);
+    b = SoABuffers{};
+}
+
+int alloc_soa(wacomm_b200_context *ctx, SoABuffers &b, size_t cap) {
+    free_soa(b);
+    size_t c = std::max<size_t>(cap, 1);
+    CUDA_TRY(ctx, cudaMalloc(&b.s.id, c * sizeof(uint64_t)));
+    CUDA_TRY(ctx, cudaMalloc(&b.s.k, c * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&b.s.j, c * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&b.s.i, c * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&b.s.health, c * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&b.s.age, c * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&b.s.time, c * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&b.s.type, c * sizeof(uint16_t)));
+    CUDA_TRY(ctx, cudaMalloc(&b.s.side, c * sizeof(int8_t)));
+    CUDA_TRY(ctx, cudaMalloc(&b.s.elapsed, c * sizeof(double)));
+    b.cap = c;
+    return WACOMM_B200_OK;
+}
+
+ParticleSoA offset_soa(const ParticleSoA &s, size_t off) {
+    ParticleSoA r = s;
+    r.id += off;
+    r.k += off;
+    r.j += off;
+    r.i += off;
+    r.health += off;
+    r.age += off;
+    r.time += off;
+    r.type += off;
+    r.side += off;
+    r.elapsed += off;
+    return r;
+}
+
+// Grows the resident particle arrays to hold `need` records, keeping the first `keep`.
+int reserve_particles(wacomm_b200_context *ctx, size_t need, size_t keep) {
+    if (need <= ctx->S.cap && ctx->S.s.id) return WACOMM_B200_OK;
+    size_t cap = std::max(need, ctx->S.cap + ctx->S.cap / 2);
+    SoABuffers fresh;
+    int rc = alloc_soa(ctx, fresh, cap);
+    if (rc) return rc;
+    if (keep) {
+        const ParticleSoA &a = ctx->S.s, &b = fresh.s;
+        CUDA_TRY(ctx, cudaMemcpyAsync(b.id, a.id, keep * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(b.k, a.k, keep * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(b.j, a.j, keep * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(b.i, a.i, keep * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(b.health, a.health, keep * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(b.age, a.age, keep * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(b.time, a.time, keep * 8, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(b.type, a.type, keep * 2, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(b.side, a.side, keep * 1, cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    free_soa(ctx->S);
+    ctx->S = fresh;
+    return WACOMM_B200_OK;
+}
+
+int reserve_work(wacomm_b200_context *ctx, size_t n) {
+    if (n <= ctx->workCap && ctx->dKeys) return WACOMM_B200_OK;
+    size_t cap = std::max(n, ctx->workCap + ctx->workCap / 2);
+    size_t c1 = 0, c2 = 0, c3 = 0, c4 = 0;
+    int rc;
+    if ((rc = grow(ctx, ctx->dKeys, c1, cap))) return rc;
+    if ((rc = grow(ctx, ctx->dOrder, c2, cap))) return rc;
+    if ((rc = grow(ctx, ctx->dFlags, c3, cap))) return rc;
+    if ((rc = grow(ctx, ctx->dPositions, c4, cap))) return rc;
+    ctx->workCap = cap;
+    return WACOMM_B200_OK;
+}
+
+int reserve_scan(wacomm_b200_context *ctx, size_t n) {
+    size_t words = scan_temp_words(n);
+    return grow(ctx, ctx->dScanTemp, ctx->scanTempCap, words);
+}
+
+int check_ready(wacomm_b200_context *ctx) {
+    if (!ctx->hasConfig) return fail(ctx, WACOMM_B200_ERR_STATE, "set_config has not been called");
+    if (!ctx->hasGrid) return fail(ctx, WACOMM_B200_ERR_STATE, "set_grid has not been called");
+    if (ctx->times.empty()) return fail(ctx, WACOMM_B200_ERR_STATE, "set_times has not been called");
+    return WACOMM_B200_OK;
+}
+
+int validate_options(wacomm_b200_context *ctx, const wacomm_b200_options &o) {
+    if (o.semantics != WACOMM_B200_SEMANTICS_HOST && o.semantics != WACOMM_B200_SEMANTICS_DEVICE)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "semantics %d out of range", o.semantics);
+    if (o.arithmetic != WACOMM_B200_ARITH_REFERENCE && o.arithmetic != WACOMM_B200_ARITH_FP32)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "arithmetic %d out of range", o.arithmetic);
+    if (o.storage < WACOMM_B200_STORAGE_FP32 || o.storage > WACOMM_B200_STORAGE_BF16)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "storage %d out of range", o.storage);
+    if (o.arithmetic == WACOMM_B200_ARITH_REFERENCE && o.storage != WACOMM_B200_STORAGE_FP32)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT,
+                    "reference arithmetic reads the forcing exactly and needs FP32 storage");
+    if (o.rng != WACOMM_B200_RNG_REFERENCE && o.rng != WACOMM_B200_RNG_PHILOX)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "rng %d out of range", o.rng);
+    if (o.block_size < 32 || o.block_size > 256 || o.block_size % 32)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "block_size %d: need a multiple of 32 in [32, 256]",
+                    o.block_size);
+    if (o.substeps_per_launch < 0)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "substeps_per_launch must be >= 0");
+    return WACOMM_B200_OK;
+}
+
+int ensure_metric(wacomm_b200_context *ctx) {
+    if (ctx->metricSemantics == ctx->opt.semantics) return WACOMM_B200_OK;
+    CUDA_TRY(ctx, build_metric(ctx->opt.semantics, ctx->eta, ctx->xi, ctx->dLon, ctx->dLat,
+                               ctx->dMetric, ctx->stream));
+    ctx->metricSemantics = ctx->opt.semantics;
+    return WACOMM_B200_OK;
+}
+
+FrameDevice frame_of(const FrameSlot &s) {
+    return FrameDevice{s.zeta, s.u, s.v, s.w, s.akt, s.windU, s.windV, s.stokesU, s.stokesV};
+}
+
+int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
+    const FrameSlot &a = ctx->slots[t0], &b = ctx->slots[t1];
+    bool env = a.windU || a.windV || a.stokesU || b.windU || b.windV || b.stokesU;
+    if (ctx->pairT0 == t0 && ctx->pairT1 == t1 && ctx->pairStorage == ctx->opt.storage &&
+        ctx->pairEnv == env)
+        return WACOMM_B200_OK;
+    size_t plane = (size_t)ctx->eta * ctx->xi;
+    size_t need = plane * ctx->sW * node_record_bytes(ctx->opt.storage);
+    if (need > ctx->nodesBytes) {
+        cudaFree(ctx->dNodes);
+        ctx->dNodes = nullptr;
+        ctx->nodesBytes = 0;
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dNodes, need));
+        ctx->nodesBytes = need;
+    }
+    if (env && !ctx->dEnv) CUDA_TRY(ctx, cudaMalloc(&ctx->dEnv, plane * sizeof(EnvPair)));
+    CUDA_TRY(ctx, pack_pair(ctx->opt.storage, ctx->eta, ctx->xi, ctx->sW, frame_of(a), frame_of(b),
+                            ctx->dH, ctx->dNodes, ctx->dSurf, env ? ctx->dEnv : nullptr,
+                            ctx->stream));
+    launches += 2;
+    ctx->pairT0 = t0;
+    ctx->pairT1 = t1;
+    ctx->pairStorage = ctx->opt.storage;
+    ctx->pairEnv = env;
+    return WACOMM_B200_OK;
+}
+
+PackedArgs packed_args(wacomm_b200_context *ctx) {
+    PackedArgs A;
+    A.eta = ctx->eta;
+    A.xi = ctx->xi;
+    A.sW = ctx->sW;
+    A.sRho = ctx->sRho;
+    A.nodes = ctx->dNodes;
+    A.surf = ctx->dSurf;
+    A.env = ctx->pairEnv ? ctx->dEnv : nullptr;
+    const FrameSlot &a = ctx->slots[ctx->pairT0];
+    A.hasWindU = ctx->pairEnv && a.windU;
+    A.hasWindV = ctx->pairEnv && a.windV;
+    A.hasStokes = ctx->pairEnv && a.stokesU && a.stokesV;
+    A.lonRad = ctx->dLon;
+    A.latRad = ctx->dLat;
+    A.depthIntervals = ctx->dDepth;
+    A.metric = ctx->dMetric;
+    return A;
+}
+
+int sort_work(wacomm_b200_context *ctx, const ParticleSoA &S, size_t count, uint32_t *keys,
+              uint32_t *order, int &launches) {
+    size_t bins = (size_t)ctx->eta * ctx->xi + 1;
+    if (ctx->binsCap < bins + 2 || !ctx->dHist || !ctx->dOffsets) {
+        cudaFree(ctx->dHist);
+        cudaFree(ctx->dOffsets);
+        ctx->dHist = ctx->dOffsets = nullptr;
+        ctx->binsCap = 0;
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dHist, (bins + 2) * sizeof(uint32_t)));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dOffsets, (bins + 2) * sizeof(uint32_t)));
+        ctx->binsCap = bins + 2;
+    }
+    int rc;
+    if ((rc = reserve_scan(ctx, std::max(bins, count)))) return rc;
+    CUDA_TRY(ctx, sort_by_cell(S.j, S.i, (int)count, ctx->eta, ctx->xi, keys, ctx->dHist,
+                               ctx->dOffsets, ctx->dScanTemp, order, ctx->stream));
+    size_t blocks = (bins + 8191) / 8192;
+    launches += 3 + (blocks > 1 ? 2 : 0);
+    return WACOMM_B200_OK;
+}
+
+// Moves `count` resident records starting at `offset` over the interval (sort, chunks, count).
+int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t offset, size_t count,
+                 uint32_t *keys, uint32_t *order, int &launches) {
+    if (count == 0) return WACOMM_B200_OK;
+    ParticleSoA S = offset_soa(ctx->S.s, offset);
+    PackedArgs A = packed_args(ctx);
+    IntervalParams P = base;
+    P.rng = ctx->opt.rng;
+    MoveLaunch L;
+    L.count = (int)count;
+    L.order = nullptr;
+    int concTime = base.t0 + base.direction;
+    bool count_here = ctx->opt.fuse_concentration && ctx->dConc && concTime >= 0 &&
+                      concTime < ctx->concTimes;
+    L.conc = count_here ? ctx->dConc : nullptr;
+    L.concTimeIndex = concTime;
+    L.concTimes = ctx->concTimes;
+    L.steps = ctx->dSteps;
+    L.err = ctx->dErr;
+    double chunk = ctx->opt.substeps_per_launch > 0 ? ctx->opt.substeps_per_launch * ctx->cfg.dti : 0;
+    int nChunks = 1;
+    if (chunk > 0 && base.length > 0) nChunks = (int)std::ceil(base.length / chunk);
+    if (nChunks < 1) nChunks = 1;
+    for (int c = 0; c < nChunks; c++) {
+        if (ctx->opt.sort_by_cell) {
+            int rc = sort_work(ctx, S, count, keys, order, launches);
+            if (rc) return rc;
+            L.order = order;
+        }
+        if (!ctx->moveTimed) {
+            CUDA_TRY(ctx, cudaEventRecord(ctx->evMove0, ctx->stream));
+            ctx->moveTimed = true;
+        }
+        P.firstChunk = c == 0;
+        P.lastChunk = c == nChunks - 1;
+        P.chunkEnd = P.lastChunk ? INFINITY : (c + 1) * chunk;
+        cudaError_t e;
+        if (ctx->opt.arithmetic == WACOMM_B200_ARITH_REFERENCE)
+            e = move_ref_dispatch(ctx->opt.semantics, ctx->cfg, P, A, S, L, ctx->opt.block_size,
+                                  ctx->stream);
+        else
+            e = move_f32_dispatch(ctx->opt.semantics, ctx->opt.storage, ctx->cfg, P, A, S, L,
+                                  ctx->opt.block_size, ctx->stream);
+        if (e != cudaSuccess)
+            return fail(ctx, WACOMM_B200_ERR_CUDA, "move launch: %s", cudaGetErrorString(e));
+        launches++;
+        CUDA_TRY(ctx, cudaEventRecord(ctx->evMove1, ctx->stream));
+    }
+    return WACOMM_B200_OK;
+}
+
+int prepare_interval(wacomm_b200_context *ctx, int time_index, IntervalParams &P, int &launches) {
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    if (time_index < 0 || time_index >= (int)ctx->times.size())
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "time_index %d out of [0, %zu)", time_index,
+                    ctx->times.size());
+    make_interval(ctx->cfg, ctx->times.data(), (int)ctx->times.size(), time_index, ctx->sW,
+                  ctx->opt.semantics, P);
+    if (P.skip) return WACOMM_B200_OK;
+    if (!ctx->slots[P.t0].loaded || !ctx->slots[P.t1].loaded)
+        return fail(ctx, WACOMM_B200_ERR_STATE, "forcing records %d and %d must be uploaded", P.t0,
+                    P.t1);
+    if ((rc = ensure_metric(ctx))) return rc;
+    if ((rc = ensure_pair(ctx, P.t0, P.t1, launches))) return rc;
+    return WACOMM_B200_OK;
+}
+
+int check_errors(wacomm_b200_context *ctx) {
+    int flags = 0;
+    CUDA_TRY(ctx, cudaMemcpy(&flags, ctx->dErr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flags & ERR_DRIFT_OBJECT) {
+        CUDA_TRY(ctx, cudaMemset(ctx->dErr, 0, sizeof(int)));
+        return fail(ctx, WACOMM_B200_ERR_DRIFT_OBJECT,
+                    "a particle names a drift object outside the catalogue (ids 0-22)");
+    }
+    return WACOMM_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *wacomm_b200_version(void) { return "wacomm_b200 1.0 (sm_100a)"; }
+
+int wacomm_b200_device_count(void) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return count;
+}
+
+int wacomm_b200_default_options(wacomm_b200_options *out) {
+    if (!out) return WACOMM_B200_ERR_ARGUMENT;
+    out->semantics = WACOMM_B200_SEMANTICS_HOST;
+    out->arithmetic = WACOMM_B200_ARITH_FP32;
+    out->storage = WACOMM_B200_STORAGE_FP32;
+    out->rng = WACOMM_B200_RNG_REFERENCE;
+    out->block_size = 256;
+    out->substeps_per_launch = 0;
+    out->sort_by_cell = 1;
+    out->fuse_concentration = 1;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_context_create(int device, wacomm_b200_context **out) {
+    if (!out) return WACOMM_B200_ERR_ARGUMENT;
+    *out = nullptr;
+    int count = wacomm_b200_device_count();
+    if (device < 0 || device >= count) return WACOMM_B200_ERR_ARGUMENT;
+    wacomm_b200_context *ctx = new wacomm_b200_context();
+    ctx->device = device;
+    wacomm_b200_default_options(&ctx->opt);
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->evMove0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->evMove1);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->dSteps, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->dErr, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->dCount, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(ctx->dErr, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        wacomm_b200_context_destroy(ctx);
+        return WACOMM_B200_ERR_CUDA;
+    }
+    *out = ctx;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
+    if (!ctx) return WACOMM_B200_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (FrameSlot &s : ctx->slots) {
+        cudaFree(s.zeta);
+        cudaFree(s.u);
+        cudaFree(s.v);
+        cudaFree(s.w);
+        cudaFree(s.akt);
+        cudaFree(s.windU);
+        cudaFree(s.windV);
+        cudaFree(s.stokesU);
+        cudaFree(s.stokesV);
+    }
+    cudaFree(ctx->dMask);
+    cudaFree(ctx->dLon);
+    cudaFree(ctx->dLat);
+    cudaFree(ctx->dH);
+    cudaFree(ctx->dDepth);
+    cudaFree(ctx->dMetric);
+    cudaFree(ctx->dNodes);
+    cudaFree(ctx->dSurf);
+    cudaFree(ctx->dEnv);
+    free_soa(ctx->S);
+    free_soa(ctx->T);
+    cudaFree(ctx->dKeys);
+    cudaFree(ctx->dOrder);
+    cudaFree(ctx->dFlags);
+    cudaFree(ctx->dPositions);
+    cudaFree(ctx->dHist);
+    cudaFree(ctx->dOffsets);
+    cudaFree(ctx->dScanTemp);
+    cudaFree(ctx->dCount);
+    cudaFree(ctx->dAos);
+    cudaFree(ctx->dConc);
+    cudaFree(ctx->dSteps);
+    cudaFree(ctx->dErr);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->evMove0) cudaEventDestroy(ctx->evMove0);
+    if (ctx->evMove1) cudaEventDestroy(ctx->evMove1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
+    if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
+    delete ctx;
+    return WACOMM_B200_OK;
+}
+
+const char *wacomm_b200_last_error(const wacomm_b200_context *ctx) {
+    return ctx ? ctx->error.c_str() : "null context";
+}
+
+int wacomm_b200_set_options(wacomm_b200_context *ctx, const wacomm_b200_options *options) {
+    if (!ctx || !options) return WACOMM_B200_ERR_ARGUMENT;
+    int rc = validate_options(ctx, *options);
+    if (rc) return rc;
+    ctx->opt = *options;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_get_options(const wacomm_b200_context *ctx, wacomm_b200_options *out) {
+    if (!ctx || !out) return WACOMM_B200_ERR_ARGUMENT;
+    *out = ctx->opt;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_set_config(wacomm_b200_context *ctx, const wacomm_b200_config *config) {
+    if (!ctx || !config) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null config");
+    if (config->trackingDirection != 1 && config->trackingDirection != -1)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "trackingDirection must be 1 or -1");
+    if (!(config->dti > 0)) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "dti must be > 0");
+    if (config->observationalCalibrationRegionCount > 16)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "more than 16 calibration regions");
+    ctx->cfg = *config;
+    ctx->hasConfig = true;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, int s_w,
+                         const double *mask, const double *lon_rad, const double *lat_rad,
+                         const double *h, const double *depth_intervals) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (eta < 2 || xi < 2 || s_rho < 1 || s_w != s_rho + 1)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "grid %dx%d with s_rho=%d s_w=%d: need eta,xi>=2, "
+                    "s_rho>=1, s_w=s_rho+1", eta, xi, s_rho, s_w);
+    if ((size_t)eta * xi >= ((size_t)1 << 31) - 2)
+        return fail(ctx, WACOMM_B200_ERR_CAPACITY, "grid of %zu cells exceeds 2^31-2",
+                    (size_t)eta * xi);
+    if (!lon_rad || !lat_rad || !h || !depth_intervals)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null grid array");
+    cudaSetDevice(ctx->device);
+    size_t plane = (size_t)eta * xi;
+    cudaFree(ctx->dMask);
+    cudaFree(ctx->dLon);
+    cudaFree(ctx->dLat);
+    cudaFree(ctx->dH);
+    cudaFree(ctx->dDepth);
+    cudaFree(ctx->dMetric);
+    cudaFree(ctx->dSurf);
+    ctx->dMask = ctx->dLon = ctx->dLat = ctx->dH = ctx->dDepth = nullptr;
+    ctx->dMetric = nullptr;
+    ctx->dSurf = nullptr;
+    cudaFree(ctx->dEnv);
+    ctx->dEnv = nullptr;
+    ctx->hasGrid = false;
+    CUDA_TRY(ctx, cudaMalloc(&ctx->dLon, plane * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&ctx->dLat, plane * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&ctx->dH, plane * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&ctx->dDepth, (size_t)(s_w - 1) * sizeof(double)));
+    CUDA_TRY(ctx, cudaMalloc(&ctx->dMetric, plane * sizeof(double2)));
+    CUDA_TRY(ctx, cudaMalloc(&ctx->dSurf, plane * sizeof(SurfPair)));
+    CUDA_TRY(ctx, cudaMemcpy(ctx->dLon, lon_rad, plane * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_TRY(ctx, cudaMemcpy(ctx->dLat, lat_rad, plane * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_TRY(ctx, cudaMemcpy(ctx->dH, h, plane * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_TRY(ctx, cudaMemcpy(ctx->dDepth, depth_intervals, (size_t)(s_w - 1) * sizeof(double),
+                             cudaMemcpyHostToDevice));
+    ctx->hasMask = mask != nullptr;
+    if (mask) {
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dMask, plane * sizeof(double)));
+        CUDA_TRY(ctx, cudaMemcpy(ctx->dMask, mask, plane * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    ctx->eta = eta;
+    ctx->xi = xi;
+    ctx->sRho = s_rho;
+    ctx->sW = s_w;
+    ctx->metricSemantics = -1;
+    ctx->pairT0 = ctx->pairT1 = -1;
+    ctx->hasGrid = true;
+    // Forcing records of another grid no longer fit.
+    for (FrameSlot &s : ctx->slots) s.loaded = false;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_set_times(wacomm_b200_context *ctx, int n_times, const double *ocean_time) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (n_times < 1 || !ocean_time) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "need >= 1 time");
+    cudaSetDevice(ctx->device);
+    ctx->times.assign(ocean_time, ocean_time + n_times);
+    if ((int)ctx->slots.size() < n_times) ctx->slots.resize(n_times);
+    ctx->pairT0 = ctx->pairT1 = -1;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_upload_frame(wacomm_b200_context *ctx, int t, const float *zeta, const float *u,
+                             const float *v, const float *w, const float *akt,
+                             const float *wind_u10, const float *wind_v10, const float *stokes_u,
+                             const float *stokes_v) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!ctx->hasGrid) return fail(ctx, WACOMM_B200_ERR_STATE, "set_grid has not been called");
+    if (t < 0 || t >= (int)ctx->times.size())
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "frame %d out of [0, %zu)", t, ctx->times.size());
+    if (!zeta || !u || !v || !w || !akt) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null field");
+    if ((stokes_u == nullptr) != (stokes_v == nullptr))
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "stokes_u and stokes_v come together");
+    cudaSetDevice(ctx->device);
+    size_t plane = (size_t)ctx->eta * ctx->xi;
+    FrameSlot &s = ctx->slots[t];
+    auto put = [&](float *&dst, const float *src, size_t count) -> int {
+        if (!src) {
+            cudaFree(dst);
+            dst = nullptr;
+            return WACOMM_B200_OK;
+        }
+        if (!dst) CUDA_TRY(ctx, cudaMalloc(&dst, count * sizeof(float)));
+        CUDA_TRY(ctx, cudaMemcpyAsync(dst, src, count * sizeof(float), cudaMemcpyHostToDevice,
+                                      ctx->h2d));
+        return WACOMM_B200_OK;
+    };
+    // The pair cache may reference this slot: finish kernels that read it first.
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    int rc;
+    if ((rc = put(s.zeta, zeta, plane))) return rc;
+    if ((rc = put(s.u, u, plane * ctx->sRho))) return rc;
+    if ((rc = put(s.v, v, plane * ctx->sRho))) return rc;
+    if ((rc = put(s.w, w, plane * ctx->sW))) return rc;
+    if ((rc = put(s.akt, akt, plane * ctx->sW))) return rc;
+    if ((rc = put(s.windU, wind_u10, plane))) return rc;
+    if ((rc = put(s.windV, wind_v10, plane))) return rc;
+    if ((rc = put(s.stokesU, stokes_u, plane))) return rc;
+    if ((rc = put(s.stokesV, stokes_v, plane))) return rc;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
+    s.loaded = true;
+    if (ctx->pairT0 == t || ctx->pairT1 == t) ctx->pairT0 = ctx->pairT1 = -1;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_set_particles(wacomm_b200_context *ctx, const wacomm_b200_particle *host,
+                              size_t n) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    ctx->n = 0;
+    return wacomm_b200_append_particles(ctx, host, n);
+}
+
+int wacomm_b200_append_particles(wacomm_b200_context *ctx, const wacomm_b200_particle *host,
+                                 size_t n) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (n == 0) return WACOMM_B200_OK;
+    if (!host) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null particles");
+    if (ctx->n + n >= MAX_PARTICLES)
+        return fail(ctx, WACOMM_B200_ERR_CAPACITY, "more than 2^31 particles");
+    cudaSetDevice(ctx->device);
+    int rc;
+    if ((rc = reserve_particles(ctx, ctx->n + n, ctx->n))) return rc;
+    if ((rc = grow(ctx, ctx->dAos, ctx->aosCap, n))) return rc;
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dAos, host, n * sizeof(wacomm_b200_particle),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, aos_to_soa(ctx->dAos, (int)n, offset_soa(ctx->S.s, ctx->n), ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->n += n;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_get_particles(wacomm_b200_context *ctx, wacomm_b200_particle *out, size_t n) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (n < ctx->n) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "buffer of %zu for %zu records", n, ctx->n);
+    if (ctx->n == 0) return WACOMM_B200_OK;
+    if (!out) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null output");
+    cudaSetDevice(ctx->device);
+    int rc;
+    if ((rc = grow(ctx, ctx->dAos, ctx->aosCap, ctx->n))) return rc;
+    CUDA_TRY(ctx, soa_to_aos(ctx->S.s, (int)ctx->n, ctx->dAos, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(out, ctx->dAos, ctx->n * sizeof(wacomm_b200_particle),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return check_errors(ctx);
+}
+
+int wacomm_b200_particle_count(const wacomm_b200_context *ctx, size_t *out) {
+    if (!ctx || !out) return WACOMM_B200_ERR_ARGUMENT;
+    *out = ctx->n;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_move_interval(wacomm_b200_context *ctx, int time_index) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    IntervalParams P;
+    int launches = 0;
+    ctx->moveTimed = false;
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->dSteps, 0, sizeof(unsigned long long), ctx->stream));
+    CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    int rc = prepare_interval(ctx, time_index, P, launches);
+    if (rc) return rc;
+    if (!P.skip && ctx->n) {
+        if ((rc = reserve_work(ctx, ctx->n))) return rc;
+        if ((rc = run_interval(ctx, P, 0, ctx->n, ctx->dKeys, ctx->dOrder, launches))) return rc;
+    }
+    CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->lastLaunches = launches;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
+                                   wacomm_b200_particle *particles, size_t n) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (n && !particles) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null particles");
+    if (n >= MAX_PARTICLES) return fail(ctx, WACOMM_B200_ERR_CAPACITY, "more than 2^31 particles");
+    cudaSetDevice(ctx->device);
+    IntervalParams P;
+    int launches = 0;
+    ctx->moveTimed = false;
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->dSteps, 0, sizeof(unsigned long long), ctx->stream));
+    int rc = prepare_interval(ctx, time_index, P, launches);
+    if (rc) return rc;
+    if ((rc = reserve_particles(ctx, n, 0))) return rc;
+    if ((rc = reserve_work(ctx, n))) return rc;
+    if ((rc = grow(ctx, ctx->dAos, ctx->aosCap, n))) return rc;
+    ctx->n = n;
+    // Slabs: the upload of slab s+1 and the download of slab s-1 overlap the move of slab s.
+    const size_t minSlab = (size_t)1 << 20;
+    int slabs = n >= 4 * minSlab ? 4 : (n >= 2 * minSlab ? 2 : 1);
+    size_t per = (n + slabs - 1) / slabs;
+    std::vector<cudaEvent_t> up(slabs), done(slabs);
+    for (int s = 0; s < slabs; s++) {
+        cudaEventCreateWithFlags(&up[s], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming);
+    }
+    CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int s = 0; s < slabs; s++) {
+        size_t off = s * per, cnt = std::min(per, n - std::min(n, off));
+        if (cnt == 0) continue;
+        CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dAos + off, particles + off,
+                                      cnt * sizeof(wacomm_b200_particle), cudaMemcpyHostToDevice,
+                                      ctx->h2d));
+        CUDA_TRY(ctx, cudaEventRecord(up[s], ctx->h2d));
+    }
+    for (int s = 0; s < slabs; s++) {
+        size_t off = s * per, cnt = std::min(per, n - std::min(n, off));
+        if (cnt == 0) continue;
+        CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, up[s], 0));
+        ParticleSoA S = offset_soa(ctx->S.s, off);
+        CUDA_TRY(ctx, aos_to_soa(ctx->dAos + off, (int)cnt, S, ctx->stream));
+        launches++;
+        if (!P.skip) {
+            if ((rc = run_interval(ctx, P, off, cnt, ctx->dKeys + off, ctx->dOrder + off, launches)))
+                return rc;
+        }
+        CUDA_TRY(ctx, soa_to_aos(S, (int)cnt, ctx->dAos + off, ctx->stream));
+        launches++;
+        CUDA_TRY(ctx, cudaEventRecord(done[s], ctx->stream));
+        CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->d2h, done[s], 0));
+        CUDA_TRY(ctx, cudaMemcpyAsync(particles + off, ctx->dAos + off,
+                                      cnt * sizeof(wacomm_b200_particle), cudaMemcpyDeviceToHost,
+                                      ctx->d2h));
+    }
+    CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->d2h));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int s = 0; s < slabs; s++) {
+        cudaEventDestroy(up[s]);
+        cudaEventDestroy(done[s]);
+    }
+    ctx->lastLaunches = launches;
+    return check_errors(ctx);
+}
+
+int wacomm_b200_remove_dead(wacomm_b200_context *ctx) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (ctx->n == 0) return WACOMM_B200_OK;
+    cudaSetDevice(ctx->device);
+    int rc;
+    if ((rc = reserve_work(ctx, ctx->n))) return rc;
+    if ((rc = reserve_scan(ctx, ctx->n))) return rc;
+    if (ctx->T.cap < ctx->n && (rc = alloc_soa(ctx, ctx->T, ctx->S.cap))) return rc;
+    CUDA_TRY(ctx, compact_alive(ctx->S.s, (int)ctx->n, ctx->T.s, ctx->dFlags, ctx->dPositions,
+                                ctx->dScanTemp, ctx->dCount, ctx->stream));
+    uint32_t kept = 0;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&kept, ctx->dCount, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    std::swap(ctx->S, ctx->T);
+    ctx->n = kept;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_concentration_reset(wacomm_b200_context *ctx, int n_conc_times) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!ctx->hasGrid) return fail(ctx, WACOMM_B200_ERR_STATE, "set_grid has not been called");
+    if (n_conc_times < 1) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "need >= 1 concentration time");
+    cudaSetDevice(ctx->device);
+    size_t cells = (size_t)n_conc_times * ctx->sRho * ctx->eta * ctx->xi;
+    if (ctx->concTimes != n_conc_times) {
+        cudaFree(ctx->dConc);
+        ctx->dConc = nullptr;
+        ctx->concTimes = 0;
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dConc, cells * sizeof(uint32_t)));
+        ctx->concTimes = n_conc_times;
+    }
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->dConc, 0, cells * sizeof(uint32_t), ctx->stream));
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_concentration_count(wacomm_b200_context *ctx, int conc_time_index) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!ctx->dConc) return fail(ctx, WACOMM_B200_ERR_STATE, "concentration_reset has not been called");
+    if (conc_time_index < 0 || conc_time_index >= ctx->concTimes)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "concentration time %d out of range", conc_time_index);
+    cudaSetDevice(ctx->device);
+    CUDA_TRY(ctx, count_concentration(ctx->S.s, (int)ctx->n, conc_time_index, ctx->sRho, ctx->eta,
+                                      ctx->xi, ctx->dConc, ctx->stream));
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_concentration_get(wacomm_b200_context *ctx, uint32_t *out, size_t n) {
+    if (!ctx || !out) return WACOMM_B200_ERR_ARGUMENT;
+    size_t cells = (size_t)ctx->concTimes * ctx->sRho * ctx->eta * ctx->xi;
+    if (!ctx->dConc) return fail(ctx, WACOMM_B200_ERR_STATE, "concentration_reset has not been called");
+    if (n < cells) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "buffer of %zu for %zu cells", n, cells);
+    cudaSetDevice(ctx->device);
+    CUDA_TRY(ctx, cudaMemcpyAsync(out, ctx->dConc, cells * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_concentration_get_float(wacomm_b200_context *ctx, float *out, size_t n,
+                                        int mask_land) {
+    if (!ctx || !out) return WACOMM_B200_ERR_ARGUMENT;
+    size_t cells = (size_t)ctx->concTimes * ctx->sRho * ctx->eta * ctx->xi;
+    if (!ctx->dConc) return fail(ctx, WACOMM_B200_ERR_STATE, "concentration_reset has not been called");
+    if (n < cells) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "buffer of %zu for %zu cells", n, cells);
+    if (mask_land && !ctx->hasMask) return fail(ctx, WACOMM_B200_ERR_STATE, "no mask was given");
+    cudaSetDevice(ctx->device);
+    float *dOut = nullptr;
+    CUDA_TRY(ctx, cudaMallocAsync((void **)&dOut, cells * sizeof(float), ctx->stream));
+    cudaError_t e = concentration_to_float(ctx->dConc, cells, ctx->concTimes, ctx->sRho, ctx->eta,
+                                           ctx->xi, mask_land ? ctx->dMask : nullptr, dOut,
+                                           ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dOut, cells * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaFreeAsync(dOut, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e));
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_synchronize(wacomm_b200_context *ctx) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return check_errors(ctx);
+}
+
+int wacomm_b200_last_interval_stats(const wacomm_b200_context *ctx, float *device_ms,
+                                    float *move_ms, int *kernel_launches, double *particle_steps) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    wacomm_b200_context *c = const_cast<wacomm_b200_context *>(ctx);
+    cudaSetDevice(c->device);
+    CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+    float ms = 0, mm = 0;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    if (c->moveTimed) CUDA_TRY(c, cudaEventElapsedTime(&mm, c->evMove0, c->evMove1));
+    unsigned long long steps = 0;
+    CUDA_TRY(c, cudaMemcpy(&steps, c->dSteps, sizeof(steps), cudaMemcpyDeviceToHost));
+    if (device_ms) *device_ms = ms;
+    if (move_ms) *move_ms = mm;
+    if (kernel_launches) *kernel_launches = c->lastLaunches;
+    if (particle_steps) *particle_steps = (double)steps;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_stream(const wacomm_b200_context *ctx, void **out) {
+    if (!ctx || !out) return WACOMM_B200_ERR_ARGUMENT;
+    *out = (void *)ctx->stream;
+    return WACOMM_B200_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// Host-side declarations of the engine's kernel launchers (defined in the .cu units).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "wacomm_b200.h"
+
+namespace wb {
+
+struct IntervalParams;
+struct ParticleSoA;
+struct MoveLaunch;
+struct SurfPair;
+struct EnvPair;
+
+struct PackedArgs {
+    int eta, xi, sW, sRho;
+    const void *nodes;  // NodeRecord<storage>[sW][eta][xi]
+    const SurfPair *surf;
+    const EnvPair *env;
+    bool hasWindU, hasWindV, hasStokes;
+    const double *lonRad, *latRad, *depthIntervals;
+    const double2 *metric;
+};
+
+// move_ref.cu (reference arithmetic, FP32 storage)
+cudaError_t move_ref_dispatch(int semantics, const wacomm_b200_config &cfg,
+                              const IntervalParams &P, const PackedArgs &A, const ParticleSoA &S,
+                              const MoveLaunch &L, int blockSize, cudaStream_t stream);
+// move_f32.cu (FP32 arithmetic, any storage)
+cudaError_t move_f32_dispatch(int semantics, int storage, const wacomm_b200_config &cfg,
+                              const IntervalParams &P, const PackedArgs &A, const ParticleSoA &S,
+                              const MoveLaunch &L, int blockSize, cudaStream_t stream);
+
+// support.cu ----------------------------------------------------------------------------
+
+// Size in bytes of one node record of the packed pair.
+size_t node_record_bytes(int storage);
+
+struct FrameDevice {  // one forcing record in the reference layout (device)
+    const float *zeta, *u, *v, *w, *akt;
+    const float *windU, *windV, *stokesU, *stokesV;
+};
+
+cudaError_t pack_pair(int storage, int eta, int xi, int sW, const FrameDevice &f0,
+                      const FrameDevice &f1, const double *h, void *nodes, SurfPair *surf,
+                      EnvPair *env, cudaStream_t stream);
+
+cudaError_t build_metric(int semantics, int eta, int xi, const double *lonRad,
+                         const double *latRad, double2 *metric, cudaStream_t stream);
+
+// Exclusive scan of n uint32 values; `temp` must hold scan_temp_words(n) words. The total is
+// written to *total (device).
+size_t scan_temp_words(size_t n);
+cudaError_t exclusive_scan(const uint32_t *in, uint32_t *out, size_t n, uint32_t *total,
+                           uint32_t *temp, cudaStream_t stream);
+
+// Counting sort of particles by forcing cell: order[] receives particle slots grouped by cell.
+// keys/hist/offsets/temp are scratch: keys[n], hist[eta*xi+1], offsets[eta*xi+2].
+cudaError_t sort_by_cell(const double *j, const double *i, int n, int eta, int xi, uint32_t *keys,
+                         uint32_t *hist, uint32_t *offsets, uint32_t *temp, uint32_t *order,
+                         cudaStream_t stream);
+
+cudaError_t aos_to_soa(const wacomm_b200_particle *aos, int n, const ParticleSoA &S,
+                       cudaStream_t stream);
+cudaError_t soa_to_aos(const ParticleSoA &S, int n, wacomm_b200_particle *aos,
+                       cudaStream_t stream);
+
+// Stable removal of records with health <= 0: compacts S in place through `tmp` (a second SoA)
+// and the scan scratch; writes the kept count to *kept (device).
+cudaError_t compact_alive(const ParticleSoA &S, int n, const ParticleSoA &tmp, uint32_t *flags,
+                          uint32_t *positions, uint32_t *temp, uint32_t *kept,
+                          cudaStream_t stream);
+
+cudaError_t count_concentration(const ParticleSoA &S, int n, int concTime, int sRho, int eta,
+                                int xi, uint32_t *conc, cudaStream_t stream);
+
+cudaError_t concentration_to_float(const uint32_t *conc, size_t n, int nTimes, int sRho, int eta,
+                                   int xi, const double *mask, float *out, cudaStream_t stream);
+
+// dropin.cu -------------------------------------------------------------------------------
+int dropin_move(const wacomm_b200_config *config, wacomm_b200_particle *particles, int timeIndex,
+                int oceanTime, int sW, int sRho, int eta, int xi, const double *times,
+                const double *lonRad, const double *latRad, const double *depthIntervals,
+                const double *h, const float *zeta, const float *u, const float *v,
+                const float *w, const float *akt, const float *windU, const float *windV,
+                const float *stokesU, const float *stokesV, int count, cudaStream_t stream);
+
+}  // namespace wb

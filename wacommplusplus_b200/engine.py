@@ -1,0 +1,209 @@
+"""Python face of the engine context (include/wacomm_b200.h).
+
+``Engine`` owns one device context: grid, forcing records and particles stay resident on the
+GPU; every method maps to one C entry point and raises ``WacommError`` with the context's message
+on a non-zero status.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import WacommError, options_t
+from .types import PARTICLE_DTYPE, config_data
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def _d(a):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(_dp)
+
+
+def _f(a):
+    if a is None:
+        return None, None
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(_fp)
+
+
+class Engine:
+    """One B200 context: ``Engine(device=0, **options)``.
+
+    Options (defaults in brackets): semantics ["host"|"device"], arithmetic ["fp32"|"reference"],
+    storage ["fp32"|"fp16"|"bf16"], rng ["reference"|"philox"], block_size [256],
+    substeps_per_launch [0 = whole interval], sort_by_cell [True], fuse_concentration [True].
+    """
+
+    _SEM = {"host": 0, "device": 1}
+    _ARITH = {"reference": 0, "fp32": 1}
+    _STORE = {"fp32": 0, "fp16": 1, "bf16": 2}
+    _RNG = {"reference": 0, "philox": 1}
+
+    def __init__(self, device=0, **options):
+        self._lib = _native.lib()
+        handle = ctypes.c_void_p()
+        status = self._lib.wacomm_b200_context_create(device, ctypes.byref(handle))
+        if status != 0:
+            raise WacommError(status, f"cannot create a context on CUDA device {device} "
+                                      f"({self._lib.wacomm_b200_device_count()} visible)")
+        self._ctx = handle
+        self.window = None
+        if options:
+            self.set_options(**options)
+
+    # -------------------------------------------------------------- plumbing
+    def _check(self, status):
+        if status != 0:
+            raise WacommError(status, self._lib.wacomm_b200_last_error(self._ctx).decode())
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._lib.wacomm_b200_context_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -------------------------------------------------------------- setup
+    def options(self):
+        o = options_t()
+        self._check(self._lib.wacomm_b200_get_options(self._ctx, ctypes.byref(o)))
+        return o
+
+    def set_options(self, **kw):
+        o = self.options()
+        table = {"semantics": self._SEM, "arithmetic": self._ARITH, "storage": self._STORE,
+                 "rng": self._RNG}
+        for key, value in kw.items():
+            if key in table and isinstance(value, str):
+                value = table[key][value]
+            setattr(o, key, int(value))
+        self._check(self._lib.wacomm_b200_set_options(self._ctx, ctypes.byref(o)))
+
+    def set_config(self, cfg):
+        assert isinstance(cfg, config_data)
+        self._check(self._lib.wacomm_b200_set_config(self._ctx, ctypes.byref(cfg)))
+
+    def set_grid(self, eta, xi, s_rho, s_w, lon_rad, lat_rad, h, depth_intervals, mask=None):
+        keep = [_d(lon_rad), _d(lat_rad), _d(h), _d(depth_intervals), _d(mask)]
+        ptrs = [None if k is None else k[1] for k in keep]
+        self._check(self._lib.wacomm_b200_set_grid(self._ctx, eta, xi, s_rho, s_w, ptrs[4], ptrs[0],
+                                                   ptrs[1], ptrs[2], ptrs[3]))
+
+    def set_times(self, times):
+        arr, ptr = _d(times)
+        self._check(self._lib.wacomm_b200_set_times(self._ctx, len(arr), ptr))
+
+    def upload_frame(self, t, zeta, u, v, w, akt, wind_u10=None, wind_v10=None, stokes_u=None,
+                     stokes_v=None):
+        fields = [_f(zeta), _f(u), _f(v), _f(w), _f(akt), _f(wind_u10), _f(wind_v10),
+                  _f(stokes_u), _f(stokes_v)]
+        self._check(self._lib.wacomm_b200_upload_frame(self._ctx, t, *[p for _, p in fields]))
+
+    def load_window(self, win, frames=None):
+        """Grid, times and forcing records of a ``synthetic.Window``-like object."""
+        self.window = win
+        self.set_grid(win.eta, win.xi, win.sRho, win.sW, win.lonRad, win.latRad, win.h,
+                      win.depthIntervals, win.mask)
+        self.set_times(win.times)
+        for t in (range(win.T) if frames is None else frames):
+            f = win.frame(t)
+            self.upload_frame(t, f["zeta"], f["u"], f["v"], f["w"], f["akt"], f["windU10"],
+                              f["windV10"], f["stokesU"], f["stokesV"])
+
+    # -------------------------------------------------------------- particles
+    def set_particles(self, particles):
+        p = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        self._check(self._lib.wacomm_b200_set_particles(self._ctx, p.ctypes.data, len(p)))
+
+    def append_particles(self, particles):
+        p = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        self._check(self._lib.wacomm_b200_append_particles(self._ctx, p.ctypes.data, len(p)))
+
+    def count(self):
+        n = ctypes.c_size_t()
+        self._check(self._lib.wacomm_b200_particle_count(self._ctx, ctypes.byref(n)))
+        return n.value
+
+    def get_particles(self):
+        n = self.count()
+        out = np.zeros(n, dtype=PARTICLE_DTYPE)
+        self._check(self._lib.wacomm_b200_get_particles(self._ctx, out.ctypes.data, n))
+        return out
+
+    # -------------------------------------------------------------- stepping
+    def move_interval(self, time_index):
+        self._check(self._lib.wacomm_b200_move_interval(self._ctx, time_index))
+
+    def move_interval_host(self, time_index, particles):
+        """Moves a host record array in place through the pipelined host-buffer entry."""
+        assert particles.dtype == PARTICLE_DTYPE and particles.flags.c_contiguous
+        self._check(self._lib.wacomm_b200_move_interval_host(self._ctx, time_index,
+                                                             particles.ctypes.data,
+                                                             len(particles)))
+        return particles
+
+    def move_interval_host_ptr(self, time_index, address, n):
+        """Same as move_interval_host on a raw host address (e.g. a pinned torch tensor)."""
+        self._check(self._lib.wacomm_b200_move_interval_host(self._ctx, time_index, address, n))
+
+    def remove_dead(self):
+        self._check(self._lib.wacomm_b200_remove_dead(self._ctx))
+
+    def synchronize(self):
+        self._check(self._lib.wacomm_b200_synchronize(self._ctx))
+
+    def stats(self):
+        """dict of the last interval: device ms of all kernels, ms of the move launches, kernel
+        launches and particle-steps."""
+        ms, move_ms = ctypes.c_float(), ctypes.c_float()
+        launches = ctypes.c_int()
+        steps = ctypes.c_double()
+        self._check(self._lib.wacomm_b200_last_interval_stats(
+            self._ctx, ctypes.byref(ms), ctypes.byref(move_ms), ctypes.byref(launches),
+            ctypes.byref(steps)))
+        return {"device_ms": ms.value, "move_ms": move_ms.value, "launches": launches.value,
+                "particle_steps": steps.value}
+
+    @property
+    def stream(self):
+        """Address of the context's cudaStream_t (for torch.cuda.ExternalStream)."""
+        out = ctypes.c_void_p()
+        self._check(self._lib.wacomm_b200_stream(self._ctx, ctypes.byref(out)))
+        return out.value
+
+    # -------------------------------------------------------------- concentration
+    def concentration_reset(self, n_times):
+        self._check(self._lib.wacomm_b200_concentration_reset(self._ctx, n_times))
+        self._conc_times = n_times
+
+    def concentration_count(self, conc_time_index):
+        self._check(self._lib.wacomm_b200_concentration_count(self._ctx, conc_time_index))
+
+    def _conc_shape(self):
+        w = self.window
+        return (self._conc_times, w.sRho, w.eta, w.xi)
+
+    def concentration(self):
+        out = np.zeros(self._conc_shape(), dtype=np.uint32)
+        self._check(self._lib.wacomm_b200_concentration_get(self._ctx, out.ctypes.data, out.size))
+        return out
+
+    def concentration_float(self, mask_land=False):
+        out = np.zeros(self._conc_shape(), dtype=np.float32)
+        self._check(self._lib.wacomm_b200_concentration_get_float(self._ctx, out.ctypes.data,
+                                                                  out.size, int(mask_land)))
+        return out
