@@ -134,6 +134,11 @@ def _reference_kernel():
 
 @pytest.mark.parametrize("case", load_move_cases(), ids=lambda c: c["name"])
 def test_against_the_reference_kernel(cuda_device, case):
+    """The reference kernel is compiled with multiply-add contraction, so it drifts from its own
+    CPU path by a few 1e-9 index units over hundreds of substeps (its snapshot tolerance is 1e-8,
+    tools/performance_evidence.py:10-11). The drop-in must stay at least as close to the CPU
+    rules (the oracle's device rules) as the reference kernel does, and agree with it on
+    alive/dead status and drift sides."""
     fn = _reference_kernel()
     if fn is None:
         pytest.skip("reference kernel build absent")
@@ -142,10 +147,14 @@ def test_against_the_reference_kernel(cuda_device, case):
     win = case["window"]
     ours = case["start"].copy()
     theirs = case["start"].copy()
+    cpu = case["start"].copy()
     for t in (0, 1):
         ours = call_dropin(cfg, ours, win, t)
         theirs = call_dropin(cfg, theirs, win, t, launcher=launcher)
+        ob.oracle_move(cfg, cpu, win, t, ob.SEMANTICS_DEVICE, threads=1)
     assert np.array_equal(ours["health"] > 0, theirs["health"] > 0)
     assert np.array_equal(ours["driftSide"], theirs["driftSide"])
-    d = max_abs_diff(ours, theirs)
-    assert max(d["i"], d["j"], d["k"]) <= 1e-9, d
+    d_ours = max(max_abs_diff(ours, cpu)[f] for f in ("i", "j", "k"))
+    d_theirs = max(max_abs_diff(theirs, cpu)[f] for f in ("i", "j", "k"))
+    assert d_ours <= max(1e-9, d_theirs), (d_ours, d_theirs)
+    assert max(max_abs_diff(ours, theirs)[f] for f in ("i", "j", "k")) <= 1e-7

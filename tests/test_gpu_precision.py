@@ -1,0 +1,110 @@
+"""FP32 interpolation and FP16/BF16 forcing storage against the FP64 oracle, and the Philox
+diffusion streams by ensemble moments.
+
+Bounds (positions as great-circle metres after the stated simulated time):
+  * FP32 forcing, FP32 interpolation: mean < 0.05 m, max < 1 m;
+  * FP16 / BF16 forcing:              mean <= 50 m, p99 <= 200 m (the precision targets).
+"""
+import numpy as np
+import pytest
+
+from helpers import great_circle_m, max_abs_diff
+from oracle import bindings as ob
+from wacommplusplus_b200 import synthetic as syn
+from wacommplusplus_b200.engine import Engine
+from wacommplusplus_b200.types import default_config
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(engine, win, cfg, particles, intervals):
+    engine.load_window(win)
+    engine.set_config(cfg)
+    engine.set_particles(particles)
+    for t in intervals:
+        engine.move_interval(t)
+    return engine.get_particles()
+
+
+def _oracle(win, cfg, particles, intervals):
+    out = particles.copy()
+    for t in intervals:
+        ob.oracle_move(cfg, out, win, t, threads=0)
+    return out
+
+
+@pytest.fixture(scope="module")
+def analytic_day():
+    win = syn.config1_window(n_frames=25)
+    p = syn.uniform_particles(8192, win.eta, win.xi, seed=7)
+    cfg = default_config(random=False, horizontalClosure=1)
+    return win, cfg, p, _oracle(win, cfg, p, range(24))
+
+
+@pytest.fixture(scope="module")
+def realistic_six_hours():
+    rf = syn.RealisticForcing(eta=160, xi=144, s_rho=12, n_frames=7, seed=31)
+    win = rf.window()
+    p = rf.release(8192, n_sources=32, seed=32)
+    p["time"] = win.times[0]
+    cfg = default_config(random=False, dti=15.0)
+    return win, cfg, p, _oracle(win, cfg, p, range(6))
+
+
+@pytest.mark.parametrize("storage,mean_max,p99_max,max_max", [
+    ("fp32", 0.05, 0.5, 1.0), ("fp16", 50.0, 200.0, None), ("bf16", 50.0, 200.0, None)])
+@pytest.mark.parametrize("scene", ["analytic_day", "realistic_six_hours"])
+def test_position_error_against_fp64_oracle(cuda_device, request, scene, storage, mean_max,
+                                            p99_max, max_max):
+    win, cfg, p, want = request.getfixturevalue(scene)
+    intervals = range(win.T - 1)
+    with Engine(cuda_device, arithmetic="fp32", storage=storage) as e:
+        got = _run(e, win, cfg, p, intervals)
+    both = (got["health"] > 0) & (want["health"] > 0)
+    flips = int(np.sum((got["health"] > 0) != (want["health"] > 0)))
+    assert flips <= max(1, len(p) // 200), f"{flips} alive/dead decisions differ"
+    err = great_circle_m(win.lon, win.lat, got[both], want[both])
+    mean, p99, mx = float(err.mean()), float(np.percentile(err, 99)), float(err.max())
+    print(f"{scene} {storage}: mean {mean:.4g} m p99 {p99:.4g} m max {mx:.4g} m, flips {flips}")
+    assert mean <= mean_max and p99 <= p99_max, (mean, p99, mx)
+    if max_max is not None:
+        assert mx <= max_max, (mean, p99, mx)
+
+
+def test_reference_draws_in_fp32_mode_track_the_oracle(cuda_device):
+    """With the reference random keys the FP32 step takes the same draws as the FP64 oracle, so
+    a stochastic trajectory stays within FP32 rounding of it."""
+    win = syn.config1_window(n_frames=3)
+    p = syn.uniform_particles(4096, win.eta, win.xi, seed=9)
+    cfg = default_config(random=True, horizontalClosure=1)
+    want = _oracle(win, cfg, p, range(2))
+    with Engine(cuda_device, arithmetic="fp32", rng="reference") as e:
+        got = _run(e, win, cfg, p, range(2))
+    d = max_abs_diff(got, want)
+    assert d["i"] < 1e-4 and d["j"] < 1e-4 and d["k"] < 1e-4, d
+
+
+@pytest.mark.parametrize("rng", ["reference", "philox"])
+def test_diffusion_ensemble_moments(cuda_device, rng):
+    """No current, constant diffusivity: after n substeps of dt=dti the horizontal displacement
+    of each particle is sigma_k * sqrt(n) * N(0, 1) metres per axis (Particle.cpp:518-533), with
+    sigma_k = sigma (1 - k/kLower) at the release depth (k stays put: w=0, AKT=0)."""
+    win = syn.config1_window(n_frames=2, u=0.0, v=0.0, akt=0.0)
+    n = 200000
+    p = syn.uniform_particles(n, win.eta, win.xi, seed=4)
+    p["i"], p["j"], p["k"] = 60.5, 60.5, 0.0
+    cfg = default_config(random=True, horizontalClosure=1)
+    with Engine(cuda_device, arithmetic="fp32", rng=rng) as e:
+        got = _run(e, win, cfg, p, [0])
+    steps = 120
+    sigma_m = cfg.sigma * np.sqrt(steps)
+    lat0 = np.radians(win.lat[60, 0])
+    dx = 6371000.0 * np.radians(win.lon[0, 1] - win.lon[0, 0]) * np.cos(lat0)
+    dy = 6371000.0 * np.radians(win.lat[1, 0] - win.lat[0, 0])
+    x = (got["i"] - 60.5) * dx / sigma_m
+    y = (got["j"] - 60.5) * dy / sigma_m
+    for z in (x, y):
+        assert abs(z.mean()) < 5 / np.sqrt(n)
+        assert abs(z.var() - 1.0) < 0.02
+        assert abs(np.mean(z ** 4) - 3.0) < 0.1
+    assert abs(np.corrcoef(x, y)[0, 1]) < 0.01

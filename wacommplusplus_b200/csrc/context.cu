@@ -49,6 +49,8 @@ struct wacomm_b200_context {
     double *dMask = nullptr, *dLon = nullptr, *dLat = nullptr, *dH = nullptr, *dDepth = nullptr;
     bool hasMask = false;
     double2 *dMetric = nullptr;
+    float2 *dInvMetric = nullptr;
+    float *dDepthF = nullptr;
     int metricSemantics = -1;
 
     std::vector<double> times;
@@ -236,9 +238,25 @@ int validate_options(wacomm_b200_context *ctx, const wacomm_b200_options &o) {
 int ensure_metric(wacomm_b200_context *ctx) {
     if (ctx->metricSemantics == ctx->opt.semantics) return WACOMM_B200_OK;
     CUDA_TRY(ctx, build_metric(ctx->opt.semantics, ctx->eta, ctx->xi, ctx->dLon, ctx->dLat,
-                               ctx->dMetric, ctx->stream));
+                               ctx->dMetric, ctx->dInvMetric, ctx->stream));
     ctx->metricSemantics = ctx->opt.semantics;
     return WACOMM_B200_OK;
+}
+
+void release_frames(wacomm_b200_context *ctx) {
+    for (FrameSlot &s : ctx->slots) {
+        cudaFree(s.zeta);
+        cudaFree(s.u);
+        cudaFree(s.v);
+        cudaFree(s.w);
+        cudaFree(s.akt);
+        cudaFree(s.windU);
+        cudaFree(s.windV);
+        cudaFree(s.stokesU);
+        cudaFree(s.stokesV);
+        s = FrameSlot{};
+    }
+    ctx->pairT0 = ctx->pairT1 = -1;
 }
 
 FrameDevice frame_of(const FrameSlot &s) {
@@ -289,6 +307,8 @@ PackedArgs packed_args(wacomm_b200_context *ctx) {
     A.latRad = ctx->dLat;
     A.depthIntervals = ctx->dDepth;
     A.metric = ctx->dMetric;
+    A.invMetric = ctx->dInvMetric;
+    A.depthIntervalsF = ctx->dDepthF;
     return A;
 }
 
@@ -452,23 +472,15 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     if (!ctx) return WACOMM_B200_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (FrameSlot &s : ctx->slots) {
-        cudaFree(s.zeta);
-        cudaFree(s.u);
-        cudaFree(s.v);
-        cudaFree(s.w);
-        cudaFree(s.akt);
-        cudaFree(s.windU);
-        cudaFree(s.windV);
-        cudaFree(s.stokesU);
-        cudaFree(s.stokesV);
-    }
+    release_frames(ctx);
     cudaFree(ctx->dMask);
     cudaFree(ctx->dLon);
     cudaFree(ctx->dLat);
     cudaFree(ctx->dH);
     cudaFree(ctx->dDepth);
     cudaFree(ctx->dMetric);
+    cudaFree(ctx->dInvMetric);
+    cudaFree(ctx->dDepthF);
     cudaFree(ctx->dNodes);
     cudaFree(ctx->dSurf);
     cudaFree(ctx->dEnv);
@@ -540,6 +552,7 @@ int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, i
     if (!lon_rad || !lat_rad || !h || !depth_intervals)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null grid array");
     cudaSetDevice(ctx->device);
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     size_t plane = (size_t)eta * xi;
     cudaFree(ctx->dMask);
     cudaFree(ctx->dLon);
@@ -547,9 +560,13 @@ int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, i
     cudaFree(ctx->dH);
     cudaFree(ctx->dDepth);
     cudaFree(ctx->dMetric);
+    cudaFree(ctx->dInvMetric);
+    cudaFree(ctx->dDepthF);
     cudaFree(ctx->dSurf);
     ctx->dMask = ctx->dLon = ctx->dLat = ctx->dH = ctx->dDepth = nullptr;
     ctx->dMetric = nullptr;
+    ctx->dInvMetric = nullptr;
+    ctx->dDepthF = nullptr;
     ctx->dSurf = nullptr;
     cudaFree(ctx->dEnv);
     ctx->dEnv = nullptr;
@@ -559,12 +576,19 @@ int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, i
     CUDA_TRY(ctx, cudaMalloc(&ctx->dH, plane * sizeof(double)));
     CUDA_TRY(ctx, cudaMalloc(&ctx->dDepth, (size_t)(s_w - 1) * sizeof(double)));
     CUDA_TRY(ctx, cudaMalloc(&ctx->dMetric, plane * sizeof(double2)));
+    CUDA_TRY(ctx, cudaMalloc(&ctx->dInvMetric, plane * sizeof(float2)));
+    CUDA_TRY(ctx, cudaMalloc(&ctx->dDepthF, (size_t)(s_w - 1) * sizeof(float)));
     CUDA_TRY(ctx, cudaMalloc(&ctx->dSurf, plane * sizeof(SurfPair)));
     CUDA_TRY(ctx, cudaMemcpy(ctx->dLon, lon_rad, plane * sizeof(double), cudaMemcpyHostToDevice));
     CUDA_TRY(ctx, cudaMemcpy(ctx->dLat, lat_rad, plane * sizeof(double), cudaMemcpyHostToDevice));
     CUDA_TRY(ctx, cudaMemcpy(ctx->dH, h, plane * sizeof(double), cudaMemcpyHostToDevice));
     CUDA_TRY(ctx, cudaMemcpy(ctx->dDepth, depth_intervals, (size_t)(s_w - 1) * sizeof(double),
                              cudaMemcpyHostToDevice));
+    {
+        std::vector<float> depthF(depth_intervals, depth_intervals + (s_w - 1));
+        CUDA_TRY(ctx, cudaMemcpy(ctx->dDepthF, depthF.data(), depthF.size() * sizeof(float),
+                                 cudaMemcpyHostToDevice));
+    }
     ctx->hasMask = mask != nullptr;
     if (mask) {
         CUDA_TRY(ctx, cudaMalloc(&ctx->dMask, plane * sizeof(double)));
@@ -577,8 +601,8 @@ int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, i
     ctx->metricSemantics = -1;
     ctx->pairT0 = ctx->pairT1 = -1;
     ctx->hasGrid = true;
-    // Forcing records of another grid no longer fit.
-    for (FrameSlot &s : ctx->slots) s.loaded = false;
+    // Forcing records of another grid no longer fit: release them.
+    release_frames(ctx);
     return WACOMM_B200_OK;
 }
 

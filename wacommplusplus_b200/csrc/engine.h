@@ -23,6 +23,8 @@ struct PackedArgs {
     bool hasWindU, hasWindV, hasStokes;
     const double *lonRad, *latRad, *depthIntervals;
     const double2 *metric;
+    const float2 *invMetric;           // {1/xdist, 1/ydist} per cell (FP32 step)
+    const float *depthIntervalsF;      // FP32 copy of depthIntervals (FP32 step)
 };
 
 // move_ref.cu (reference arithmetic, FP32 storage)
@@ -49,7 +51,8 @@ cudaError_t pack_pair(int storage, int eta, int xi, int sW, const FrameDevice &f
                       EnvPair *env, cudaStream_t stream);
 
 cudaError_t build_metric(int semantics, int eta, int xi, const double *lonRad,
-                         const double *latRad, double2 *metric, cudaStream_t stream);
+                         const double *latRad, double2 *metric, float2 *invMetric,
+                         cudaStream_t stream);
 
 // Exclusive scan of n uint32 values; `temp` must hold scan_temp_words(n) words. The total is
 // written to *total (device).

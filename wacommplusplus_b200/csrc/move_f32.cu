@@ -1,5 +1,5 @@
-// Move kernels with FP32 interpolation over FP32, FP16 or BF16 forcing storage; positions,
-// time weights and metric ratios stay FP64.
+// FP32 move kernels (step_fast.cuh) over FP32, FP16 or BF16 forcing storage; positions and
+// closures stay FP64.
 #include "engine.h"
 #include "move_kernels.cuh"
 
@@ -22,20 +22,29 @@ static PackedView<STORE> typed_view(const PackedArgs &A) {
     return V;
 }
 
+template <int STORE>
+static FastView<STORE> fast_view(const PackedArgs &A) {
+    FastView<STORE> F;
+    F.V = typed_view<STORE>(A);
+    F.X.invMetric = A.invMetric;
+    F.X.depthIntervals = A.depthIntervalsF;
+    return F;
+}
+
 template <int SEM>
 static cudaError_t by_storage(int storage, const wacomm_b200_config &cfg, const IntervalParams &P,
                               const PackedArgs &A, const ParticleSoA &S, const MoveLaunch &L,
                               int blockSize, cudaStream_t stream) {
     switch (storage) {
         case STORE_F16:
-            return launch_move_soa<SEM, ARITH_F32, STORE_F16>(cfg, P, typed_view<STORE_F16>(A), S, L,
-                                                             blockSize, stream);
+            return launch_move_fast<SEM, STORE_F16>(cfg, P, fast_view<STORE_F16>(A), S, L,
+                                                    blockSize, stream);
         case STORE_BF16:
-            return launch_move_soa<SEM, ARITH_F32, STORE_BF16>(cfg, P, typed_view<STORE_BF16>(A), S,
-                                                              L, blockSize, stream);
+            return launch_move_fast<SEM, STORE_BF16>(cfg, P, fast_view<STORE_BF16>(A), S, L,
+                                                     blockSize, stream);
         default:
-            return launch_move_soa<SEM, ARITH_F32, STORE_F32>(cfg, P, typed_view<STORE_F32>(A), S, L,
-                                                             blockSize, stream);
+            return launch_move_fast<SEM, STORE_F32>(cfg, P, fast_view<STORE_F32>(A), S, L,
+                                                    blockSize, stream);
     }
 }
 

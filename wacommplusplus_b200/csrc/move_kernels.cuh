@@ -2,6 +2,7 @@
 #pragma once
 
 #include "step.cuh"
+#include "step_fast.cuh"
 
 namespace wb {
 
@@ -83,6 +84,53 @@ __global__ void __launch_bounds__(256) move_soa_kernel(const wacomm_b200_config 
     }
     if (L.steps) warp_sum_steps(L.steps, steps);
     if (L.conc && P.lastChunk) warp_count(L.conc, cell);
+}
+
+// FP32 step over the packed pair (step_fast.cuh); same state handling as move_soa_kernel.
+template <int SEM, int STORE>
+__global__ void __launch_bounds__(256) move_fast_kernel(const wacomm_b200_config cfg,
+                                                        const IntervalParams P,
+                                                        const FastView<STORE> F, ParticleSoA S,
+                                                        const MoveLaunch L) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    long long cell = -1;
+    int steps = 0;
+    if (t < L.count) {
+        uint32_t slot = L.order ? L.order[t] : (uint32_t)t;
+        ParticleState p;
+        p.id = S.id[slot];
+        p.k = S.k[slot];
+        p.j = S.j[slot];
+        p.i = S.i[slot];
+        p.health = S.health[slot];
+        p.age = S.age[slot];
+        p.time = S.time[slot];
+        p.type = S.type[slot];
+        p.side = S.side[slot];
+        double elapsed = P.firstChunk ? P.elapsed0 : S.elapsed[slot];
+        steps = move_particle_fast<SEM, STORE>(cfg, P, F, p, elapsed, L.err);
+        S.k[slot] = p.k;
+        S.j[slot] = p.j;
+        S.i[slot] = p.i;
+        S.health[slot] = p.health;
+        S.age[slot] = p.age;
+        S.side[slot] = (int8_t)p.side;
+        if (!P.lastChunk) S.elapsed[slot] = elapsed;
+        if (L.conc && P.lastChunk)
+            cell = concentration_cell(p, L.concTimeIndex, F.V.g.sRho, F.V.g.eta, F.V.g.xi);
+    }
+    if (L.steps) warp_sum_steps(L.steps, steps);
+    if (L.conc && P.lastChunk) warp_count(L.conc, cell);
+}
+
+template <int SEM, int STORE>
+cudaError_t launch_move_fast(const wacomm_b200_config &cfg, const IntervalParams &P,
+                             const FastView<STORE> &F, const ParticleSoA &S, const MoveLaunch &L,
+                             int blockSize, cudaStream_t stream) {
+    if (L.count <= 0) return cudaSuccess;
+    int blocks = (L.count + blockSize - 1) / blockSize;
+    move_fast_kernel<SEM, STORE><<<blocks, blockSize, 0, stream>>>(cfg, P, F, S, L);
+    return cudaGetLastError();
 }
 
 // Host launchers (one per template instance, defined in the instantiation units).

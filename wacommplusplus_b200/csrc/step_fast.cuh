@@ -1,0 +1,365 @@
+// The FP32 particle step: the same algorithm as step.cuh with FP32 interpolation and metric,
+// FP64 kept for the position accumulation, the closures and the interval clock.
+//
+// Differences from the reference arithmetic (all below the reference's own CPU/GPU snapshot
+// tolerance once forcing is FP32, and stated per configuration in the parity tests):
+//   * corner weights, time blends and the velocity/diffusivity sums are FP32 with fused
+//     multiply-adds;
+//   * cell sizes come from a per-cell table of reciprocals, so index increments are products
+//     (u dt / dx) instead of double divisions, and the midpoint stage is written directly in
+//     index units (u* dt / dx*, algebraically the reference's s u* dt dx/dx* / dx);
+//   * the time weight uses a multiply by 1/length.
+// Host and device rules keep their differences in closures, level checks and metric formula.
+#pragma once
+
+#include "step.cuh"
+
+namespace wb {
+
+struct FastExtras {
+    const float2 *invMetric;     // [eta][xi] {1/xdist, 1/ydist}
+    const float *depthIntervals; // [sW-1]
+};
+
+template <int STORE>
+struct FastView {
+    PackedView<STORE> V;
+    FastExtras X;
+};
+
+// Bilinear FP32 interpolation of the four surface records (h, zeta blended in time).
+template <class View>
+__device__ __forceinline__ float surface_fast(const View &V, int jI, int iI, float jF, float iF,
+                                              float a) {
+    SurfPair s1 = V.surface(jI, iI), s2 = V.surface(jI + 1, iI);
+    SurfPair s3 = V.surface(jI + 1, iI + 1), s4 = V.surface(jI, iI + 1);
+    float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
+    float c1 = (float)s1.h + at_f32(s1.z0, s1.z1, a);
+    float c2 = (float)s2.h + at_f32(s2.z0, s2.z1, a);
+    float c3 = (float)s3.h + at_f32(s3.z0, s3.z1, a);
+    float c4 = (float)s4.h + at_f32(s4.z0, s4.z1, a);
+    return c1 * w1 + c2 * w2 + c3 * w3 + c4 * w4;
+}
+
+// Leeway and Stokes velocity of a drifting object (the drift branch of advective_velocity),
+// kept out of line so the passive-particle step carries none of its registers.
+template <class View>
+__device__ __noinline__ void drift_velocity(const wacomm_b200_config &cfg, const IntervalParams &P,
+                                            const View &V, uint64_t id, int type, int side,
+                                            int jI, double jF, int iI, double iF, double sa,
+                                            double elapsed, double physicalTime, double stepDt,
+                                            float &du, float &dv) {
+    double windU = cfg.windU10, windV = cfg.windV10;
+    EnvPair e1{}, e2{}, e3{}, e4{};
+    if (V.hasWindU || V.hasWindV || V.hasStokes) {
+        e1 = V.environment(jI, iI);
+        e2 = V.environment(jI + 1, iI);
+        e3 = V.environment(jI + 1, iI + 1);
+        e4 = V.environment(jI, iI + 1);
+    }
+    float fi = (float)iF, fj = (float)jF, a = (float)sa;
+    float w1 = (1.f - fi) * (1.f - fj), w2 = (1.f - fi) * fj, w3 = fi * fj, w4 = fi * (1.f - fj);
+    if (V.hasWindU)
+        windU = at_f32(e1.wu0 * w1 + e2.wu0 * w2 + e3.wu0 * w3 + e4.wu0 * w4,
+                       e1.wu1 * w1 + e2.wu1 * w2 + e3.wu1 * w3 + e4.wu1 * w4, a);
+    if (V.hasWindV)
+        windV = at_f32(e1.wv0 * w1 + e2.wv0 * w2 + e3.wv0 * w3 + e4.wv0 * w4,
+                       e1.wv1 * w1 + e2.wv1 * w2 + e3.wv1 * w3 + e4.wv1 * w4, a);
+    double longitude = V.lon(jI, iI) * (1.0 - iF) * (1.0 - jF) + V.lon(jI + 1, iI) * (1.0 - iF) * jF +
+                       V.lon(jI + 1, iI + 1) * iF * jF + V.lon(jI, iI + 1) * iF * (1.0 - jF);
+    double latitude = V.lat(jI, iI) * (1.0 - iF) * (1.0 - jF) + V.lat(jI + 1, iI) * (1.0 - iF) * jF +
+                      V.lat(jI + 1, iI + 1) * iF * jF + V.lat(jI, iI + 1) * iF * (1.0 - jF);
+    double stdDev = cfg.windErrorStdDev, corr = cfg.windErrorComponentCorrelation;
+    double spatial = cfg.windErrorSpatialScale, temporal = cfg.windErrorTemporalScale;
+    int region = calibration_region(cfg, longitude, latitude);
+    if (region >= 0) {
+        const wacomm_b200_calibration_region &g = cfg.observationalCalibrationRegions[region];
+        stdDev = g.windErrorStdDev;
+        corr = g.windErrorComponentCorrelation;
+        spatial = g.windErrorSpatialScale;
+        temporal = g.windErrorTemporalScale;
+    }
+    if (stdDev > 0) {
+        uint64_t substep = (uint64_t)floor(elapsed / cfg.dti);
+        double when = physicalTime + .5 * P.direction * stepDt;
+        double first = forcing_error_normal(cfg.randomSeed, id, P.intervalKey, substep,
+                                            WIND_U_COMPONENT, longitude, latitude, when, spatial,
+                                            temporal);
+        double second = forcing_error_normal(cfg.randomSeed, id, P.intervalKey, substep,
+                                             WIND_V_COMPONENT, longitude, latitude, when, spatial,
+                                             temporal);
+        windU += stdDev * first;
+        windV += stdDev * correlated_normal(first, second, corr);
+    }
+    double dn = 0, cn = 0;
+    if (cfg.leewayCoefficientEnsemble) {
+        uint64_t ens = key_prefix(cfg.randomSeed, id, ENSEMBLE_INTERVAL, 0);
+        dn = prefix_normal(ens, 0);
+        cn = correlated_normal(dn, prefix_normal(ens, 1), cfg.leewayResidualCorrelation);
+    }
+    Leeway lw = compute_leeway(type, windU, windV, side, dn, cn);
+    du = (float)lw.u;
+    dv = (float)lw.v;
+    if (V.hasStokes) {
+        du += at_f32(e1.su0 * w1 + e2.su0 * w2 + e3.su0 * w3 + e4.su0 * w4,
+                     e1.su1 * w1 + e2.su1 * w2 + e3.su1 * w3 + e4.su1 * w4, a);
+        dv += at_f32(e1.sv0 * w1 + e2.sv0 * w2 + e3.sv0 * w3 + e4.sv0 * w4,
+                     e1.sv1 * w1 + e2.sv1 * w2 + e3.sv1 * w3 + e4.sv1 * w4, a);
+    }
+}
+
+// Ocean velocity (u, v, w) at a fractional position, FP32.
+template <class View>
+__device__ __forceinline__ void current_fast(const View &V, int kI, float kF, int jI, float jF,
+                                             int iI, float iF, float a, float &uu, float &vv,
+                                             float &ww) {
+    NodeUp c1 = V.up(kI, jI, iI), c2 = V.up(kI, jI + 1, iI);
+    NodeUp c3 = V.up(kI, jI + 1, iI + 1), c4 = V.up(kI, jI, iI + 1);
+    NodeLo l1 = V.lo(kI, jI, iI), l2 = V.lo(kI, jI + 1, iI);
+    NodeLo l3 = V.lo(kI, jI + 1, iI + 1), l4 = V.lo(kI, jI, iI + 1);
+    float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
+    uu = at_f32(c1.u0, c1.u1, a) * w1 + at_f32(c2.u0, c2.u1, a) * w2 + at_f32(c3.u0, c3.u1, a) * w3 +
+         at_f32(c4.u0, c4.u1, a) * w4;
+    vv = at_f32(c1.v0, c1.v1, a) * w1 + at_f32(c2.v0, c2.v1, a) * w2 + at_f32(c3.v0, c3.v1, a) * w3 +
+         at_f32(c4.v0, c4.v1, a) * w4;
+    float up = at_f32(c1.w0, c1.w1, a) * w1 + at_f32(c2.w0, c2.w1, a) * w2 +
+               at_f32(c3.w0, c3.w1, a) * w3 + at_f32(c4.w0, c4.w1, a) * w4;
+    float lo = at_f32(l1.w0, l1.w1, a) * w1 + at_f32(l2.w0, l2.w1, a) * w2 +
+               at_f32(l3.w0, l3.w1, a) * w3 + at_f32(l4.w0, l4.w1, a) * w4;
+    ww = up + (lo - up) * kF;
+}
+
+template <class View>
+__device__ __forceinline__ float akt_fast(const View &V, int kI, float kF, int jI, float jF, int iI,
+                                          float iF, float a) {
+    NodeUp c1 = V.up(kI, jI, iI), c2 = V.up(kI, jI + 1, iI);
+    NodeUp c3 = V.up(kI, jI + 1, iI + 1), c4 = V.up(kI, jI, iI + 1);
+    NodeLo l1 = V.lo(kI, jI, iI), l2 = V.lo(kI, jI + 1, iI);
+    NodeLo l3 = V.lo(kI, jI + 1, iI + 1), l4 = V.lo(kI, jI, iI + 1);
+    float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
+    float up = at_f32(c1.a0, c1.a1, a) * w1 + at_f32(c2.a0, c2.a1, a) * w2 +
+               at_f32(c3.a0, c3.a1, a) * w3 + at_f32(c4.a0, c4.a1, a) * w4;
+    float lo = at_f32(l1.a0, l1.a1, a) * w1 + at_f32(l2.a0, l2.a1, a) * w2 +
+               at_f32(l3.a0, l3.a1, a) * w3 + at_f32(l4.a0, l4.a1, a) * w4;
+    return up + (lo - up) * kF;
+}
+
+__device__ __forceinline__ float signf_of(float a, float b) {
+    return fabsf(a) * (float)((b > 0.f) - (b < 0.f));
+}
+
+template <int SEM, int STORE>
+__device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalParams &P,
+                                  const FastView<STORE> &F, ParticleState &p, double &elapsed,
+                                  int *err) {
+    const PackedView<STORE> &V = F.V;
+    const int eta = V.g.eta, xi = V.g.xi, sW = V.g.sW;
+    const double kLower = P.kLower, length = P.length;
+    const double invLength = length == 0 ? 0.0 : 1.0 / length;
+    const int direction = P.direction;
+    const float dirf = (float)direction;
+    const float sv = (float)cfg.sv, shore = (float)cfg.shoreLimit;
+    const bool midpoint = cfg.integrator == INTEGRATOR_MIDPOINT;
+    const bool diffuse = cfg.random && (direction > 0 || cfg.backwardDiffusion);
+    const bool drift = cfg.driftModel == 1 && p.type != 0;
+    const bool jibe = cfg.leewayJibeProbabilityHourly > 0 && p.type != 0;
+    if (drift && SEM == SEM_HOST && (p.type < 0 || p.type > 22)) atomicOr(err, ERR_DRIFT_OBJECT);
+    bool lazy = false;
+    int steps = 0;
+
+    if (P.firstChunk) {
+        if (p.k > 0) close_upper(cfg, p.k, p.health, lazy);
+        if (p.k < kLower) close_lower(cfg, kLower, p.k, p.health, lazy);
+    }
+    const uint64_t prefix = fold(fold(mix64(cfg.randomSeed), p.id), (uint64_t)P.intervalKey);
+    const uint64_t philoxKey = p.id ^ mix64(cfg.randomSeed);
+    const double stop = P.chunkEnd < length ? P.chunkEnd : length;
+
+    while (elapsed < stop) {
+        double stepDt = fmin(cfg.dti, length - elapsed);
+        double physicalTime = P.start + direction * elapsed;
+        if (direction > 0 && p.time > physicalTime) {
+            elapsed = fmin(length, p.time - P.start);
+            continue;
+        }
+        bool dead = lazy ? (p.age >= P.ageKillHi ||
+                            (p.age > P.ageKillLo && exp(-p.age / cfg.tau0) < cfg.survprob))
+                         : p.health < cfg.survprob;
+        if (dead) {
+            p.health = -1;
+            lazy = false;
+            elapsed = length;
+            break;
+        }
+        double kc = ceil(p.k), fj0 = floor(p.j), fi0 = floor(p.i);
+        int kI = to_index<SEM>(kc), jI = to_index<SEM>(fj0), iI = to_index<SEM>(fi0);
+        if (!valid_cell(jI, iI, eta, xi) || (SEM == SEM_DEVICE && (kI > 0 || kI <= -sW + 1))) {
+            p.health = -1;
+            lazy = false;
+            elapsed = length;
+            break;
+        }
+        steps++;
+        const float kF = (float)(kc - p.k), jF = (float)(p.j - fj0), iF = (float)(p.i - fi0);
+        const float dt = (float)stepDt;
+        const float alpha = (float)((elapsed + 0.5 * stepDt) * invLength);
+        const float alphaStart = (float)(elapsed * invLength);
+        const float hc = surface_fast(V, jI, iI, jF, iF, alpha);
+        if (hc <= shore && cfg.horizontalClosure == CLOSURE_KILL) {
+            p.health = -1;
+            lazy = false;
+            if (SEM == SEM_DEVICE) {
+                elapsed = length;
+                break;
+            }
+        }
+        const int kM = mem_level(kI, sW);
+        const float sa = midpoint ? alphaStart : alpha;
+        float uu, vv, ww;
+        current_fast(V, kM, kF, jI, jF, iI, iF, sa, uu, vv, ww);
+        if (drift) {
+            float du, dv;
+            drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, (double)jF, iI, (double)iF, sa,
+                           elapsed, physicalTime, stepDt, du, dv);
+            uu += du;
+            vv += dv;
+        }
+        uint64_t substep = 0, stepKey = 0;
+        if (diffuse || jibe) {
+            substep = (uint64_t)floor(elapsed / cfg.dti);
+            stepKey = fold(prefix, substep);
+        }
+        float rx = 0.f, ry = 0.f, rz = 0.f;
+        if (diffuse) {
+            float aa = akt_fast(V, kM, kF, jI, jF, iI, iF, alpha);
+            float sigmaDepth = (float)(cfg.sigma * (1 - p.k / kLower));
+            float scale = sqrtf(dt / (float)cfg.dti);
+            float n0, n1, n2;
+            if (P.rng == WACOMM_B200_RNG_PHILOX) {
+                philox_normals3(philoxKey, P.intervalKey, substep, n0, n1, n2);
+            } else {
+                n0 = (float)prefix_normal(stepKey, 0);
+                n1 = (float)prefix_normal(stepKey, 1);
+                n2 = (float)prefix_normal(stepKey, 2);
+            }
+            rx = sigmaDepth * n0 * scale;
+            ry = sigmaDepth * n1 * scale;
+            rz = sigmaDepth * n2 * aa * (float)cfg.crid * scale;
+        }
+        const float2 inv = __ldg(F.X.invMetric + (size_t)jI * xi + iI);
+        const float zdist = hc * __ldg(F.X.depthIntervals + (kM + sW - 2));
+        // index increments (i, j) and the vertical leap in metres
+        float dI, dJ, zleap;
+        if (midpoint) {
+            float kHalf = dirf * (sv + ww) * 0.5f * dt;
+            if (fabsf(kHalf) > zdist) kHalf = signf_of(zdist, kHalf);
+            double iMid = p.i + (double)(dirf * uu * 0.5f * dt * inv.x);
+            double jMid = p.j + (double)(dirf * vv * 0.5f * dt * inv.y);
+            double kMid = fmin(0.0, fmax(kLower, p.k + (double)(kHalf / zdist)));
+            double fim = floor(iMid), fjm = floor(jMid);
+            int iMI = to_index<SEM>(fim), jMI = to_index<SEM>(fjm);
+            bool midValid = valid_cell(jMI, iMI, eta, xi);
+            float hcMid = 0.f, iMF = 0.f, jMF = 0.f;
+            if (midValid) {
+                iMF = (float)(iMid - fim);
+                jMF = (float)(jMid - fjm);
+                hcMid = surface_fast(V, jMI, iMI, jMF, iMF, alpha);
+                midValid = hcMid > shore && hcMid > 0.f;
+            }
+            float detZ;
+            if (midValid) {
+                double kmc = ceil(kMid);
+                int kMI = mem_level(to_index<SEM>(kmc), sW);
+                float kMF = (float)(kmc - kMid);
+                float um, vm, wm;
+                current_fast(V, kMI, kMF, jMI, jMF, iMI, iMF, alpha, um, vm, wm);
+                if (drift) {
+                    float du, dv;
+                    drift_velocity(cfg, P, V, p.id, p.type, p.side, jMI, (double)jMF, iMI,
+                                   (double)iMF, (double)alpha, elapsed, physicalTime, stepDt, du, dv);
+                    um += du;
+                    vm += dv;
+                }
+                const float2 im = __ldg(F.X.invMetric + (size_t)jMI * xi + iMI);
+                float zdistMid = hcMid * __ldg(F.X.depthIntervals + (kMI + sW - 2));
+                dI = dirf * um * dt * im.x;
+                dJ = dirf * vm * dt * im.y;
+                detZ = dirf * (sv + wm) * dt * zdist / zdistMid;
+            } else {
+                float ue, ve, we;
+                current_fast(V, kM, kF, jI, jF, iI, iF, alpha, ue, ve, we);
+                if (drift) {
+                    float du, dv;
+                    drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, (double)jF, iI,
+                                   (double)iF, (double)alpha, elapsed, physicalTime, stepDt, du, dv);
+                    ue += du;
+                    ve += dv;
+                }
+                dI = dirf * ue * dt * inv.x;
+                dJ = dirf * ve * dt * inv.y;
+                detZ = dirf * (sv + we) * dt;
+            }
+            dI += rx * inv.x;
+            dJ += ry * inv.y;
+            zleap = detZ + rz;
+        } else {
+            dI = (dirf * uu * dt + rx) * inv.x;
+            dJ = (dirf * vv * dt + ry) * inv.y;
+            zleap = dirf * (sv + ww) * dt + rz;
+        }
+        if (fabsf(zleap) > zdist) zleap = signf_of(zdist, zleap);
+        double jdet = p.j + (double)dJ;
+        double idet = p.i + (double)dI;
+        double kdet = p.k + (double)(zleap / zdist);
+        if (kdet > 0.) close_upper(cfg, kdet, p.health, lazy);
+        if (kdet < kLower) close_lower(cfg, kLower, kdet, p.health, lazy);
+
+        double fjd = floor(jdet), fid = floor(idet);
+        int jdetI = to_index<SEM>(fjd), idetI = to_index<SEM>(fid);
+        if (valid_cell(jdetI, idetI, eta, xi)) {
+            float hcdet = surface_fast(V, jdetI, idetI, (float)(jdet - fjd), (float)(idet - fid), alpha);
+            if (hcdet <= shore) {
+                if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
+                    idet = p.i;
+                    jdet = p.j;
+                } else if (cfg.horizontalClosure == CLOSURE_KILL) {
+                    p.health = -1;
+                    lazy = false;
+                } else if (cfg.horizontalClosure == CLOSURE_REFLECTION) {
+                    idet = reflect_cell(p.i, iI, idet, idetI);
+                    jdet = reflect_cell(p.j, jI, jdet, jdetI);
+                }
+            }
+            p.i = idet;
+            p.j = jdet;
+            p.k = kdet;
+        } else {
+            if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
+                p.k = kdet;
+            } else if (cfg.horizontalClosure == CLOSURE_KILL) {
+                p.health = -1;
+                lazy = false;
+            } else if (cfg.horizontalClosure == CLOSURE_REFLECTION) {
+                p.i = reflect_domain(idet, xi - 1);
+                p.j = reflect_domain(jdet, eta - 1);
+                p.k = kdet;
+            }
+        }
+        bool alive = lazy ? (p.age < P.ageUnder || exp(-p.age / cfg.tau0) > 0) : p.health > 0;
+        if (alive) {
+            p.age = p.age + stepDt;
+            lazy = true;
+            if (jibe) {
+                double probability = stepDt == cfg.dti
+                                         ? P.jibeFullStep
+                                         : jibe_step_probability(cfg.leewayJibeProbabilityHourly, stepDt);
+                if (prefix_uniform(stepKey, JIBE_COMPONENT) < probability) p.side = -p.side;
+            }
+        }
+        elapsed += stepDt;
+    }
+    if (lazy) p.health = exp(-p.age / cfg.tau0);
+    return steps;
+}
+
+}  // namespace wb

@@ -121,13 +121,14 @@ cudaError_t pack_pair(int storage, int eta, int xi, int sW, const FrameDevice &f
 // with the cross difference dropped (Particle.cpp:548-574); device rules: full haversine between
 // the nodes (kernel.cu:145-149,278-279). Cells on the last row/column are never valid.
 __global__ void metric_kernel(int semantics, int eta, int xi, const double *lat,
-                              const double *lon, double2 *metric) {
+                              const double *lon, double2 *metric, float2 *invMetric) {
     size_t plane = (size_t)eta * xi;
     for (size_t n = blockIdx.x * (size_t)blockDim.x + threadIdx.x; n < plane;
          n += (size_t)gridDim.x * blockDim.x) {
         int j = (int)(n / xi), i = (int)(n - (size_t)j * xi);
         if (j + 1 >= eta || i + 1 >= xi) {
             metric[n] = make_double2(0.0, 0.0);
+            invMetric[n] = make_float2(0.f, 0.f);
             continue;
         }
         double lat0 = lat[n], lon0 = lon[n];
@@ -151,13 +152,15 @@ __global__ void metric_kernel(int semantics, int eta, int xi, const double *lat,
             xdist = 2.0 * atan2(sqrt(value), sqrt(1.0 - value)) * 6371000.0;
         }
         metric[n] = make_double2(xdist, ydist);
+        invMetric[n] = make_float2((float)(1.0 / xdist), (float)(1.0 / ydist));
     }
 }
 
 cudaError_t build_metric(int semantics, int eta, int xi, const double *lonRad,
-                         const double *latRad, double2 *metric, cudaStream_t stream) {
+                         const double *latRad, double2 *metric, float2 *invMetric,
+                         cudaStream_t stream) {
     metric_kernel<<<grid_for((size_t)eta * xi, 256), 256, 0, stream>>>(semantics, eta, xi, latRad,
-                                                                      lonRad, metric);
+                                                                      lonRad, metric, invMetric);
     return cudaGetLastError();
 }
 
