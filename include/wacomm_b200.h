@@ -105,6 +105,9 @@ typedef struct wacomm_b200_options {
     int substeps_per_launch;  /* 0: one launch per interval; else launches of this many dti */
     int sort_by_cell;         /* 1: order the work by forcing cell before each launch */
     int fuse_concentration;   /* 1: count the concentration in the move kernel's epilogue */
+    int launch_shape;         /* FP32 step: 0 = 256 threads, registers unbounded; 1 = 128 threads,
+                                 3 blocks/SM; 2 = 256 threads, 2 blocks/SM; 3 = 128 threads,
+                                 5 blocks/SM (fewer registers, more resident warps) */
 } wacomm_b200_options;
 
 /* ------------------------------------------------------------------ context */
@@ -121,7 +124,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx);
 const char *wacomm_b200_last_error(const wacomm_b200_context *ctx);
 
 /* Fills *out with the defaults: host semantics, FP32 arithmetic and storage, reference RNG,
- * 256 threads, one launch per interval, cell sort on, fused concentration on. */
+ * 256 threads, one launch per interval, cell sort on, fused concentration on, launch shape 1. */
 int wacomm_b200_default_options(wacomm_b200_options *out);
 int wacomm_b200_set_options(wacomm_b200_context *ctx, const wacomm_b200_options *options);
 int wacomm_b200_get_options(const wacomm_b200_context *ctx, wacomm_b200_options *out);

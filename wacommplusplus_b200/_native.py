@@ -30,7 +30,7 @@ class options_t(ctypes.Structure):
         ("semantics", ctypes.c_int), ("arithmetic", ctypes.c_int), ("storage", ctypes.c_int),
         ("rng", ctypes.c_int), ("block_size", ctypes.c_int),
         ("substeps_per_launch", ctypes.c_int), ("sort_by_cell", ctypes.c_int),
-        ("fuse_concentration", ctypes.c_int),
+        ("fuse_concentration", ctypes.c_int), ("launch_shape", ctypes.c_int),
     ]
 
 

@@ -58,6 +58,9 @@ struct wacomm_b200_context {
 
     void *dNodes = nullptr;
     size_t nodesBytes = 0;
+    void *dCells = nullptr, *dCellSurface = nullptr;
+    size_t cellsBytes = 0, cellSurfaceBytes = 0;
+    bool pairCells = false;
     SurfPair *dSurf = nullptr;
     EnvPair *dEnv = nullptr;
     int pairT0 = -1, pairT1 = -1, pairStorage = -1;
@@ -232,6 +235,8 @@ int validate_options(wacomm_b200_context *ctx, const wacomm_b200_options &o) {
                     o.block_size);
     if (o.substeps_per_launch < 0)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "substeps_per_launch must be >= 0");
+    if (o.launch_shape < 0 || o.launch_shape > 3)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "launch_shape %d out of [0, 3]", o.launch_shape);
     return WACOMM_B200_OK;
 }
 
@@ -266,8 +271,9 @@ FrameDevice frame_of(const FrameSlot &s) {
 int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
     const FrameSlot &a = ctx->slots[t0], &b = ctx->slots[t1];
     bool env = a.windU || a.windV || a.stokesU || b.windU || b.windV || b.stokesU;
+    bool cells = ctx->opt.arithmetic == WACOMM_B200_ARITH_FP32;
     if (ctx->pairT0 == t0 && ctx->pairT1 == t1 && ctx->pairStorage == ctx->opt.storage &&
-        ctx->pairEnv == env)
+        ctx->pairEnv == env && (!cells || ctx->pairCells))
         return WACOMM_B200_OK;
     size_t plane = (size_t)ctx->eta * ctx->xi;
     size_t need = plane * ctx->sW * node_record_bytes(ctx->opt.storage);
@@ -283,10 +289,32 @@ int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
                             ctx->dH, ctx->dNodes, ctx->dSurf, env ? ctx->dEnv : nullptr,
                             ctx->stream));
     launches += 2;
+    if (cells) {
+        size_t cneed = plane * ctx->sW * cell_record_bytes(ctx->opt.storage);
+        if (cneed > ctx->cellsBytes) {
+            cudaFree(ctx->dCells);
+            ctx->dCells = nullptr;
+            ctx->cellsBytes = 0;
+            CUDA_TRY(ctx, cudaMalloc(&ctx->dCells, cneed));
+            ctx->cellsBytes = cneed;
+        }
+        size_t sneed = plane * cell_surface_bytes();
+        if (sneed > ctx->cellSurfaceBytes) {
+            cudaFree(ctx->dCellSurface);
+            ctx->dCellSurface = nullptr;
+            ctx->cellSurfaceBytes = 0;
+            CUDA_TRY(ctx, cudaMalloc(&ctx->dCellSurface, sneed));
+            ctx->cellSurfaceBytes = sneed;
+        }
+        CUDA_TRY(ctx, pack_cells(ctx->opt.storage, ctx->eta, ctx->xi, ctx->sW, frame_of(a),
+                                 frame_of(b), ctx->dH, ctx->dCells, ctx->dCellSurface, ctx->stream));
+        launches += 2;
+    }
     ctx->pairT0 = t0;
     ctx->pairT1 = t1;
     ctx->pairStorage = ctx->opt.storage;
     ctx->pairEnv = env;
+    ctx->pairCells = cells;
     return WACOMM_B200_OK;
 }
 
@@ -309,6 +337,8 @@ PackedArgs packed_args(wacomm_b200_context *ctx) {
     A.metric = ctx->dMetric;
     A.invMetric = ctx->dInvMetric;
     A.depthIntervalsF = ctx->dDepthF;
+    A.cells = ctx->dCells;
+    A.cellSurface = ctx->dCellSurface;
     return A;
 }
 
@@ -374,8 +404,8 @@ int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t of
             e = move_ref_dispatch(ctx->opt.semantics, ctx->cfg, P, A, S, L, ctx->opt.block_size,
                                   ctx->stream);
         else
-            e = move_f32_dispatch(ctx->opt.semantics, ctx->opt.storage, ctx->cfg, P, A, S, L,
-                                  ctx->opt.block_size, ctx->stream);
+            e = move_f32_dispatch(ctx->opt.semantics, ctx->opt.storage, ctx->opt.launch_shape,
+                                  ctx->cfg, P, A, S, L, ctx->stream);
         if (e != cudaSuccess)
             return fail(ctx, WACOMM_B200_ERR_CUDA, "move launch: %s", cudaGetErrorString(e));
         launches++;
@@ -437,6 +467,7 @@ int wacomm_b200_default_options(wacomm_b200_options *out) {
     out->substeps_per_launch = 0;
     out->sort_by_cell = 1;
     out->fuse_concentration = 1;
+    out->launch_shape = 1;
     return WACOMM_B200_OK;
 }
 
@@ -482,6 +513,8 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dInvMetric);
     cudaFree(ctx->dDepthF);
     cudaFree(ctx->dNodes);
+    cudaFree(ctx->dCells);
+    cudaFree(ctx->dCellSurface);
     cudaFree(ctx->dSurf);
     cudaFree(ctx->dEnv);
     free_soa(ctx->S);

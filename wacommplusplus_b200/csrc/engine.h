@@ -25,6 +25,8 @@ struct PackedArgs {
     const double2 *metric;
     const float2 *invMetric;           // {1/xdist, 1/ydist} per cell (FP32 step)
     const float *depthIntervalsF;      // FP32 copy of depthIntervals (FP32 step)
+    const void *cells;                 // CellQuad<storage>[eta*xi][sW][2] (FP32 step)
+    const void *cellSurface;           // CellSurface[eta*xi] (FP32 step)
 };
 
 // move_ref.cu (reference arithmetic, FP32 storage)
@@ -32,9 +34,9 @@ cudaError_t move_ref_dispatch(int semantics, const wacomm_b200_config &cfg,
                               const IntervalParams &P, const PackedArgs &A, const ParticleSoA &S,
                               const MoveLaunch &L, int blockSize, cudaStream_t stream);
 // move_f32.cu (FP32 arithmetic, any storage)
-cudaError_t move_f32_dispatch(int semantics, int storage, const wacomm_b200_config &cfg,
+cudaError_t move_f32_dispatch(int semantics, int storage, int shape, const wacomm_b200_config &cfg,
                               const IntervalParams &P, const PackedArgs &A, const ParticleSoA &S,
-                              const MoveLaunch &L, int blockSize, cudaStream_t stream);
+                              const MoveLaunch &L, cudaStream_t stream);
 
 // support.cu ----------------------------------------------------------------------------
 
@@ -49,6 +51,14 @@ struct FrameDevice {  // one forcing record in the reference layout (device)
 cudaError_t pack_pair(int storage, int eta, int xi, int sW, const FrameDevice &f0,
                       const FrameDevice &f1, const double *h, void *nodes, SurfPair *surf,
                       EnvPair *env, cudaStream_t stream);
+
+// Cell-column layout of the pair for the FP32 step (views.cuh): bytes per (cell, level) and per
+// cell surface, and the packing kernel.
+size_t cell_record_bytes(int storage);
+size_t cell_surface_bytes();
+cudaError_t pack_cells(int storage, int eta, int xi, int sW, const FrameDevice &f0,
+                       const FrameDevice &f1, const double *h, void *cells, void *cellSurface,
+                       cudaStream_t stream);
 
 cudaError_t build_metric(int semantics, int eta, int xi, const double *lonRad,
                          const double *latRad, double2 *metric, float2 *invMetric,

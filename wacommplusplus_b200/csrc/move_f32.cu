@@ -28,32 +28,44 @@ static FastView<STORE> fast_view(const PackedArgs &A) {
     F.V = typed_view<STORE>(A);
     F.X.invMetric = A.invMetric;
     F.X.depthIntervals = A.depthIntervalsF;
+    F.C.eta = A.eta;
+    F.C.xi = A.xi;
+    F.C.sW = A.sW;
+    F.C.columns = static_cast<const CellQuad<STORE> *>(A.cells);
+    F.C.surface = static_cast<const CellSurface *>(A.cellSurface);
     return F;
 }
 
-template <int SEM>
-static cudaError_t by_storage(int storage, const wacomm_b200_config &cfg, const IntervalParams &P,
-                              const PackedArgs &A, const ParticleSoA &S, const MoveLaunch &L,
-                              int blockSize, cudaStream_t stream) {
-    switch (storage) {
-        case STORE_F16:
-            return launch_move_fast<SEM, STORE_F16>(cfg, P, fast_view<STORE_F16>(A), S, L,
-                                                    blockSize, stream);
-        case STORE_BF16:
-            return launch_move_fast<SEM, STORE_BF16>(cfg, P, fast_view<STORE_BF16>(A), S, L,
-                                                     blockSize, stream);
-        default:
-            return launch_move_fast<SEM, STORE_F32>(cfg, P, fast_view<STORE_F32>(A), S, L,
-                                                    blockSize, stream);
+template <int SEM, int STORE>
+static cudaError_t by_shape(int shape, const wacomm_b200_config &cfg, const IntervalParams &P,
+                            const PackedArgs &A, const ParticleSoA &S, const MoveLaunch &L,
+                            cudaStream_t stream) {
+    FastView<STORE> F = fast_view<STORE>(A);
+    switch (shape) {
+        case 0: return launch_move_fast<SEM, STORE, 0>(cfg, P, F, S, L, stream);
+        case 2: return launch_move_fast<SEM, STORE, 2>(cfg, P, F, S, L, stream);
+        case 3: return launch_move_fast<SEM, STORE, 3>(cfg, P, F, S, L, stream);
+        default: return launch_move_fast<SEM, STORE, 1>(cfg, P, F, S, L, stream);
     }
 }
 
-cudaError_t move_f32_dispatch(int semantics, int storage, const wacomm_b200_config &cfg,
+template <int SEM>
+static cudaError_t by_storage(int storage, int shape, const wacomm_b200_config &cfg,
                               const IntervalParams &P, const PackedArgs &A, const ParticleSoA &S,
-                              const MoveLaunch &L, int blockSize, cudaStream_t stream) {
+                              const MoveLaunch &L, cudaStream_t stream) {
+    switch (storage) {
+        case STORE_F16: return by_shape<SEM, STORE_F16>(shape, cfg, P, A, S, L, stream);
+        case STORE_BF16: return by_shape<SEM, STORE_BF16>(shape, cfg, P, A, S, L, stream);
+        default: return by_shape<SEM, STORE_F32>(shape, cfg, P, A, S, L, stream);
+    }
+}
+
+cudaError_t move_f32_dispatch(int semantics, int storage, int shape, const wacomm_b200_config &cfg,
+                              const IntervalParams &P, const PackedArgs &A, const ParticleSoA &S,
+                              const MoveLaunch &L, cudaStream_t stream) {
     if (semantics == SEM_HOST)
-        return by_storage<SEM_HOST>(storage, cfg, P, A, S, L, blockSize, stream);
-    return by_storage<SEM_DEVICE>(storage, cfg, P, A, S, L, blockSize, stream);
+        return by_storage<SEM_HOST>(storage, shape, cfg, P, A, S, L, stream);
+    return by_storage<SEM_DEVICE>(storage, shape, cfg, P, A, S, L, stream);
 }
 
 }  // namespace wb

@@ -86,9 +86,31 @@ __global__ void __launch_bounds__(256) move_soa_kernel(const wacomm_b200_config 
     if (L.conc && P.lastChunk) warp_count(L.conc, cell);
 }
 
-// FP32 step over the packed pair (step_fast.cuh); same state handling as move_soa_kernel.
-template <int SEM, int STORE>
-__global__ void __launch_bounds__(256) move_fast_kernel(const wacomm_b200_config cfg,
+// Launch shapes of the FP32 kernel: threads per block and the minimum resident blocks per SM the
+// register allocation must allow (WACOMM_B200 launch_shape 0..3).
+template <int SHAPE>
+struct LaunchShape;
+template <>
+struct LaunchShape<0> {
+    static constexpr int threads = 256, minBlocks = 1;
+};
+template <>
+struct LaunchShape<1> {
+    static constexpr int threads = 128, minBlocks = 3;
+};
+template <>
+struct LaunchShape<2> {
+    static constexpr int threads = 256, minBlocks = 2;
+};
+template <>
+struct LaunchShape<3> {
+    static constexpr int threads = 128, minBlocks = 5;
+};
+
+// FP32 step over the cell-column pair (step_fast.cuh); same state handling as move_soa_kernel.
+template <int SEM, int STORE, int SHAPE>
+__global__ void __launch_bounds__(LaunchShape<SHAPE>::threads, LaunchShape<SHAPE>::minBlocks)
+    move_fast_kernel(const wacomm_b200_config cfg,
                                                         const IntervalParams P,
                                                         const FastView<STORE> F, ParticleSoA S,
                                                         const MoveLaunch L) {
@@ -123,13 +145,14 @@ __global__ void __launch_bounds__(256) move_fast_kernel(const wacomm_b200_config
     if (L.conc && P.lastChunk) warp_count(L.conc, cell);
 }
 
-template <int SEM, int STORE>
+template <int SEM, int STORE, int SHAPE>
 cudaError_t launch_move_fast(const wacomm_b200_config &cfg, const IntervalParams &P,
                              const FastView<STORE> &F, const ParticleSoA &S, const MoveLaunch &L,
-                             int blockSize, cudaStream_t stream) {
+                             cudaStream_t stream) {
     if (L.count <= 0) return cudaSuccess;
-    int blocks = (L.count + blockSize - 1) / blockSize;
-    move_fast_kernel<SEM, STORE><<<blocks, blockSize, 0, stream>>>(cfg, P, F, S, L);
+    constexpr int threads = LaunchShape<SHAPE>::threads;
+    int blocks = (L.count + threads - 1) / threads;
+    move_fast_kernel<SEM, STORE, SHAPE><<<blocks, threads, 0, stream>>>(cfg, P, F, S, L);
     return cudaGetLastError();
 }
 

@@ -23,28 +23,79 @@ struct FastExtras {
 
 template <int STORE>
 struct FastView {
-    PackedView<STORE> V;
+    PackedView<STORE> V;   // node layout: wind/Stokes pair, lon/lat (drift model)
+    CellView<STORE> C;     // cell-column layout: velocity stencil and surface
     FastExtras X;
 };
 
-// Bilinear FP32 interpolation of the four surface records (h, zeta blended in time).
-template <class View>
-__device__ __forceinline__ float surface_fast(const View &V, int jI, int iI, float jF, float iF,
-                                              float a) {
-    SurfPair s1 = V.surface(jI, iI), s2 = V.surface(jI + 1, iI);
-    SurfPair s3 = V.surface(jI + 1, iI + 1), s4 = V.surface(jI, iI + 1);
+// Space-time weights of the 8 stencil values of one field: (1-a) w_c for record t0 and a w_c for
+// record t1, corners (j,i), (j+1,i), (j+1,i+1), (j,i+1).
+struct Weights8 {
+    float p1, p2, p3, p4, q1, q2, q3, q4;
+};
+
+__device__ __forceinline__ Weights8 weights8(float jF, float iF, float a) {
     float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
-    float c1 = (float)s1.h + at_f32(s1.z0, s1.z1, a);
-    float c2 = (float)s2.h + at_f32(s2.z0, s2.z1, a);
-    float c3 = (float)s3.h + at_f32(s3.z0, s3.z1, a);
-    float c4 = (float)s4.h + at_f32(s4.z0, s4.z1, a);
-    return c1 * w1 + c2 * w2 + c3 * w3 + c4 * w4;
+    float b = 1.f - a;
+    return Weights8{b * w1, b * w2, b * w3, b * w4, a * w1, a * w2, a * w3, a * w4};
 }
 
-// Leeway and Stokes velocity of a drifting object (the drift branch of advective_velocity),
-// kept out of line so the passive-particle step carries none of its registers.
+__device__ __forceinline__ float blend(const QuadPair &q, const Weights8 &w) {
+    float r = q.t0.c1 * w.p1;
+    r = fmaf(q.t0.c2, w.p2, r);
+    r = fmaf(q.t0.c3, w.p3, r);
+    r = fmaf(q.t0.c4, w.p4, r);
+    r = fmaf(q.t1.c1, w.q1, r);
+    r = fmaf(q.t1.c2, w.q2, r);
+    r = fmaf(q.t1.c3, w.q3, r);
+    return fmaf(q.t1.c4, w.q4, r);
+}
+
+// Water column height h + zeta at a fractional position of a cell (FP32).
+template <int STORE>
+__device__ __forceinline__ float column_height(const CellView<STORE> &C, int jI, int iI, float jF,
+                                               float iF, float a) {
+    CellSurface s = C.surf(jI, iI);
+    float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
+    float b = 1.f - a;
+    float r = s.h.x * w1;
+    r = fmaf(s.h.y, w2, r);
+    r = fmaf(s.h.z, w3, r);
+    r = fmaf(s.h.w, w4, r);
+    r = fmaf(s.z0.x, b * w1, r);
+    r = fmaf(s.z0.y, b * w2, r);
+    r = fmaf(s.z0.z, b * w3, r);
+    r = fmaf(s.z0.w, b * w4, r);
+    r = fmaf(s.z1.x, a * w1, r);
+    r = fmaf(s.z1.y, a * w2, r);
+    r = fmaf(s.z1.z, a * w3, r);
+    return fmaf(s.z1.w, a * w4, r);
+}
+
+// Current (u, v, w) and, when wanted, AKT at a fractional position: one stencil read.
+template <int STORE>
+__device__ __forceinline__ void current_cell(const CellView<STORE> &C, int kI, float kF, int jI,
+                                             float jF, int iI, float iF, float a, float aAkt,
+                                             bool wantAkt, float &uu, float &vv, float &ww,
+                                             float &aa) {
+    QuadPair u, v, wUp, aUp, wLo, aLo;
+    C.stencil(kI, jI, iI, u, v, wUp, aUp, wLo, aLo);
+    Weights8 w = weights8(jF, iF, a);
+    uu = blend(u, w);
+    vv = blend(v, w);
+    float up = blend(wUp, w), lo = blend(wLo, w);
+    ww = fmaf(lo - up, kF, up);
+    if (wantAkt) {
+        Weights8 wa = aAkt == a ? w : weights8(jF, iF, aAkt);
+        float au = blend(aUp, wa), al = blend(aLo, wa);
+        aa = fmaf(al - au, kF, au);
+    }
+}
+
+
+// Leeway and Stokes velocity of a drifting object (the drift branch of advective_velocity).
 template <class View>
-__device__ __noinline__ void drift_velocity(const wacomm_b200_config &cfg, const IntervalParams &P,
+__device__ __forceinline__ void drift_velocity(const wacomm_b200_config &cfg, const IntervalParams &P,
                                             const View &V, uint64_t id, int type, int side,
                                             int jI, double jF, int iI, double iF, double sa,
                                             double elapsed, double physicalTime, double stepDt,
@@ -108,42 +159,6 @@ __device__ __noinline__ void drift_velocity(const wacomm_b200_config &cfg, const
     }
 }
 
-// Ocean velocity (u, v, w) at a fractional position, FP32.
-template <class View>
-__device__ __forceinline__ void current_fast(const View &V, int kI, float kF, int jI, float jF,
-                                             int iI, float iF, float a, float &uu, float &vv,
-                                             float &ww) {
-    NodeUp c1 = V.up(kI, jI, iI), c2 = V.up(kI, jI + 1, iI);
-    NodeUp c3 = V.up(kI, jI + 1, iI + 1), c4 = V.up(kI, jI, iI + 1);
-    NodeLo l1 = V.lo(kI, jI, iI), l2 = V.lo(kI, jI + 1, iI);
-    NodeLo l3 = V.lo(kI, jI + 1, iI + 1), l4 = V.lo(kI, jI, iI + 1);
-    float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
-    uu = at_f32(c1.u0, c1.u1, a) * w1 + at_f32(c2.u0, c2.u1, a) * w2 + at_f32(c3.u0, c3.u1, a) * w3 +
-         at_f32(c4.u0, c4.u1, a) * w4;
-    vv = at_f32(c1.v0, c1.v1, a) * w1 + at_f32(c2.v0, c2.v1, a) * w2 + at_f32(c3.v0, c3.v1, a) * w3 +
-         at_f32(c4.v0, c4.v1, a) * w4;
-    float up = at_f32(c1.w0, c1.w1, a) * w1 + at_f32(c2.w0, c2.w1, a) * w2 +
-               at_f32(c3.w0, c3.w1, a) * w3 + at_f32(c4.w0, c4.w1, a) * w4;
-    float lo = at_f32(l1.w0, l1.w1, a) * w1 + at_f32(l2.w0, l2.w1, a) * w2 +
-               at_f32(l3.w0, l3.w1, a) * w3 + at_f32(l4.w0, l4.w1, a) * w4;
-    ww = up + (lo - up) * kF;
-}
-
-template <class View>
-__device__ __forceinline__ float akt_fast(const View &V, int kI, float kF, int jI, float jF, int iI,
-                                          float iF, float a) {
-    NodeUp c1 = V.up(kI, jI, iI), c2 = V.up(kI, jI + 1, iI);
-    NodeUp c3 = V.up(kI, jI + 1, iI + 1), c4 = V.up(kI, jI, iI + 1);
-    NodeLo l1 = V.lo(kI, jI, iI), l2 = V.lo(kI, jI + 1, iI);
-    NodeLo l3 = V.lo(kI, jI + 1, iI + 1), l4 = V.lo(kI, jI, iI + 1);
-    float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
-    float up = at_f32(c1.a0, c1.a1, a) * w1 + at_f32(c2.a0, c2.a1, a) * w2 +
-               at_f32(c3.a0, c3.a1, a) * w3 + at_f32(c4.a0, c4.a1, a) * w4;
-    float lo = at_f32(l1.a0, l1.a1, a) * w1 + at_f32(l2.a0, l2.a1, a) * w2 +
-               at_f32(l3.a0, l3.a1, a) * w3 + at_f32(l4.a0, l4.a1, a) * w4;
-    return up + (lo - up) * kF;
-}
-
 __device__ __forceinline__ float signf_of(float a, float b) {
     return fabsf(a) * (float)((b > 0.f) - (b < 0.f));
 }
@@ -153,6 +168,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                                   const FastView<STORE> &F, ParticleState &p, double &elapsed,
                                   int *err) {
     const PackedView<STORE> &V = F.V;
+    const CellView<STORE> &C = F.C;
     const int eta = V.g.eta, xi = V.g.xi, sW = V.g.sW;
     const double kLower = P.kLower, length = P.length;
     const double invLength = length == 0 ? 0.0 : 1.0 / length;
@@ -204,7 +220,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         const float dt = (float)stepDt;
         const float alpha = (float)((elapsed + 0.5 * stepDt) * invLength);
         const float alphaStart = (float)(elapsed * invLength);
-        const float hc = surface_fast(V, jI, iI, jF, iF, alpha);
+        const float hc = column_height(C, jI, iI, jF, iF, alpha);
         if (hc <= shore && cfg.horizontalClosure == CLOSURE_KILL) {
             p.health = -1;
             lazy = false;
@@ -215,8 +231,8 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         }
         const int kM = mem_level(kI, sW);
         const float sa = midpoint ? alphaStart : alpha;
-        float uu, vv, ww;
-        current_fast(V, kM, kF, jI, jF, iI, iF, sa, uu, vv, ww);
+        float uu, vv, ww, aa = 0.f;
+        current_cell(C, kM, kF, jI, jF, iI, iF, sa, alpha, diffuse, uu, vv, ww, aa);
         if (drift) {
             float du, dv;
             drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, (double)jF, iI, (double)iF, sa,
@@ -231,7 +247,6 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         }
         float rx = 0.f, ry = 0.f, rz = 0.f;
         if (diffuse) {
-            float aa = akt_fast(V, kM, kF, jI, jF, iI, iF, alpha);
             float sigmaDepth = (float)(cfg.sigma * (1 - p.k / kLower));
             float scale = sqrtf(dt / (float)cfg.dti);
             float n0, n1, n2;
@@ -263,7 +278,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
             if (midValid) {
                 iMF = (float)(iMid - fim);
                 jMF = (float)(jMid - fjm);
-                hcMid = surface_fast(V, jMI, iMI, jMF, iMF, alpha);
+                hcMid = column_height(C, jMI, iMI, jMF, iMF, alpha);
                 midValid = hcMid > shore && hcMid > 0.f;
             }
             float detZ;
@@ -271,8 +286,8 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 double kmc = ceil(kMid);
                 int kMI = mem_level(to_index<SEM>(kmc), sW);
                 float kMF = (float)(kmc - kMid);
-                float um, vm, wm;
-                current_fast(V, kMI, kMF, jMI, jMF, iMI, iMF, alpha, um, vm, wm);
+                float um, vm, wm, unused;
+                current_cell(C, kMI, kMF, jMI, jMF, iMI, iMF, alpha, alpha, false, um, vm, wm, unused);
                 if (drift) {
                     float du, dv;
                     drift_velocity(cfg, P, V, p.id, p.type, p.side, jMI, (double)jMF, iMI,
@@ -286,8 +301,8 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 dJ = dirf * vm * dt * im.y;
                 detZ = dirf * (sv + wm) * dt * zdist / zdistMid;
             } else {
-                float ue, ve, we;
-                current_fast(V, kM, kF, jI, jF, iI, iF, alpha, ue, ve, we);
+                float ue, ve, we, unused;
+                current_cell(C, kM, kF, jI, jF, iI, iF, alpha, alpha, false, ue, ve, we, unused);
                 if (drift) {
                     float du, dv;
                     drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, (double)jF, iI,
@@ -317,7 +332,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         double fjd = floor(jdet), fid = floor(idet);
         int jdetI = to_index<SEM>(fjd), idetI = to_index<SEM>(fid);
         if (valid_cell(jdetI, idetI, eta, xi)) {
-            float hcdet = surface_fast(V, jdetI, idetI, (float)(jdet - fjd), (float)(idet - fid), alpha);
+            float hcdet = column_height(C, jdetI, idetI, (float)(jdet - fjd), (float)(idet - fid), alpha);
             if (hcdet <= shore) {
                 if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
                     idet = p.i;

@@ -115,6 +115,134 @@ cudaError_t pack_pair(int storage, int eta, int xi, int sW, const FrameDevice &f
     return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------ cell-column packing
+
+size_t cell_record_bytes(int storage) {
+    return 2 * (storage == STORE_F32 ? sizeof(CellQuad<STORE_F32>) : sizeof(CellQuad<STORE_F16>));
+}
+size_t cell_surface_bytes() { return sizeof(CellSurface); }
+
+template <int STORE>
+__device__ __forceinline__ void store_quad(CellQuad<STORE> *dst, const float (&a0)[4],
+                                           const float (&a1)[4], const float (&b0)[4],
+                                           const float (&b1)[4]);
+template <>
+__device__ __forceinline__ void store_quad<STORE_F32>(CellQuad<STORE_F32> *dst, const float (&a0)[4],
+                                                      const float (&a1)[4], const float (&b0)[4],
+                                                      const float (&b1)[4]) {
+    dst->a0 = make_float4(a0[0], a0[1], a0[2], a0[3]);
+    dst->a1 = make_float4(a1[0], a1[1], a1[2], a1[3]);
+    dst->b0 = make_float4(b0[0], b0[1], b0[2], b0[3]);
+    dst->b1 = make_float4(b1[0], b1[1], b1[2], b1[3]);
+}
+template <>
+__device__ __forceinline__ void store_quad<STORE_F16>(CellQuad<STORE_F16> *dst, const float (&a0)[4],
+                                                      const float (&a1)[4], const float (&b0)[4],
+                                                      const float (&b1)[4]) {
+    CellQuad<STORE_F16> r;
+    r.a0[0] = __floats2half2_rn(a0[0], a0[1]);
+    r.a0[1] = __floats2half2_rn(a0[2], a0[3]);
+    r.a1[0] = __floats2half2_rn(a1[0], a1[1]);
+    r.a1[1] = __floats2half2_rn(a1[2], a1[3]);
+    r.b0[0] = __floats2half2_rn(b0[0], b0[1]);
+    r.b0[1] = __floats2half2_rn(b0[2], b0[3]);
+    r.b1[0] = __floats2half2_rn(b1[0], b1[1]);
+    r.b1[1] = __floats2half2_rn(b1[2], b1[3]);
+    *dst = r;
+}
+template <>
+__device__ __forceinline__ void store_quad<STORE_BF16>(CellQuad<STORE_BF16> *dst, const float (&a0)[4],
+                                                       const float (&a1)[4], const float (&b0)[4],
+                                                       const float (&b1)[4]) {
+    CellQuad<STORE_BF16> r;
+    r.a0[0] = __floats2bfloat162_rn(a0[0], a0[1]);
+    r.a0[1] = __floats2bfloat162_rn(a0[2], a0[3]);
+    r.a1[0] = __floats2bfloat162_rn(a1[0], a1[1]);
+    r.a1[1] = __floats2bfloat162_rn(a1[2], a1[3]);
+    r.b0[0] = __floats2bfloat162_rn(b0[0], b0[1]);
+    r.b0[1] = __floats2bfloat162_rn(b0[2], b0[3]);
+    r.b1[0] = __floats2bfloat162_rn(b1[0], b1[1]);
+    r.b1[1] = __floats2bfloat162_rn(b1[2], b1[3]);
+    *dst = r;
+}
+
+// One thread per (W level L, cell): writes A(L) and B(L) of the cell (views.cuh). Cells on the
+// last row or column (never valid) are zero.
+template <int STORE>
+__global__ void pack_cells_kernel(int eta, int xi, int sW, FrameDevice f0, FrameDevice f1,
+                                  CellQuad<STORE> *cells) {
+    size_t plane = (size_t)eta * xi, total = plane * sW;
+    for (size_t n = blockIdx.x * (size_t)blockDim.x + threadIdx.x; n < total;
+         n += (size_t)gridDim.x * blockDim.x) {
+        size_t L = n / plane, cell = n - L * plane;
+        int j = (int)(cell / xi), i = (int)(cell - (size_t)j * xi);
+        float u0[4] = {0, 0, 0, 0}, u1[4] = {0, 0, 0, 0}, v0[4] = {0, 0, 0, 0}, v1[4] = {0, 0, 0, 0};
+        float w0[4] = {0, 0, 0, 0}, w1[4] = {0, 0, 0, 0}, a0[4] = {0, 0, 0, 0}, a1[4] = {0, 0, 0, 0};
+        if (j + 1 < eta && i + 1 < xi) {
+            const size_t corner[4] = {cell, cell + xi, cell + xi + 1, cell + 1};
+            for (int c = 0; c < 4; c++) {
+                size_t q = L * plane + corner[c];
+                w0[c] = f0.w[q];
+                w1[c] = f1.w[q];
+                a0[c] = f0.akt[q];
+                a1[c] = f1.akt[q];
+                if (L > 0) {
+                    size_t r = (L - 1) * plane + corner[c];
+                    u0[c] = f0.u[r];
+                    u1[c] = f1.u[r];
+                    v0[c] = f0.v[r];
+                    v1[c] = f1.v[r];
+                }
+            }
+        }
+        CellQuad<STORE> *dst = cells + (cell * sW + L) * 2;
+        store_quad<STORE>(dst, u0, u1, v0, v1);
+        store_quad<STORE>(dst + 1, w0, w1, a0, a1);
+    }
+}
+
+__global__ void pack_cell_surface_kernel(int eta, int xi, FrameDevice f0, FrameDevice f1,
+                                         const double *h, CellSurface *out) {
+    size_t plane = (size_t)eta * xi;
+    for (size_t cell = blockIdx.x * (size_t)blockDim.x + threadIdx.x; cell < plane;
+         cell += (size_t)gridDim.x * blockDim.x) {
+        int j = (int)(cell / xi), i = (int)(cell - (size_t)j * xi);
+        CellSurface s;
+        if (j + 1 < eta && i + 1 < xi) {
+            size_t c1 = cell, c2 = cell + xi, c3 = cell + xi + 1, c4 = cell + 1;
+            s.h = make_float4((float)h[c1], (float)h[c2], (float)h[c3], (float)h[c4]);
+            s.z0 = make_float4(f0.zeta[c1], f0.zeta[c2], f0.zeta[c3], f0.zeta[c4]);
+            s.z1 = make_float4(f1.zeta[c1], f1.zeta[c2], f1.zeta[c3], f1.zeta[c4]);
+        } else {
+            s.h = s.z0 = s.z1 = make_float4(0, 0, 0, 0);
+        }
+        out[cell] = s;
+    }
+}
+
+cudaError_t pack_cells(int storage, int eta, int xi, int sW, const FrameDevice &f0,
+                       const FrameDevice &f1, const double *h, void *cells, void *cellSurface,
+                       cudaStream_t stream) {
+    size_t total = (size_t)eta * xi * sW;
+    int blocks = grid_for(total, 256);
+    switch (storage) {
+        case STORE_F16:
+            pack_cells_kernel<STORE_F16><<<blocks, 256, 0, stream>>>(
+                eta, xi, sW, f0, f1, static_cast<CellQuad<STORE_F16> *>(cells));
+            break;
+        case STORE_BF16:
+            pack_cells_kernel<STORE_BF16><<<blocks, 256, 0, stream>>>(
+                eta, xi, sW, f0, f1, static_cast<CellQuad<STORE_BF16> *>(cells));
+            break;
+        default:
+            pack_cells_kernel<STORE_F32><<<blocks, 256, 0, stream>>>(
+                eta, xi, sW, f0, f1, static_cast<CellQuad<STORE_F32> *>(cells));
+    }
+    pack_cell_surface_kernel<<<grid_for((size_t)eta * xi, 256), 256, 0, stream>>>(
+        eta, xi, f0, f1, h, static_cast<CellSurface *>(cellSurface));
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ cell metric
 
 // Cell sizes in metres along j (ydist) and i (xdist). Host rules: haversine along one grid axis

@@ -148,6 +148,112 @@ struct PackedView {
     }
 };
 
+// ------------------------------------------------------------------ cell-column layout
+// FP32 step layout. For every cell (j, i) and W level L the bracketing pair is stored at the
+// four corners of the cell, corner order (j,i), (j+1,i), (j+1,i+1), (j,i+1):
+//     A(L) = u, v of rho level L-1        B(L) = w, akt of W level L
+// each as {field0 @ t0, field0 @ t1, field1 @ t0, field1 @ t1} x 4 corners, and the records of a
+// cell are consecutive in L: ... A(L-1) B(L-1) A(L) B(L) ... so the stencil of a particle at
+// level kI (L = kI + sW - 1) is the contiguous run B(L-1), A(L), B(L) read from one address.
+// Surface per cell: h at the corners, zeta at t0 and t1 at the corners.
+
+template <int STORE>
+struct CellQuad;  // one field pair at 4 corners x 2 records
+template <>
+struct alignas(16) CellQuad<STORE_F32> {
+    float4 a0, a1, b0, b1;  // field a @t0 corners, a @t1, field b @t0, b @t1
+};
+template <>
+struct alignas(16) CellQuad<STORE_F16> {
+    __half2 a0[2], a1[2], b0[2], b1[2];
+};
+template <>
+struct alignas(16) CellQuad<STORE_BF16> {
+    __nv_bfloat162 a0[2], a1[2], b0[2], b1[2];
+};
+
+struct Quad {
+    float c1, c2, c3, c4;
+};
+struct QuadPair {  // a field at 4 corners for the two bracketing records
+    Quad t0, t1;
+};
+
+__device__ __forceinline__ Quad quad_of(float4 v) { return Quad{v.x, v.y, v.z, v.w}; }
+
+template <int STORE>
+__device__ __forceinline__ void load_quad(const CellQuad<STORE> *p, QuadPair &a, QuadPair &b);
+
+template <>
+__device__ __forceinline__ void load_quad<STORE_F32>(const CellQuad<STORE_F32> *p, QuadPair &a,
+                                                     QuadPair &b) {
+    const float4 *q = reinterpret_cast<const float4 *>(p);
+    a.t0 = quad_of(__ldg(q));
+    a.t1 = quad_of(__ldg(q + 1));
+    b.t0 = quad_of(__ldg(q + 2));
+    b.t1 = quad_of(__ldg(q + 3));
+}
+
+__device__ __forceinline__ Quad quad_h(uint32_t x, uint32_t y) {
+    float2 lo = __half22float2(*reinterpret_cast<__half2 *>(&x));
+    float2 hi = __half22float2(*reinterpret_cast<__half2 *>(&y));
+    return Quad{lo.x, lo.y, hi.x, hi.y};
+}
+__device__ __forceinline__ Quad quad_bf(uint32_t x, uint32_t y) {
+    float2 lo = __bfloat1622float2(*reinterpret_cast<__nv_bfloat162 *>(&x));
+    float2 hi = __bfloat1622float2(*reinterpret_cast<__nv_bfloat162 *>(&y));
+    return Quad{lo.x, lo.y, hi.x, hi.y};
+}
+
+template <>
+__device__ __forceinline__ void load_quad<STORE_F16>(const CellQuad<STORE_F16> *p, QuadPair &a,
+                                                     QuadPair &b) {
+    const uint4 *q = reinterpret_cast<const uint4 *>(p);
+    uint4 x = __ldg(q), y = __ldg(q + 1);
+    a.t0 = quad_h(x.x, x.y);
+    a.t1 = quad_h(x.z, x.w);
+    b.t0 = quad_h(y.x, y.y);
+    b.t1 = quad_h(y.z, y.w);
+}
+
+template <>
+__device__ __forceinline__ void load_quad<STORE_BF16>(const CellQuad<STORE_BF16> *p, QuadPair &a,
+                                                      QuadPair &b) {
+    const uint4 *q = reinterpret_cast<const uint4 *>(p);
+    uint4 x = __ldg(q), y = __ldg(q + 1);
+    a.t0 = quad_bf(x.x, x.y);
+    a.t1 = quad_bf(x.z, x.w);
+    b.t0 = quad_bf(y.x, y.y);
+    b.t1 = quad_bf(y.z, y.w);
+}
+
+struct CellSurface {  // FP32: h, zeta@t0, zeta@t1 at the 4 corners
+    float4 h, z0, z1;
+};
+
+template <int STORE>
+struct CellView {
+    int eta, xi, sW;
+    const CellQuad<STORE> *columns;   // [cell][sW][2] (A, B)
+    const CellSurface *surface;       // [cell]
+
+    // Velocity stencil of level kI (valid memory level) in cell (j, i): u, v at rho level kI;
+    // w, akt at W levels kI (up) and kI-1 (lo).
+    __device__ __forceinline__ void stencil(int kI, int j, int i, QuadPair &u, QuadPair &v,
+                                            QuadPair &wUp, QuadPair &aUp, QuadPair &wLo,
+                                            QuadPair &aLo) const {
+        size_t L = (size_t)(kI + sW - 1);
+        const CellQuad<STORE> *col = columns + (((size_t)j * xi + i) * sW + L) * 2;
+        load_quad<STORE>(col - 1, wLo, aLo);  // B(L-1)
+        load_quad<STORE>(col, u, v);          // A(L)
+        load_quad<STORE>(col + 1, wUp, aUp);  // B(L)
+    }
+    __device__ __forceinline__ CellSurface surf(int j, int i) const {
+        const float4 *q = reinterpret_cast<const float4 *>(surface + ((size_t)j * xi + i));
+        return CellSurface{__ldg(q), __ldg(q + 1), __ldg(q + 2)};
+    }
+};
+
 // Reference device layout (kernel.cu:63-69), whole window, records t0/t1 given per interval.
 struct RawView {
     GridShape g;
