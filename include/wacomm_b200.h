@@ -124,7 +124,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx);
 const char *wacomm_b200_last_error(const wacomm_b200_context *ctx);
 
 /* Fills *out with the defaults: host semantics, FP32 arithmetic and storage, reference RNG,
- * 256 threads, one launch per interval, cell sort on, fused concentration on, launch shape 1. */
+ * 256 threads, one launch per interval, cell sort on, fused concentration on, launch shape 2. */
 int wacomm_b200_default_options(wacomm_b200_options *out);
 int wacomm_b200_set_options(wacomm_b200_context *ctx, const wacomm_b200_options *options);
 int wacomm_b200_get_options(const wacomm_b200_context *ctx, wacomm_b200_options *out);

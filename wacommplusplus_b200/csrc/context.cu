@@ -467,7 +467,7 @@ int wacomm_b200_default_options(wacomm_b200_options *out) {
     out->substeps_per_launch = 0;
     out->sort_by_cell = 1;
     out->fuse_concentration = 1;
-    out->launch_shape = 1;
+    out->launch_shape = 2;
     return WACOMM_B200_OK;
 }
 
