@@ -218,6 +218,31 @@ int wacomm_b200_cuda_move_particle(const wacomm_b200_config *config_device,
                                    const float *stokes_v, int particle_count, int num_thread,
                                    int num_gpu, void *stream);
 
+/* No counterpart in the reference. The launcher above for callers that may not allocate device
+ * memory: cudaFree synchronizes the whole device (and cudaMalloc may), stalling every other
+ * stream a multi-stream or multi-GPU driver keeps in flight, and some host frameworks own all
+ * device memory through their own pool. Same arguments, meaning and results as
+ * wacomm_b200_cuda_move_particle; it also orders the work by horizontal cell, and its working
+ * memory (keys, histogram, scan, order) is a fixed array of about 25 MB compiled into the library
+ * and held on every GPU that loads it. Limits: particle_count <= 2,097,152 and eta*xi <=
+ * 1,048,576; larger calls return -WACOMM_B200_ERR_CAPACITY and do nothing. Otherwise returns 0 or
+ * a CUDA error code. Every call on a device shares the array: calls that overlap on the GPU race
+ * and must not be issued; calls on one stream are ordered and safe. The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress, with that device current); make it
+ * before any stream capture begins. */
+int wacomm_b200_cuda_move_particle_noalloc(const wacomm_b200_config *config_device,
+                                           wacomm_b200_particle *particles_device, int time_index,
+                                           int ocean_time, int s_w, int s_rho, int eta, int xi,
+                                           const double *times, const double *mask,
+                                           const double *lon_rad, const double *lat_rad,
+                                           const double *depth_intervals, const double *h,
+                                           const float *zeta, const float *u, const float *v,
+                                           const float *w, const float *akt,
+                                           const float *wind_u10, const float *wind_v10,
+                                           const float *stokes_u, const float *stokes_v,
+                                           int particle_count, int num_thread, int num_gpu,
+                                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,8 @@ SIGNATURES = {
     "wacomm_b200_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
     "wacomm_b200_cuda_move_particle": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i] + [_vp] * 15 +
                                        [_i, _i, _i, _vp]),
+    "wacomm_b200_cuda_move_particle_noalloc": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i] +
+                                               [_vp] * 15 + [_i, _i, _i, _vp]),
 }
 
 _lib = None
