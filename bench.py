@@ -272,7 +272,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": None if traffic_per_step is None else traffic_per_step * per_launch_steps,
-                "kernel": "move_soa_kernel (fp32 interpolation)", "kernel_ms": kernel_ms,
+                "kernel": "move_fast_kernel (FP32 step)" if args.arithmetic == "fp32" else "move_soa_kernel (reference arithmetic)", "kernel_ms": kernel_ms,
                 "algorithmic_bytes_per_particle_step": B_ALG}
 
     e2e = None
