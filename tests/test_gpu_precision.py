@@ -112,3 +112,24 @@ def test_diffusion_ensemble_moments(cuda_device, rng):
         assert abs(z.var() - 1.0) < 0.02
         assert abs(np.mean(z ** 4) - 3.0) < 0.1
     assert abs(np.corrcoef(x, y)[0, 1]) < 0.01
+
+
+@pytest.mark.parametrize("case_name", ["drift_i1", "drift_i2", "realistic_i2_c123"])
+def test_fp32_step_on_reference_fixture_cases(cuda_device, case_name):
+    """The FP32 step (drift model, diffusion with the reference draws, land and closures) over
+    the fixture cases, two intervals, against the FP64 oracle."""
+    from helpers import load_move_cases
+    case = {c["name"]: c for c in load_move_cases()}[case_name]
+    cfg = default_config(**case["overrides"])
+    win = case["window"]
+    want = _oracle(win, cfg, case["start"], range(2))
+    with Engine(cuda_device, arithmetic="fp32") as e:
+        got = _run(e, win, cfg, case["start"], range(2))
+    assert np.array_equal(got["driftSide"], want["driftSide"])
+    both = (got["health"] > 0) & (want["health"] > 0)
+    flips = int(np.sum((got["health"] > 0) != (want["health"] > 0)))
+    err = great_circle_m(win.lon, win.lat, got[both], want[both])
+    print(f"{case_name}: mean {err.mean():.3g} m p99 {np.percentile(err, 99):.3g} m "
+          f"max {err.max():.3g} m flips {flips}")
+    assert flips <= max(2, len(got) // 100)
+    assert err.mean() <= 0.1 and np.percentile(err, 99) <= 1.0

@@ -42,6 +42,7 @@ struct wacomm_b200_context {
     std::string error;
     wacomm_b200_options opt{};
     wacomm_b200_config cfg{};
+    wacomm_b200_config *dCfg = nullptr;  // device copy (drift branch of the FP32 step)
     bool hasConfig = false;
 
     int eta = 0, xi = 0, sRho = 0, sW = 0;
@@ -337,6 +338,7 @@ PackedArgs packed_args(wacomm_b200_context *ctx) {
     A.metric = ctx->dMetric;
     A.invMetric = ctx->dInvMetric;
     A.depthIntervalsF = ctx->dDepthF;
+    A.cfgDevice = ctx->dCfg;
     A.cells = ctx->dCells;
     A.cellSurface = ctx->dCellSurface;
     return A;
@@ -531,6 +533,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dConc);
     cudaFree(ctx->dSteps);
     cudaFree(ctx->dErr);
+    cudaFree(ctx->dCfg);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->evMove0) cudaEventDestroy(ctx->evMove0);
@@ -567,6 +570,11 @@ int wacomm_b200_set_config(wacomm_b200_context *ctx, const wacomm_b200_config *c
     if (!(config->dti > 0)) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "dti must be > 0");
     if (config->observationalCalibrationRegionCount > 16)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "more than 16 calibration regions");
+    cudaSetDevice(ctx->device);
+    if (!ctx->dCfg) CUDA_TRY(ctx, cudaMalloc(&ctx->dCfg, sizeof(wacomm_b200_config)));
+    // kernels of earlier intervals may still read the previous copy
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpy(ctx->dCfg, config, sizeof(wacomm_b200_config), cudaMemcpyHostToDevice));
     ctx->cfg = *config;
     ctx->hasConfig = true;
     return WACOMM_B200_OK;

@@ -25,6 +25,7 @@ struct PackedArgs {
     const double2 *metric;
     const float2 *invMetric;           // {1/xdist, 1/ydist} per cell (FP32 step)
     const float *depthIntervalsF;      // FP32 copy of depthIntervals (FP32 step)
+    const wacomm_b200_config *cfgDevice;  // device copy of the run parameters (FP32 step, drift)
     const void *cells;                 // CellQuad<storage>[eta*xi][sW][2] (FP32 step)
     const void *cellSurface;           // CellSurface[eta*xi] (FP32 step)
 };

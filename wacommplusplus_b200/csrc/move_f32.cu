@@ -28,6 +28,7 @@ static FastView<STORE> fast_view(const PackedArgs &A) {
     F.V = typed_view<STORE>(A);
     F.X.invMetric = A.invMetric;
     F.X.depthIntervals = A.depthIntervalsF;
+    F.X.cfgDevice = A.cfgDevice;
     F.C.eta = A.eta;
     F.C.xi = A.xi;
     F.C.sW = A.sW;

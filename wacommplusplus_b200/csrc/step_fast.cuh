@@ -19,6 +19,7 @@ namespace wb {
 struct FastExtras {
     const float2 *invMetric;     // [eta][xi] {1/xdist, 1/ydist}
     const float *depthIntervals; // [sW-1]
+    const wacomm_b200_config *cfgDevice;  // device copy of the run parameters
 };
 
 template <int STORE>
@@ -40,15 +41,16 @@ __device__ __forceinline__ Weights8 weights8(float jF, float iF, float a) {
     return Weights8{b * w1, b * w2, b * w3, b * w4, a * w1, a * w2, a * w3, a * w4};
 }
 
+// Two independent FMA chains (record t0, record t1) keep the dependency depth at four.
 __device__ __forceinline__ float blend(const QuadPair &q, const Weights8 &w) {
-    float r = q.t0.c1 * w.p1;
-    r = fmaf(q.t0.c2, w.p2, r);
-    r = fmaf(q.t0.c3, w.p3, r);
-    r = fmaf(q.t0.c4, w.p4, r);
-    r = fmaf(q.t1.c1, w.q1, r);
-    r = fmaf(q.t1.c2, w.q2, r);
-    r = fmaf(q.t1.c3, w.q3, r);
-    return fmaf(q.t1.c4, w.q4, r);
+    float x = q.t0.c1 * w.p1, y = q.t1.c1 * w.q1;
+    x = fmaf(q.t0.c2, w.p2, x);
+    y = fmaf(q.t1.c2, w.q2, y);
+    x = fmaf(q.t0.c3, w.p3, x);
+    y = fmaf(q.t1.c3, w.q3, y);
+    x = fmaf(q.t0.c4, w.p4, x);
+    y = fmaf(q.t1.c4, w.q4, y);
+    return x + y;
 }
 
 // Water column height h + zeta at a fractional position of a cell (FP32).
@@ -57,19 +59,17 @@ __device__ __forceinline__ float column_height(const CellView<STORE> &C, int jI,
                                                float iF, float a) {
     CellSurface s = C.surf(jI, iI);
     float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
-    float b = 1.f - a;
-    float r = s.h.x * w1;
-    r = fmaf(s.h.y, w2, r);
-    r = fmaf(s.h.z, w3, r);
-    r = fmaf(s.h.w, w4, r);
-    r = fmaf(s.z0.x, b * w1, r);
-    r = fmaf(s.z0.y, b * w2, r);
-    r = fmaf(s.z0.z, b * w3, r);
-    r = fmaf(s.z0.w, b * w4, r);
-    r = fmaf(s.z1.x, a * w1, r);
-    r = fmaf(s.z1.y, a * w2, r);
-    r = fmaf(s.z1.z, a * w3, r);
-    return fmaf(s.z1.w, a * w4, r);
+    float h = s.h.x * w1, z0 = s.z0.x * w1, z1 = s.z1.x * w1;
+    h = fmaf(s.h.y, w2, h);
+    z0 = fmaf(s.z0.y, w2, z0);
+    z1 = fmaf(s.z1.y, w2, z1);
+    h = fmaf(s.h.z, w3, h);
+    z0 = fmaf(s.z0.z, w3, z0);
+    z1 = fmaf(s.z1.z, w3, z1);
+    h = fmaf(s.h.w, w4, h);
+    z0 = fmaf(s.z0.w, w4, z0);
+    z1 = fmaf(s.z1.w, w4, z1);
+    return h + at_f32(z0, z1, a);
 }
 
 // Current (u, v, w) and, when wanted, AKT at a fractional position: one stencil read.
