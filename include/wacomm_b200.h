@@ -13,9 +13,10 @@
  *   - the per-interval device staging of Wacomm::run           Wacomm.cpp:386-610
  *   - dead-particle removal                                     Wacomm.cpp:711-713
  *   - Concentration::evaluate(...) and the land mask            Concentration.hpp:16-44, Wacomm.cpp:722-739
- *   - sourceEmissionTimes / Source::emit / Sources::emit        SourceEmission.hpp:38-79, Source.cpp:25-45,
- *                                                               Sources.cpp:233-249
+ *   - sourceEmissionTimes / Source::emit / Sources::emit        SourceEmission.hpp:38-79, Source.cpp:16-45,
+ *                                                               Sources.cpp:233-249 (wacomm_b200_emit)
  *   - OceanModelAdapter::kji2deplatlon                          OceanModelAdapter.cpp:271-327
+ *                                                               (wacomm_b200_geo_positions)
  * The drop-in C++ launcher with the reference's exact signature is declared in
  * include/wacomm_b200_kernel.h.
  */
@@ -80,6 +81,21 @@ typedef struct wacomm_b200_config {
     WACOMM_B200_BOOL hasWind;
     double windU10, windV10;
 } wacomm_b200_config;
+
+/* A release point (the fields of Source, Source.hpp:19-60). k, j, i are grid indices; start and
+ * end are days as the reference stores them (start < 0: the run start; end < 0: no end); mode is
+ * the source's own mode field, and only mode 1 emits (Source.cpp:18). */
+#define WACOMM_B200_EMISSION_UNIFORM_RATE 0           /* emission_value particles per hour */
+#define WACOMM_B200_EMISSION_FORCING_INTERVAL_BATCH 1 /* emission_value particles per record */
+#define WACOMM_B200_EMISSION_SINGLE_PULSE 2           /* emission_value particles once, at start */
+
+typedef struct wacomm_b200_source {
+    double k, j, i;
+    double start, end;
+    double emission_value;
+    int32_t emission_mode; /* WACOMM_B200_EMISSION_* */
+    int32_t mode;
+} wacomm_b200_source;
 
 /* ------------------------------------------------------------------ engine options */
 
@@ -175,6 +191,33 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
 
 /* Stable removal of records with health <= 0 (Wacomm.cpp:711-713). */
 int wacomm_b200_remove_dead(wacomm_b200_context *ctx);
+
+/* Emission of one interval on the device (Sources::emit, Sources.cpp:233-249): the release times
+ * of every source in [interval_start, interval_end) seconds (sourceEmissionTimes,
+ * SourceEmission.hpp:38-79, with source times start*86400 s, or julian_start*86400 s when start
+ * < 0), merged across sources in time order with ties kept in source order, are appended to the
+ * resident records in that order. Ids continue from the last resident record's id + 1 (0 when
+ * none); positions take the seeded 0.25 N(0,1) index offsets when randomSources is set; type and
+ * side follow the run parameters, the side drawn per id when leewayRandomSide is set
+ * (Source.cpp:25-45). An invalid schedule (a non-finite or negative value, an empty interval, a
+ * fractional count for the batch modes) returns WACOMM_B200_ERR_ARGUMENT and appends nothing.
+ * *emitted (may be NULL) receives the number appended. Requires set_config. */
+int wacomm_b200_emit(wacomm_b200_context *ctx, const wacomm_b200_source *sources, int n_sources,
+                     double julian_start, double interval_start, double interval_end,
+                     size_t *emitted);
+
+/* The output grid of kji2deplatlon (OceanModelAdapter.hpp:20-34): lon and lat [eta][xi] (degrees
+ * in the reference) and the s_w coordinate values (s_w entries, level 0 at the bottom), on the
+ * grid of the last set_grid. */
+int wacomm_b200_set_geo_grid(wacomm_b200_context *ctx, const double *lon, const double *lat,
+                             const double *s_w_values);
+
+/* Geographic position of every resident record (OceanModelAdapter::kji2deplatlon,
+ * OceanModelAdapter.cpp:271-327) into host arrays of capacity n: depth in metres (negative
+ * down) and lat/lon interpolated from the set_geo_grid arrays; 1e37 in all three for a record
+ * outside the grid or its valid levels. Requires set_grid and set_geo_grid. */
+int wacomm_b200_geo_positions(wacomm_b200_context *ctx, double *depth, double *lat, double *lon,
+                              size_t n);
 
 /* Concentration grid of n_conc_times records [n_conc_times][s_rho][eta][xi] as uint32 counts.
  * reset zeroes it; count adds the resident alive particles at conc_time_index

@@ -12,7 +12,7 @@ import os
 
 import numpy as np
 
-from wacommplusplus_b200.types import PARTICLE_DTYPE, config_data
+from wacommplusplus_b200.types import PARTICLE_DTYPE, SOURCE_DTYPE, config_data
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
@@ -114,6 +114,9 @@ def oracle_lib():
                                                  ctypes.c_long]
         lib.wo_source_position_offset.restype = d
         lib.wo_source_position_offset.argtypes = [u64, u64, u64]
+        lib.wo_sources_emit.restype = ctypes.c_long
+        lib.wo_sources_emit.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, d, d, d,
+                                        u64, ctypes.c_void_p, ctypes.c_long]
         geo = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _c_double_p, _c_double_p, _c_double_p,
                _c_double_p, d, d, d, _c_double_p, _c_double_p, _c_double_p]
         lib.wo_kji2deplatlon.restype = ctypes.c_int
@@ -233,6 +236,21 @@ def emission_times(lib_kind, mode, value, source_start, source_end, interval_sta
     if count < 0:
         return None
     return out[:min(count, cap)].copy()
+
+
+def sources_emit(config, sources, julian_start, interval_start, interval_end, first_id):
+    """Sources::emit restated by the oracle: the new records (PARTICLE_DTYPE) in emission order,
+    or None on an invalid schedule."""
+    src = np.ascontiguousarray(sources, dtype=SOURCE_DTYPE)
+    lib = oracle_lib()
+    count = lib.wo_sources_emit(ctypes.addressof(config), src.ctypes.data, len(src), julian_start,
+                                interval_start, interval_end, first_id, None, 0)
+    if count < 0:
+        return None
+    out = np.zeros(count, dtype=PARTICLE_DTYPE)
+    lib.wo_sources_emit(ctypes.addressof(config), src.ctypes.data, len(src), julian_start,
+                        interval_start, interval_end, first_id, out.ctypes.data, count)
+    return out
 
 
 def kji2deplatlon(grid, k, j, i):

@@ -810,6 +810,84 @@ double wo_source_position_offset(uint64_t seed, uint64_t particle, uint64_t comp
     return 0.25 * wo_normal(seed, particle, WO_SOURCE_INTERVAL, 0, component);
 }
 
+/* Sources::emit (Sources.cpp:233-249): (time, source) pairs in source-major order, stably sorted
+ * by time; each becomes a record through Source::emit (Source.cpp:25-45). */
+typedef struct wo_release {
+    double time;
+    long order; /* position in the source-major list: the stable tie-break */
+    int source;
+} wo_release;
+
+static int release_cmp(const void *a, const void *b) {
+    const wo_release *x = (const wo_release *)a, *y = (const wo_release *)b;
+    if (x->time < y->time) return -1;
+    if (y->time < x->time) return 1;
+    return (x->order > y->order) - (x->order < y->order);
+}
+
+long wo_sources_emit(const wo_config *config, const wo_source *sources, int n_sources,
+                     double julian_start, double interval_start, double interval_end,
+                     uint64_t first_id, wo_particle *out, long cap) {
+    long total = 0;
+    for (int s = 0; s < n_sources; s++) {
+        const wo_source *src = &sources[s];
+        if (src->mode != 1) continue; /* Source.cpp:18 */
+        double start = src->start < 0 ? julian_start * 86400.0 : src->start * 86400.0;
+        double end = src->end < 0 ? -1 : src->end * 86400.0;
+        long c = wo_source_emission_times(src->emission_mode, src->emission_value, start, end,
+                                          interval_start, interval_end, NULL, 0);
+        if (c < 0) return -1;
+        total += c;
+    }
+    wo_release *list = (wo_release *)malloc((size_t)(total > 0 ? total : 1) * sizeof(wo_release));
+    double *times = NULL;
+    long at = 0;
+    for (int s = 0; s < n_sources; s++) {
+        const wo_source *src = &sources[s];
+        if (src->mode != 1) continue;
+        double start = src->start < 0 ? julian_start * 86400.0 : src->start * 86400.0;
+        double end = src->end < 0 ? -1 : src->end * 86400.0;
+        long c = wo_source_emission_times(src->emission_mode, src->emission_value, start, end,
+                                          interval_start, interval_end, NULL, 0);
+        times = (double *)realloc(times, (size_t)(c > 0 ? c : 1) * sizeof(double));
+        wo_source_emission_times(src->emission_mode, src->emission_value, start, end,
+                                 interval_start, interval_end, times, c);
+        for (long n = 0; n < c; n++, at++) {
+            list[at].time = times[n];
+            list[at].order = at;
+            list[at].source = s;
+        }
+    }
+    free(times);
+    qsort(list, (size_t)total, sizeof(wo_release), release_cmp);
+    for (long r = 0; r < total && r < cap; r++) {
+        const wo_source *src = &sources[list[r].source];
+        uint64_t id = first_id + (uint64_t)r;
+        wo_particle p;
+        memset(&p, 0, sizeof p);
+        p.id = id;
+        p.k = src->k;
+        p.j = src->j;
+        p.i = src->i;
+        if (config->randomSources) {
+            p.k = src->k + wo_source_position_offset(config->randomSeed, id, 0);
+            p.j = src->j + wo_source_position_offset(config->randomSeed, id, 1);
+            p.i = src->i + wo_source_position_offset(config->randomSeed, id, 2);
+        }
+        p.health = 1.0; /* Particle.cpp:30-44 */
+        p.age = 0.0;
+        p.time = list[r].time;
+        p.driftObjectType = config->driftObjectType;
+        p.driftSide = config->driftSide;
+        if (config->leewayRandomSide)
+            p.driftSide = (int8_t)wo_sample_drift_side(config->randomSeed, id,
+                                                       config->leewayRightSideProbability);
+        out[r] = p;
+    }
+    free(list);
+    return total;
+}
+
 /* ---------------------------------------------------------------- kji <-> geo */
 
 int wo_kji2deplatlon(int eta, int xi, int sW, const double *lon, const double *lat,

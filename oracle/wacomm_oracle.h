@@ -117,6 +117,23 @@ long wo_source_emission_times(int mode, double value, double sourceStart, double
                               double intervalStart, double intervalEnd, double *out, long cap);
 double wo_source_position_offset(uint64_t seed, uint64_t particle, uint64_t component);
 
+/* A release point: the fields of Source (Source.hpp:19-60); start/end in days (< 0: run start /
+ * no end), emission_mode as in wo_source_emission_times, and only mode 1 emits. */
+typedef struct wo_source {
+    double k, j, i;
+    double start, end;
+    double emission_value;
+    int32_t emission_mode;
+    int32_t mode;
+} wo_source;
+
+/* Sources::emit + Source::emissionTimes + Source::emit (Sources.cpp:233-249, Source.cpp:16-45):
+ * appends the interval's releases of every source to out[0..) in stable time order, ids from
+ * first_id on. Returns the count (writing at most cap records) or -1 on an invalid schedule. */
+long wo_sources_emit(const wo_config *config, const wo_source *sources, int n_sources,
+                     double julian_start, double interval_start, double interval_end,
+                     uint64_t first_id, wo_particle *out, long cap);
+
 /* kji2deplatlon / deplatlon2kji (OceanModelAdapter.cpp:271-442) on a grid with lon/lat in
  * degrees [eta][xi], h [eta][xi] and sW[sW] (indexed k+sW-1). kji2deplatlon returns -1 and
  * 1e37 outputs off the grid; deplatlon2kji returns -1 when the point is not on the grid. */

@@ -23,6 +23,7 @@ SEMANTICS_HOST, SEMANTICS_DEVICE = 0, 1
 ARITH_REFERENCE, ARITH_FP32 = 0, 1
 STORAGE_FP32, STORAGE_FP16, STORAGE_BF16 = 0, 1, 2
 RNG_REFERENCE, RNG_PHILOX = 0, 1
+EMISSION_UNIFORM_RATE, EMISSION_FORCING_INTERVAL_BATCH, EMISSION_SINGLE_PULSE = 0, 1, 2
 
 
 class options_t(ctypes.Structure):
@@ -58,6 +59,9 @@ SIGNATURES = {
     "wacomm_b200_move_interval": (_i, [_vp, _i]),
     "wacomm_b200_move_interval_host": (_i, [_vp, _i, _vp, _sz]),
     "wacomm_b200_remove_dead": (_i, [_vp]),
+    "wacomm_b200_emit": (_i, [_vp, _vp, _i, _d, _d, _d, ctypes.POINTER(_sz)]),
+    "wacomm_b200_set_geo_grid": (_i, [_vp, _dp, _dp, _dp]),
+    "wacomm_b200_geo_positions": (_i, [_vp, _dp, _dp, _dp, _sz]),
     "wacomm_b200_concentration_reset": (_i, [_vp, _i]),
     "wacomm_b200_concentration_count": (_i, [_vp, _i]),
     "wacomm_b200_concentration_get": (_i, [_vp, _vp, _sz]),

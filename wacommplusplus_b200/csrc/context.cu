@@ -83,6 +83,16 @@ struct wacomm_b200_context {
     uint32_t *dConc = nullptr;
     int concTimes = 0;
 
+    wacomm_b200_source *dSources = nullptr;  // emission: the sources of the last call
+    size_t sourcesCap = 0;
+    unsigned char *dEmitScratch = nullptr;
+    size_t emitScratchCap = 0;
+
+    double *dGeoLon = nullptr, *dGeoLat = nullptr, *dSWValues = nullptr;  // kji2deplatlon grid
+    bool hasGeo = false;
+    double *dGeoOut = nullptr;  // [3][n] depth, lat, lon
+    size_t geoOutCap = 0;
+
     unsigned long long *dSteps = nullptr;
     int *dErr = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evMove0 = nullptr, evMove1 = nullptr;
@@ -531,6 +541,12 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dCount);
     cudaFree(ctx->dAos);
     cudaFree(ctx->dConc);
+    cudaFree(ctx->dSources);
+    cudaFree(ctx->dEmitScratch);
+    cudaFree(ctx->dGeoLon);
+    cudaFree(ctx->dGeoLat);
+    cudaFree(ctx->dSWValues);
+    cudaFree(ctx->dGeoOut);
     cudaFree(ctx->dSteps);
     cudaFree(ctx->dErr);
     cudaFree(ctx->dCfg);
@@ -612,6 +628,11 @@ int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, i
     cudaFree(ctx->dEnv);
     ctx->dEnv = nullptr;
     ctx->hasGrid = false;
+    cudaFree(ctx->dGeoLon);
+    cudaFree(ctx->dGeoLat);
+    cudaFree(ctx->dSWValues);
+    ctx->dGeoLon = ctx->dGeoLat = ctx->dSWValues = nullptr;
+    ctx->hasGeo = false;
     CUDA_TRY(ctx, cudaMalloc(&ctx->dLon, plane * sizeof(double)));
     CUDA_TRY(ctx, cudaMalloc(&ctx->dLat, plane * sizeof(double)));
     CUDA_TRY(ctx, cudaMalloc(&ctx->dH, plane * sizeof(double)));
@@ -846,6 +867,87 @@ int wacomm_b200_remove_dead(wacomm_b200_context *ctx) {
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     std::swap(ctx->S, ctx->T);
     ctx->n = kept;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_emit(wacomm_b200_context *ctx, const wacomm_b200_source *sources, int n_sources,
+                     double julian_start, double interval_start, double interval_end,
+                     size_t *emitted) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (emitted) *emitted = 0;
+    if (n_sources < 0 || (n_sources > 0 && !sources))
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "%d sources at %p", n_sources, (const void *)sources);
+    if (!ctx->hasConfig) return fail(ctx, WACOMM_B200_ERR_STATE, "set_config has not been called");
+    if (n_sources == 0) return WACOMM_B200_OK;
+    cudaSetDevice(ctx->device);
+    int rc;
+    if ((rc = grow(ctx, ctx->dSources, ctx->sourcesCap, (size_t)n_sources))) return rc;
+    if ((rc = grow(ctx, ctx->dEmitScratch, ctx->emitScratchCap, emission_scratch_bytes(n_sources))))
+        return rc;
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dSources, sources, n_sources * sizeof(wacomm_b200_source),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    uint64_t firstId = 0;  // Source.cpp:27: the last record's id + 1, or 0
+    if (ctx->n) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(&firstId, ctx->S.s.id + ctx->n - 1, sizeof(uint64_t),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    unsigned long long total = 0;
+    int err = 0;
+    CUDA_TRY(ctx, emission_plan(ctx->dSources, n_sources, julian_start, interval_start,
+                                interval_end, ctx->dEmitScratch, &total, &err, ctx->stream));
+    if (ctx->n) firstId += 1;
+    if (err & 2) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "invalid source emission schedule");
+    if (err & 4 || ctx->n + total >= MAX_PARTICLES)
+        return fail(ctx, WACOMM_B200_ERR_CAPACITY, "emission of %llu records beyond 2^31", total);
+    if (total == 0) return WACOMM_B200_OK;
+    if ((rc = reserve_particles(ctx, ctx->n + total, ctx->n))) return rc;
+    CUDA_TRY(ctx, emission_fill(ctx->dSources, n_sources, ctx->dEmitScratch, total, ctx->dCfg,
+                                firstId, ctx->S.s, ctx->n, ctx->stream));
+    ctx->n += total;
+    if (emitted) *emitted = total;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_set_geo_grid(wacomm_b200_context *ctx, const double *lon, const double *lat,
+                             const double *s_w_values) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!ctx->hasGrid) return fail(ctx, WACOMM_B200_ERR_STATE, "set_grid has not been called");
+    if (!lon || !lat || !s_w_values) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null geo array");
+    cudaSetDevice(ctx->device);
+    size_t plane = (size_t)ctx->eta * ctx->xi;
+    if (!ctx->dGeoLon) {
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dGeoLon, plane * sizeof(double)));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dGeoLat, plane * sizeof(double)));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dSWValues, (size_t)ctx->sW * sizeof(double)));
+    }
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dGeoLon, lon, plane * sizeof(double), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dGeoLat, lat, plane * sizeof(double), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dSWValues, s_w_values, (size_t)ctx->sW * sizeof(double),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->hasGeo = true;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_geo_positions(wacomm_b200_context *ctx, double *depth, double *lat, double *lon,
+                              size_t n) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!ctx->hasGeo) return fail(ctx, WACOMM_B200_ERR_STATE, "set_geo_grid has not been called");
+    if (n < ctx->n) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "buffers of %zu for %zu records", n, ctx->n);
+    if (ctx->n == 0) return WACOMM_B200_OK;
+    if (!depth || !lat || !lon) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null output");
+    cudaSetDevice(ctx->device);
+    int rc;
+    if ((rc = grow(ctx, ctx->dGeoOut, ctx->geoOutCap, 3 * ctx->n))) return rc;
+    double *dDep = ctx->dGeoOut, *dLat = dDep + ctx->n, *dLon = dLat + ctx->n;
+    CUDA_TRY(ctx, geo_positions(ctx->S.s, (int)ctx->n, ctx->eta, ctx->xi, ctx->sW, ctx->dGeoLon,
+                                ctx->dGeoLat, ctx->dH, ctx->dSWValues, dDep, dLat, dLon, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(depth, dDep, ctx->n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(lat, dLat, ctx->n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(lon, dLon, ctx->n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return WACOMM_B200_OK;
 }
 

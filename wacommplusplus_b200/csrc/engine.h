@@ -94,6 +94,29 @@ cudaError_t count_concentration(const ParticleSoA &S, int n, int concTime, int s
 cudaError_t concentration_to_float(const uint32_t *conc, size_t n, int nTimes, int sRho, int eta,
                                    int xi, const double *mask, float *out, cudaStream_t stream);
 
+// emission.cu ------------------------------------------------------------------------------
+
+// Scratch for one emission of n sources (release schedules, counts, offsets, status).
+size_t emission_scratch_bytes(int nSources);
+
+// First pass: schedules, per-source counts and their offsets on the device; the total number of
+// releases and an error word (bit 1: invalid schedule, bit 2: too many releases) are copied to
+// the host (the call synchronizes the stream).
+cudaError_t emission_plan(const wacomm_b200_source *sources, int nSources, double julianStart,
+                          double intervalStart, double intervalEnd, void *scratch,
+                          unsigned long long *totalHost, int *errHost, cudaStream_t stream);
+
+// Second pass: writes the `total` releases in merged time order into S at slots base.. with ids
+// firstId.. .
+cudaError_t emission_fill(const wacomm_b200_source *sources, int nSources, const void *scratch,
+                          unsigned long long total, const wacomm_b200_config *cfgDevice,
+                          uint64_t firstId, const ParticleSoA &S, size_t base, cudaStream_t stream);
+
+// kji2deplatlon of n records into device arrays.
+cudaError_t geo_positions(const ParticleSoA &S, int n, int eta, int xi, int sW, const double *lon,
+                          const double *lat, const double *h, const double *sWValues, double *dep,
+                          double *latOut, double *lonOut, cudaStream_t stream);
+
 // dropin.cu -------------------------------------------------------------------------------
 int dropin_move(const wacomm_b200_config *config, wacomm_b200_particle *particles, int timeIndex,
                 int oceanTime, int sW, int sRho, int eta, int xi, const double *times,

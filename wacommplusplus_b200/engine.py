@@ -10,7 +10,7 @@ import numpy as np
 
 from . import _native
 from ._native import WacommError, options_t
-from .types import PARTICLE_DTYPE, config_data
+from .types import PARTICLE_DTYPE, SOURCE_DTYPE, config_data
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _fp = ctypes.POINTER(ctypes.c_float)
@@ -162,6 +162,32 @@ class Engine:
 
     def remove_dead(self):
         self._check(self._lib.wacomm_b200_remove_dead(self._ctx))
+
+    # -------------------------------------------------------------- emission and geography
+    def emit(self, sources, interval_start, interval_end, julian_start=0.0):
+        """Appends the releases of ``sources`` (SOURCE_DTYPE) in [interval_start, interval_end)
+        seconds, merged in time order (Sources::emit); returns how many were appended."""
+        src = np.ascontiguousarray(sources, dtype=SOURCE_DTYPE)
+        n = ctypes.c_size_t()
+        self._check(self._lib.wacomm_b200_emit(self._ctx, src.ctypes.data if len(src) else None,
+                                               len(src), julian_start, interval_start,
+                                               interval_end, ctypes.byref(n)))
+        return n.value
+
+    def set_geo_grid(self, lon, lat, s_w_values):
+        """Output grid of geo_positions: lon/lat [eta][xi] and the s_w coordinate values."""
+        self._geo = [_d(lon), _d(lat), _d(s_w_values)]
+        self._check(self._lib.wacomm_b200_set_geo_grid(self._ctx, self._geo[0][1],
+                                                       self._geo[1][1], self._geo[2][1]))
+
+    def geo_positions(self):
+        """(depth, lat, lon) float64 arrays of the resident records (kji2deplatlon)."""
+        n = self.count()
+        dep, lat, lon = (np.empty(n, dtype=np.float64) for _ in range(3))
+        self._check(self._lib.wacomm_b200_geo_positions(self._ctx, dep.ctypes.data_as(_dp),
+                                                        lat.ctypes.data_as(_dp),
+                                                        lon.ctypes.data_as(_dp), n))
+        return dep, lat, lon
 
     def synchronize(self):
         self._check(self._lib.wacomm_b200_synchronize(self._ctx))

@@ -93,6 +93,29 @@ PARTICLE_DTYPE = np.dtype({
 })
 
 
+# Release point of wacomm_b200_emit (the fields of Source, Source.hpp:19-60): grid indices, start
+# and end in days (negative: run start / open end), the emission value and schedule, and the
+# source's own mode (only mode 1 emits).
+SOURCE_DTYPE = np.dtype({
+    "names": ["k", "j", "i", "start", "end", "emission_value", "emission_mode", "mode"],
+    "formats": ["<f8", "<f8", "<f8", "<f8", "<f8", "<f8", "<i4", "<i4"],
+    "offsets": [0, 8, 16, 24, 32, 40, 48, 52],
+    "itemsize": 56,
+})
+EMISSION_MODES = {"uniform_rate": 0, "forcing_interval_batch": 1, "single_pulse": 2}
+
+
+def make_sources(rows):
+    """A SOURCE_DTYPE array from (k, j, i, start, end, value, schedule[, mode]) tuples, schedule
+    a name of EMISSION_MODES or its number; mode defaults to 1."""
+    out = np.zeros(len(rows), dtype=SOURCE_DTYPE)
+    for n, row in enumerate(rows):
+        k, j, i, start, end, value, schedule = row[:7]
+        out[n] = (k, j, i, start, end, value,
+                  EMISSION_MODES.get(schedule, schedule), row[7] if len(row) > 7 else 1)
+    return out
+
+
 def default_config(**overrides):
     """A ``config_data`` holding the reference defaults (Config.cpp:46-205): dti 30 s,
     deltat 3600 s, tau0 86400 s, survprob 1e-4, sv 0, crid 1, sigma 3.46, shore 0.25 m,
