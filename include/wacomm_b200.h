@@ -124,6 +124,8 @@ typedef struct wacomm_b200_options {
     int launch_shape;         /* FP32 step: 0 = 256 threads, registers unbounded; 1 = 128 threads,
                                  3 blocks/SM; 2 = 256 threads, 2 blocks/SM; 3 = 128 threads,
                                  5 blocks/SM (fewer registers, more resident warps) */
+    int surrogate;            /* 1: deterministic forward intervals by the learned surrogate
+                                 (wacomm_b200_set_surrogate), the rest by the FP32 step */
 } wacomm_b200_options;
 
 /* ------------------------------------------------------------------ context */
@@ -140,7 +142,8 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx);
 const char *wacomm_b200_last_error(const wacomm_b200_context *ctx);
 
 /* Fills *out with the defaults: host semantics, FP32 arithmetic and storage, reference RNG,
- * 256 threads, one launch per interval, cell sort on, fused concentration on, launch shape 2. */
+ * 256 threads, one launch per interval, cell sort on, fused concentration on, launch shape 2,
+ * surrogate off. */
 int wacomm_b200_default_options(wacomm_b200_options *out);
 int wacomm_b200_set_options(wacomm_b200_context *ctx, const wacomm_b200_options *options);
 int wacomm_b200_get_options(const wacomm_b200_context *ctx, wacomm_b200_options *out);
@@ -237,6 +240,20 @@ int wacomm_b200_synchronize(wacomm_b200_context *ctx);
  * kernels it launched and how many particle-steps (substeps of active particles) it took. */
 int wacomm_b200_last_interval_stats(const wacomm_b200_context *ctx, float *device_ms,
                                     float *move_ms, int *kernel_launches, double *particle_steps);
+
+/* No counterpart in the reference: the learned one-interval advection surrogate. parameters holds
+ * count = 231,939 FP32 values: w1 [256][388] (inputs: the 4x4x4 u, v, w stencil at both records,
+ * then jF, iF, kF and the activation fraction), b1 [256], w2 [256][256], b2, w3 [256][256], b3,
+ * w4 [3][256], b4 [3]. With the surrogate option on, move_interval moves each active particle of
+ * a deterministic forward interval by one MLP evaluation (BF16 tensor-core GEMMs) plus the
+ * closures in closed form; random walk, backward tracking, drifting objects, restart-clipped
+ * intervals, starts outside the valid cells and paths near dry nodes use the FP32 step. */
+int wacomm_b200_set_surrogate(wacomm_b200_context *ctx, const float *parameters, size_t count);
+
+/* Of the last move_interval with the surrogate on: particles it moved, particles handed to the
+ * FP32 step, and device milliseconds of the per-cell layer-1 kernel and of the particle kernel. */
+int wacomm_b200_last_surrogate_stats(const wacomm_b200_context *ctx, size_t *run, size_t *fallback,
+                                     float *cell_ms, float *step_ms);
 
 /* The CUDA stream (cudaStream_t) the context launches on, for callers that order their own work
  * or events against it. */

@@ -32,6 +32,7 @@ class options_t(ctypes.Structure):
         ("rng", ctypes.c_int), ("block_size", ctypes.c_int),
         ("substeps_per_launch", ctypes.c_int), ("sort_by_cell", ctypes.c_int),
         ("fuse_concentration", ctypes.c_int), ("launch_shape", ctypes.c_int),
+        ("surrogate", ctypes.c_int),
     ]
 
 
@@ -69,6 +70,9 @@ SIGNATURES = {
     "wacomm_b200_synchronize": (_i, [_vp]),
     "wacomm_b200_last_interval_stats": (_i, [_vp, _fp, _fp, ctypes.POINTER(_i), _dp]),
     "wacomm_b200_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
+    "wacomm_b200_set_surrogate": (_i, [_vp, _fp, _sz]),
+    "wacomm_b200_last_surrogate_stats": (_i, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz), _fp,
+                                              _fp]),
     "wacomm_b200_cuda_move_particle": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i] + [_vp] * 15 +
                                        [_i, _i, _i, _vp]),
     "wacomm_b200_cuda_move_particle_noalloc": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i] +

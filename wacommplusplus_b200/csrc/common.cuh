@@ -25,6 +25,7 @@ constexpr int INTEGRATOR_MIDPOINT = 2;  // Config.hpp:207
 
 // Error bits raised by kernels into the context's status word.
 constexpr int ERR_DRIFT_OBJECT = 1;
+constexpr int ERR_SURROGATE_WAIT = 8;  // a surrogate kernel gave up on a bounded barrier wait
 
 // Random-key coordinates of the drift model (DriftModel.hpp:110-114).
 constexpr long long ENSEMBLE_INTERVAL = (-9223372036854775807LL - 1);

@@ -88,6 +88,25 @@ struct wacomm_b200_context {
     unsigned char *dEmitScratch = nullptr;
     size_t emitScratchCap = 0;
 
+    // learned surrogate (surrogate.cu)
+    uint8_t *dSurrogate = nullptr;  // packed weights
+    bool hasSurrogate = false;
+    __half *dZ = nullptr;           // per-cell-level layer-1 sums [cell-levels][256]
+    float *dGate = nullptr;         // per-cell-level uniformity gate
+    size_t zCap = 0;                // cell-levels held
+    int zT0 = -1, zT1 = -1;         // forcing pair z was computed for
+    int *dDry = nullptr;            // dry-node prefix sums
+    size_t dryCap = 0;
+    double dryShore = NAN;
+    bool dryValid = false;
+    uint32_t *dFallback = nullptr;  // fallback list
+    size_t fallbackCap = 0;
+    unsigned long long *dSurrCounts = nullptr;  // [0]: fallback count (low 32 bits), [1]: run count
+    cudaEvent_t evCell0 = nullptr, evCell1 = nullptr, evStep0 = nullptr, evStep1 = nullptr;
+    bool surrTimed = false;
+    size_t lastRun = 0, lastFallback = 0;
+    int smCount = 148;
+
     double *dGeoLon = nullptr, *dGeoLat = nullptr, *dSWValues = nullptr;  // kji2deplatlon grid
     bool hasGeo = false;
     double *dGeoOut = nullptr;  // [3][n] depth, lat, lon
@@ -248,6 +267,11 @@ int validate_options(wacomm_b200_context *ctx, const wacomm_b200_options &o) {
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "substeps_per_launch must be >= 0");
     if (o.launch_shape < 0 || o.launch_shape > 3)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "launch_shape %d out of [0, 3]", o.launch_shape);
+    if (o.surrogate != 0 && o.surrogate != 1)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "surrogate %d: 0 or 1", o.surrogate);
+    if (o.surrogate && o.arithmetic != WACOMM_B200_ARITH_FP32)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT,
+                    "the surrogate hands uncovered particles to the FP32 step: needs FP32 arithmetic");
     return WACOMM_B200_OK;
 }
 
@@ -273,6 +297,7 @@ void release_frames(wacomm_b200_context *ctx) {
         s = FrameSlot{};
     }
     ctx->pairT0 = ctx->pairT1 = -1;
+    ctx->zT0 = ctx->zT1 = -1;
 }
 
 FrameDevice frame_of(const FrameSlot &s) {
@@ -443,6 +468,120 @@ int prepare_interval(wacomm_b200_context *ctx, int time_index, IntervalParams &P
     return WACOMM_B200_OK;
 }
 
+// Surrogate interval: per-cell layer 1 for the forcing pair, cell sort, the tensor-core step, then
+// the plain FP32 step over the particles the surrogate handed back.
+int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launches) {
+    if (!ctx->hasSurrogate)
+        return fail(ctx, WACOMM_B200_ERR_STATE, "the surrogate option needs set_surrogate weights");
+    const size_t count = ctx->n;
+    if (count == 0) return WACOMM_B200_OK;
+    int rc;
+    const FrameSlot &a = ctx->slots[P.t0], &b = ctx->slots[P.t1];
+    // dry-node table
+    const size_t dryNeed = (size_t)(ctx->eta + 1) * (ctx->xi + 1);
+    if (!ctx->dryValid || !(ctx->dryShore == ctx->cfg.shoreLimit)) {
+        if ((rc = grow(ctx, ctx->dDry, ctx->dryCap, dryNeed))) return rc;
+        CUDA_TRY(ctx, surrogate_dry_prefix(ctx->hasMask ? ctx->dMask : nullptr, ctx->dH,
+                                           ctx->cfg.shoreLimit, ctx->eta, ctx->xi, ctx->dDry,
+                                           ctx->stream));
+        launches += 2;
+        ctx->dryShore = ctx->cfg.shoreLimit;
+        ctx->dryValid = true;
+    }
+    // layer 1 per cell-level
+    const long long nCL = surrogate_cell_levels(ctx->eta, ctx->xi, ctx->sW);
+    CUDA_TRY(ctx, cudaEventRecord(ctx->evCell0, ctx->stream));
+    if (ctx->zT0 != P.t0 || ctx->zT1 != P.t1) {
+        if ((size_t)nCL > ctx->zCap) {
+            cudaFree(ctx->dZ);
+            cudaFree(ctx->dGate);
+            ctx->dZ = nullptr;
+            ctx->dGate = nullptr;
+            ctx->zCap = 0;
+            CUDA_TRY(ctx, cudaMalloc(&ctx->dZ, (size_t)nCL * 256 * sizeof(__half)));
+            CUDA_TRY(ctx, cudaMalloc(&ctx->dGate, (size_t)nCL * sizeof(float)));
+            ctx->zCap = (size_t)nCL;
+        }
+        CUDA_TRY(ctx, surrogate_cells(ctx->eta, ctx->xi, ctx->sW, ctx->sRho, frame_of(a), frame_of(b),
+                                      ctx->dSurrogate, ctx->dZ, ctx->dGate, ctx->dErr, ctx->smCount,
+                                      ctx->stream));
+        launches++;
+        ctx->zT0 = P.t0;
+        ctx->zT1 = P.t1;
+    }
+    CUDA_TRY(ctx, cudaEventRecord(ctx->evCell1, ctx->stream));
+    // work order and fallback list
+    if ((rc = reserve_work(ctx, count))) return rc;
+    if ((rc = grow(ctx, ctx->dFallback, ctx->fallbackCap, count))) return rc;
+    if ((rc = sort_work(ctx, ctx->S.s, count, ctx->dKeys, ctx->dOrder, launches))) return rc;
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->dSurrCounts, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    MoveLaunch L;
+    L.count = (int)count;
+    L.order = ctx->dOrder;
+    const int concTime = P.t0 + P.direction;
+    const bool countHere = ctx->opt.fuse_concentration && ctx->dConc && concTime >= 0 &&
+                           concTime < ctx->concTimes;
+    L.conc = countHere ? ctx->dConc : nullptr;
+    L.concTimeIndex = concTime;
+    L.concTimes = ctx->concTimes;
+    L.steps = ctx->dSteps;
+    L.err = ctx->dErr;
+    SurrogateStep st;
+    st.eta = ctx->eta;
+    st.xi = ctx->xi;
+    st.sW = ctx->sW;
+    st.sRho = ctx->sRho;
+    st.start = P.start;
+    st.length = P.length;
+    st.cfg = ctx->cfg;
+    const bool diffuse = ctx->cfg.random && (P.direction > 0 || ctx->cfg.backwardDiffusion);
+    st.fallbackAll = diffuse || P.direction < 0 || P.elapsed0 != 0 || P.length <= 0 ||
+                     ctx->cfg.leewayJibeProbabilityHourly > 0;
+    st.f0 = frame_of(a);
+    st.f1 = frame_of(b);
+    st.h = ctx->dH;
+    st.depthIntervals = ctx->dDepth;
+    st.metric = ctx->dMetric;
+    st.dry = ctx->dDry;
+    st.z = ctx->dZ;
+    st.gate = ctx->dGate;
+    st.weights = ctx->dSurrogate;
+    st.fallback = ctx->dFallback;
+    st.fallbackCount = reinterpret_cast<uint32_t *>(ctx->dSurrCounts);
+    st.runCount = ctx->dSurrCounts + 1;
+    CUDA_TRY(ctx, cudaEventRecord(ctx->evMove0, ctx->stream));
+    CUDA_TRY(ctx, cudaEventRecord(ctx->evStep0, ctx->stream));
+    ctx->moveTimed = true;
+    CUDA_TRY(ctx, surrogate_step(st, ctx->S.s, L, ctx->smCount, ctx->stream));
+    launches++;
+    CUDA_TRY(ctx, cudaEventRecord(ctx->evStep1, ctx->stream));
+    unsigned long long counts[2] = {0, 0};
+    CUDA_TRY(ctx, cudaMemcpyAsync(counts, ctx->dSurrCounts, sizeof(counts), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    const size_t nFallback = (size_t)(counts[0] & 0xffffffffull);
+    ctx->lastFallback = nFallback;
+    ctx->lastRun = (size_t)counts[1];
+    ctx->surrTimed = true;
+    if (nFallback) {
+        IntervalParams Q = P;
+        Q.rng = ctx->opt.rng;
+        Q.firstChunk = 1;
+        Q.lastChunk = 1;
+        Q.chunkEnd = INFINITY;
+        MoveLaunch F = L;
+        F.count = (int)nFallback;
+        F.order = ctx->dFallback;
+        cudaError_t e = move_f32_dispatch(ctx->opt.semantics, ctx->opt.storage, ctx->opt.launch_shape,
+                                          ctx->cfg, Q, packed_args(ctx), ctx->S.s, F, ctx->stream);
+        if (e != cudaSuccess)
+            return fail(ctx, WACOMM_B200_ERR_CUDA, "fallback move launch: %s", cudaGetErrorString(e));
+        launches++;
+    }
+    CUDA_TRY(ctx, cudaEventRecord(ctx->evMove1, ctx->stream));
+    return WACOMM_B200_OK;
+}
+
 int check_errors(wacomm_b200_context *ctx) {
     int flags = 0;
     CUDA_TRY(ctx, cudaMemcpy(&flags, ctx->dErr, sizeof(int), cudaMemcpyDeviceToHost));
@@ -450,6 +589,11 @@ int check_errors(wacomm_b200_context *ctx) {
         CUDA_TRY(ctx, cudaMemset(ctx->dErr, 0, sizeof(int)));
         return fail(ctx, WACOMM_B200_ERR_DRIFT_OBJECT,
                     "a particle names a drift object outside the catalogue (ids 0-22)");
+    }
+    if (flags & ERR_SURROGATE_WAIT) {
+        CUDA_TRY(ctx, cudaMemset(ctx->dErr, 0, sizeof(int)));
+        return fail(ctx, WACOMM_B200_ERR_CUDA,
+                    "a surrogate kernel gave up waiting on a tensor-core or copy barrier");
     }
     return WACOMM_B200_OK;
 }
@@ -480,6 +624,7 @@ int wacomm_b200_default_options(wacomm_b200_options *out) {
     out->sort_by_cell = 1;
     out->fuse_concentration = 1;
     out->launch_shape = 2;
+    out->surrogate = 0;
     return WACOMM_B200_OK;
 }
 
@@ -503,6 +648,12 @@ int wacomm_b200_context_create(int device, wacomm_b200_context **out) {
     if (e == cudaSuccess) e = cudaMalloc(&ctx->dErr, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&ctx->dCount, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(ctx->dErr, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->evCell0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->evCell1);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->evStep0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->evStep1);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->dSurrCounts, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->smCount, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) {
         wacomm_b200_context_destroy(ctx);
         return WACOMM_B200_ERR_CUDA;
@@ -541,6 +692,16 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dCount);
     cudaFree(ctx->dAos);
     cudaFree(ctx->dConc);
+    cudaFree(ctx->dSurrogate);
+    cudaFree(ctx->dZ);
+    cudaFree(ctx->dGate);
+    cudaFree(ctx->dDry);
+    cudaFree(ctx->dFallback);
+    cudaFree(ctx->dSurrCounts);
+    if (ctx->evCell0) cudaEventDestroy(ctx->evCell0);
+    if (ctx->evCell1) cudaEventDestroy(ctx->evCell1);
+    if (ctx->evStep0) cudaEventDestroy(ctx->evStep0);
+    if (ctx->evStep1) cudaEventDestroy(ctx->evStep1);
     cudaFree(ctx->dSources);
     cudaFree(ctx->dEmitScratch);
     cudaFree(ctx->dGeoLon);
@@ -662,6 +823,8 @@ int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, i
     ctx->sW = s_w;
     ctx->metricSemantics = -1;
     ctx->pairT0 = ctx->pairT1 = -1;
+    ctx->zT0 = ctx->zT1 = -1;
+    ctx->dryValid = false;
     ctx->hasGrid = true;
     // Forcing records of another grid no longer fit: release them.
     release_frames(ctx);
@@ -675,6 +838,7 @@ int wacomm_b200_set_times(wacomm_b200_context *ctx, int n_times, const double *o
     ctx->times.assign(ocean_time, ocean_time + n_times);
     if ((int)ctx->slots.size() < n_times) ctx->slots.resize(n_times);
     ctx->pairT0 = ctx->pairT1 = -1;
+    ctx->zT0 = ctx->zT1 = -1;
     return WACOMM_B200_OK;
 }
 
@@ -718,6 +882,7 @@ int wacomm_b200_upload_frame(wacomm_b200_context *ctx, int t, const float *zeta,
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
     s.loaded = true;
     if (ctx->pairT0 == t || ctx->pairT1 == t) ctx->pairT0 = ctx->pairT1 = -1;
+    if (ctx->zT0 == t || ctx->zT1 == t) ctx->zT0 = ctx->zT1 = -1;
     return WACOMM_B200_OK;
 }
 
@@ -778,9 +943,14 @@ int wacomm_b200_move_interval(wacomm_b200_context *ctx, int time_index) {
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     int rc = prepare_interval(ctx, time_index, P, launches);
     if (rc) return rc;
+    ctx->surrTimed = false;
     if (!P.skip && ctx->n) {
-        if ((rc = reserve_work(ctx, ctx->n))) return rc;
-        if ((rc = run_interval(ctx, P, 0, ctx->n, ctx->dKeys, ctx->dOrder, launches))) return rc;
+        if (ctx->opt.surrogate) {
+            if ((rc = run_surrogate(ctx, P, launches))) return rc;
+        } else {
+            if ((rc = reserve_work(ctx, ctx->n))) return rc;
+            if ((rc = run_interval(ctx, P, 0, ctx->n, ctx->dKeys, ctx->dOrder, launches))) return rc;
+        }
     }
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     ctx->lastLaunches = launches;
@@ -1017,6 +1187,39 @@ int wacomm_b200_synchronize(wacomm_b200_context *ctx) {
     cudaSetDevice(ctx->device);
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return check_errors(ctx);
+}
+
+int wacomm_b200_set_surrogate(wacomm_b200_context *ctx, const float *parameters, size_t count) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!parameters) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null surrogate parameters");
+    if (count != surrogate_parameter_count())
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "surrogate needs %zu parameters, got %zu",
+                    surrogate_parameter_count(), count);
+    cudaSetDevice(ctx->device);
+    std::vector<uint8_t> image(surrogate_packed_bytes());
+    surrogate_pack(parameters, image.data());
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (!ctx->dSurrogate) CUDA_TRY(ctx, cudaMalloc(&ctx->dSurrogate, image.size()));
+    CUDA_TRY(ctx, cudaMemcpy(ctx->dSurrogate, image.data(), image.size(), cudaMemcpyHostToDevice));
+    ctx->hasSurrogate = true;
+    ctx->zT0 = ctx->zT1 = -1;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_last_surrogate_stats(const wacomm_b200_context *ctx, size_t *run, size_t *fallback,
+                                     float *cell_ms, float *step_ms) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (run) *run = ctx->surrTimed ? ctx->lastRun : 0;
+    if (fallback) *fallback = ctx->surrTimed ? ctx->lastFallback : 0;
+    float c = 0.f, s = 0.f;
+    if (ctx->surrTimed) {
+        cudaSetDevice(ctx->device);
+        if (cudaEventElapsedTime(&c, ctx->evCell0, ctx->evCell1) != cudaSuccess) c = 0.f;
+        if (cudaEventElapsedTime(&s, ctx->evStep0, ctx->evStep1) != cudaSuccess) s = 0.f;
+    }
+    if (cell_ms) *cell_ms = c;
+    if (step_ms) *step_ms = s;
+    return WACOMM_B200_OK;
 }
 
 int wacomm_b200_last_interval_stats(const wacomm_b200_context *ctx, float *device_ms,

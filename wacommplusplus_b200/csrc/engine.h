@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "wacomm_b200.h"
@@ -116,6 +117,42 @@ cudaError_t emission_fill(const wacomm_b200_source *sources, int nSources, const
 cudaError_t geo_positions(const ParticleSoA &S, int n, int eta, int xi, int sW, const double *lon,
                           const double *lat, const double *h, const double *sWValues, double *dep,
                           double *latOut, double *lonOut, cudaStream_t stream);
+
+// surrogate.cu -----------------------------------------------------------------------------
+
+// One surrogate interval: grid, interval, run parameters, the bracketing records (FP32 reference
+// layout), the static grid tables, the per-cell layer-1 sums and gate, the packed weights and the
+// fallback outputs.
+struct SurrogateStep {
+    int eta, xi, sW, sRho;
+    double start, length;
+    wacomm_b200_config cfg;
+    int fallbackAll;
+    FrameDevice f0, f1;
+    const double *h, *depthIntervals;
+    const double2 *metric;
+    const int *dry;
+    const __half *z;
+    const float *gate;
+    const uint8_t *weights;
+    uint32_t *fallback, *fallbackCount;
+    unsigned long long *runCount;
+};
+
+size_t surrogate_packed_bytes();
+size_t surrogate_parameter_count();
+// Packs the flat FP32 parameters (w1 [256][388], b1, w2 [256][256], b2, w3, b3, w4 [3][256], b4)
+// into the device image: BF16 swizzled K-blocks of the GEMM weights, FP32 vectors.
+void surrogate_pack(const float *flat, uint8_t *out);
+long long surrogate_cell_levels(int eta, int xi, int sW);
+cudaError_t surrogate_cells(int eta, int xi, int sW, int sRho, const FrameDevice &f0,
+                            const FrameDevice &f1, const uint8_t *weights, __half *z, float *gate,
+                            int *err, int smCount, cudaStream_t stream);
+cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const MoveLaunch &L,
+                           int smCount, cudaStream_t stream);
+// Inclusive 2-D prefix sums [(eta+1)][(xi+1)] of nodes with mask 0 or h <= shore.
+cudaError_t surrogate_dry_prefix(const double *mask, const double *h, double shore, int eta, int xi,
+                                 int *pre, cudaStream_t stream);
 
 // dropin.cu -------------------------------------------------------------------------------
 int dropin_move(const wacomm_b200_config *config, wacomm_b200_particle *particles, int timeIndex,

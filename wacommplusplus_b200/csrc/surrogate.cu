@@ -1,0 +1,848 @@
+// Learned one-interval advection surrogate on the tensor cores (tcgen05, sm_100a).
+//
+// The MLP 388 -> 256 -> 256 -> 256 -> 3 (GELU, tanh form) is split in two kernels:
+//
+// * surrogate_cell_kernel: the stencil part of layer 1 depends only on the cell and level a
+//   particle starts in, so it is evaluated once per cell-level as a GEMM
+//   [cell-levels x 384] x [384 x 256] (BF16 operands, FP32 accumulation in TMEM) and stored as
+//   FP16 pre-activations z, together with the uniformity gate of the stencil;
+// * surrogate_step_kernel: per tile of 128 particles (in cell order), layer 1 is finished on the
+//   CUDA cores from z and the four particle features, layers 2 and 3 run as two
+//   [128 x 256] x [256 x 256] tcgen05 GEMMs with the weights streamed through a 3-stage
+//   shared-memory ring by bulk copies, layer 3's epilogue folds in the 3-output layer 4, and the
+//   displacement is applied with the closures in closed form. Particles the surrogate does not
+//   cover are appended to a fallback list for the plain kernel.
+//
+// Warp roles of the step kernel (320 threads): warps 0-7 own the tile's rows (warp w holds rows
+// 32(w%4).. and columns 128(w/4).. of the accumulator, the TMEM lane quarter it may access), warp
+// 8 streams weights, warp 9 issues the MMAs and owns the TMEM allocation. Every wait is bounded;
+// a timeout raises an error flag and the block drains and exits.
+#include <cstring>
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "engine.h"
+#include "move_kernels.cuh"
+#include "umma.cuh"
+
+namespace wb {
+
+namespace {
+
+constexpr int HID = 256;
+constexpr int N_STENCIL = 384;
+constexpr int N_INPUT = 388;
+constexpr int TILE = 128;
+constexpr uint32_t KBLOCK_A = TILE * 128;  // 16 KB: 128 rows x 64 BF16
+constexpr uint32_t KBLOCK_W = HID * 128;   // 32 KB: 256 rows x 64 BF16
+constexpr int CELL_KB = N_STENCIL / 64;    // 6
+constexpr int HID_KB = HID / 64;           // 4
+constexpr int RING = 3;
+constexpr float W_FEATURE = 1000.f;        // 1 / (w feature scale, m/s)
+constexpr float OUT_H = 100.f, OUT_V = 1.f;
+constexpr float GATE_SIGMA = 0.01f;
+constexpr int GATE_REF = (1 * 4 + 1) * 4 + 1;
+
+// Offsets in the packed weight buffer (bytes; every block starts on 1024 bytes).
+constexpr size_t OFF_W1 = 0;
+constexpr size_t OFF_W2 = OFF_W1 + (size_t)CELL_KB * KBLOCK_W;
+constexpr size_t OFF_W3 = OFF_W2 + (size_t)HID_KB * KBLOCK_W;
+constexpr size_t OFF_B1 = OFF_W3 + (size_t)HID_KB * KBLOCK_W;
+constexpr size_t OFF_B2 = OFF_B1 + 1024;
+constexpr size_t OFF_B3 = OFF_B2 + 1024;
+constexpr size_t OFF_W1P = OFF_B3 + 1024;
+constexpr size_t OFF_W4 = OFF_W1P + 4096;
+constexpr size_t OFF_B4 = OFF_W4 + 3072;
+constexpr size_t PACKED_BYTES = OFF_B4 + 1024;
+
+__device__ __forceinline__ float gelu_tanh(float x) {
+    float inner = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(inner));
+    return 0.5f * x * (1.f + t);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+__device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
+    return (uint8_t *)(((uintptr_t)p + 1023) & ~(uintptr_t)1023);
+}
+
+// ------------------------------------------------------------------ per-cell layer 1
+
+struct CellArgs {
+    int eta, xi, sW, sRho;
+    long long nCL;  // (eta-1) * (xi-1) * (sW-1) cell-levels, index ((j*(xi-1)) + i)*(sW-1) + kI+sW-2
+    const float *u0, *v0, *w0, *u1, *v1, *w1;
+    const uint8_t *weights;
+    __half *z;      // [nCL][256]
+    float *gate;    // [nCL]
+    int *err;
+};
+
+constexpr size_t CELL_SMEM = (size_t)CELL_KB * KBLOCK_A + 2 * (size_t)KBLOCK_W + 1024;
+
+__global__ void __launch_bounds__(128, 1) surrogate_cell_kernel(const CellArgs a) {
+    using namespace umma;
+    extern __shared__ uint8_t dynSmem[];
+    uint8_t *sA = align1024(dynSmem);
+    uint8_t *sW = sA + CELL_KB * KBLOCK_A;
+    __shared__ __align__(8) uint64_t full[2], empty[2], accFull;
+    __shared__ uint32_t tmemSlot;
+    __shared__ int abortFlag;
+    __shared__ float b1s[HID];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    if (tid == 0) {
+        for (int s = 0; s < 2; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&accFull, 1);
+        abortFlag = 0;
+        fence_barrier_init();
+    }
+    const float *b1 = reinterpret_cast<const float *>(a.weights + OFF_B1);
+    for (int c = tid; c < HID; c += 128) b1s[c] = b1[c];
+    if (warp == 0) tmem_alloc(&tmemSlot, 256);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = tmemSlot;
+    const int levels = a.sW - 1;
+    const long long nTiles = (a.nCL + TILE - 1) / TILE;
+    const uint32_t idesc = idesc_bf16(TILE, HID);
+    uint32_t g = 0;                      // weight blocks loaded so far (thread 0)
+    int issued[2] = {-1, -1}, consumed[2] = {-1, -1};
+    int it = 0;
+    for (long long tile = blockIdx.x; tile < nTiles; tile += gridDim.x, it++) {
+        // ---- gather: thread = row = cell-level
+        const long long cl = tile * TILE + tid;
+        float gsum = 0.f;
+        if (cl < a.nCL) {
+            const int lev = (int)(cl % levels);
+            const long long cell = cl / levels;
+            const int j = (int)(cell / (a.xi - 1)), i = (int)(cell % (a.xi - 1));
+            const int kI = lev - (a.sW - 2);
+#pragma unroll 1
+            for (int q = 0; q < N_STENCIL / 8; q++) {
+                const int f = q * 8;
+                const int rec = f / 192, field = (f / 64) % 3, c = (f / 16) % 4, a0 = (f % 16) / 4;
+                const float *src = rec == 0 ? (field == 0 ? a.u0 : field == 1 ? a.v0 : a.w0)
+                                            : (field == 0 ? a.u1 : field == 1 ? a.v1 : a.w1);
+                const int nlev = field == 2 ? a.sW : a.sRho;
+                int L = kI - 2 + c;
+                L = L < -nlev + 1 ? -nlev + 1 : (L > 0 ? 0 : L);
+                L += nlev - 1;
+                const float scale = field == 2 ? W_FEATURE : 1.f;
+                float v[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    int jj = j - 1 + a0 + e / 4, ii = i - 1 + e % 4;
+                    jj = jj < 0 ? 0 : (jj > a.eta - 1 ? a.eta - 1 : jj);
+                    ii = ii < 0 ? 0 : (ii > a.xi - 1 ? a.xi - 1 : ii);
+                    v[e] = __ldg(src + ((size_t)L * a.eta + jj) * a.xi + ii) * scale;
+                }
+                uint4 pk;
+                pk.x = pack_bf16(v[0], v[1]);
+                pk.y = pack_bf16(v[2], v[3]);
+                pk.z = pack_bf16(v[4], v[5]);
+                pk.w = pack_bf16(v[6], v[7]);
+                *reinterpret_cast<uint4 *>(sA + (f / 64) * KBLOCK_A + sw128_offset(tid, f % 64)) = pk;
+            }
+            // uniformity gate from the FP32 forcing: squared deviations of the u and v blocks of
+            // both records from each block's node GATE_REF
+            auto node = [&](const float *src, int n) {
+                int lv = kI - 2 + n / 16;
+                lv = lv < -a.sRho + 1 ? -a.sRho + 1 : (lv > 0 ? 0 : lv);
+                lv += a.sRho - 1;
+                int jj = j - 1 + (n % 16) / 4, ii = i - 1 + n % 4;
+                jj = jj < 0 ? 0 : (jj > a.eta - 1 ? a.eta - 1 : jj);
+                ii = ii < 0 ? 0 : (ii > a.xi - 1 ? a.xi - 1 : ii);
+                return __ldg(src + ((size_t)lv * a.eta + jj) * a.xi + ii);
+            };
+            const float *blocks[4] = {a.u0, a.v0, a.u1, a.v1};
+#pragma unroll 1
+            for (int blk = 0; blk < 4; blk++) {
+                const float x0 = node(blocks[blk], GATE_REF);
+                float sum = 0.f;
+                for (int n = 0; n < 64; n++) {
+                    const float d = node(blocks[blk], n) - x0;
+                    sum = fmaf(d, d, sum);
+                }
+                gsum += sum;
+            }
+        } else {
+            const uint4 zero = make_uint4(0, 0, 0, 0);
+            for (int q = 0; q < N_STENCIL / 8; q++)
+                *reinterpret_cast<uint4 *>(sA + (q * 8 / 64) * KBLOCK_A + sw128_offset(tid, (q * 8) % 64)) = zero;
+        }
+        fence_async_shared();
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+        if (abortFlag) break;
+        // ---- weights through a 2-stage ring and the MMAs (thread 0)
+        if (tid == 0) {
+            bool ok = true;
+            auto load = [&](uint32_t gg, int kb) {
+                const uint32_t s = gg & 1, n = gg >> 1;
+                if (!mbar_wait(&empty[s], (n & 1) ^ 1, &abortFlag)) return false;
+                mbar_expect_tx(&full[s], KBLOCK_W);
+                bulk_g2s(sW + s * KBLOCK_W, a.weights + OFF_W1 + (size_t)kb * KBLOCK_W, KBLOCK_W, &full[s]);
+                issued[s] = (int)n;
+                return true;
+            };
+            ok = load(g, 0) && load(g + 1, 1);
+            for (int kb = 0; kb < CELL_KB && ok; kb++) {
+                const uint32_t gg = g + kb, s = gg & 1, n = gg >> 1;
+                if (!mbar_wait(&full[s], n & 1, &abortFlag)) {
+                    ok = false;
+                    break;
+                }
+                consumed[s] = (int)n;
+                fence_after_sync();
+#pragma unroll
+                for (int ks = 0; ks < 4; ks++)
+                    mma_bf16(tmem, desc_sw128(smem_u32(sA + kb * KBLOCK_A + ks * 32)),
+                             desc_sw128(smem_u32(sW + s * KBLOCK_W + ks * 32)), idesc, (kb | ks) != 0);
+                mma_commit(&empty[s]);
+                if (kb + 2 < CELL_KB) ok = load(gg + 2, kb + 2);
+            }
+            mma_commit(&accFull);
+            g += CELL_KB;
+        }
+        __syncwarp();
+        mbar_wait(&accFull, it & 1, &abortFlag);
+        __syncwarp();
+        fence_after_sync();
+        // ---- epilogue: z = acc + b1 (FP16), gate
+        const bool write = cl < a.nCL && !abortFlag;
+#pragma unroll 1
+        for (int c0 = 0; c0 < HID; c0 += 32) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+            if (write) {
+                uint4 *dst = reinterpret_cast<uint4 *>(a.z + (size_t)cl * HID + c0);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    __half2 h0 = __floats2half2_rn(v[8 * q + 0] + b1s[c0 + 8 * q + 0], v[8 * q + 1] + b1s[c0 + 8 * q + 1]);
+                    __half2 h1 = __floats2half2_rn(v[8 * q + 2] + b1s[c0 + 8 * q + 2], v[8 * q + 3] + b1s[c0 + 8 * q + 3]);
+                    __half2 h2 = __floats2half2_rn(v[8 * q + 4] + b1s[c0 + 8 * q + 4], v[8 * q + 5] + b1s[c0 + 8 * q + 5]);
+                    __half2 h3 = __floats2half2_rn(v[8 * q + 6] + b1s[c0 + 8 * q + 6], v[8 * q + 7] + b1s[c0 + 8 * q + 7]);
+                    uint4 pk;
+                    pk.x = *reinterpret_cast<uint32_t *>(&h0);
+                    pk.y = *reinterpret_cast<uint32_t *>(&h1);
+                    pk.z = *reinterpret_cast<uint32_t *>(&h2);
+                    pk.w = *reinterpret_cast<uint32_t *>(&h3);
+                    dst[q] = pk;
+                }
+            }
+        }
+        if (write) a.gate[cl] = fminf(sqrtf(gsum / 256.f) / GATE_SIGMA, 1.f);
+        fence_before_sync();
+        __syncthreads();
+        if (abortFlag) break;
+    }
+    if (tid == 0) {
+        for (int s = 0; s < 2; s++)
+            if (issued[s] > consumed[s]) mbar_wait_bounded(&full[s], (uint32_t)issued[s] & 1);
+        if (abortFlag) atomicOr(a.err, ERR_SURROGATE_WAIT);
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after_sync();
+        tmem_dealloc(tmem, 256);
+    }
+}
+
+// ------------------------------------------------------------------ per-particle step
+
+struct StepArgs {
+    int eta, xi, sW, sRho;
+    double start, length, dti, tau0, survprob, sv, shoreLimit;
+    int upper, lower, horizontal;
+    int fallbackAll;  // run parameters outside the surrogate: every active particle falls back
+    int drift;        // driftModel == 1: drifting objects fall back
+    const float *u0, *v0, *w0, *z0, *u1, *v1, *w1, *z1;
+    const double *h, *depthIntervals;
+    const double2 *metric;
+    const int *dry;        // inclusive 2-D prefix sums of dry nodes, [(eta+1)][(xi+1)]
+    const __half *z;       // [nCL][256]
+    const float *gate;     // [nCL]
+    const uint8_t *weights;
+    uint32_t *fallback, *fallbackCount;
+    unsigned long long *runCount;
+};
+
+constexpr int STEP_THREADS = 320;
+constexpr size_t STEP_SMEM = (size_t)HID_KB * KBLOCK_A + RING * (size_t)KBLOCK_W + 1024;
+
+enum : int { ROW_NONE = 0, ROW_RUN = 1, ROW_FALLBACK = 2, ROW_EMPTY = 3 };
+
+__device__ __forceinline__ double bil_f(const float *f, size_t plane, int xi, int jI, int iI,
+                                        double jF, double iF) {
+    const float *p = f + plane + (size_t)jI * xi + iI;
+    const double f00 = p[0], f01 = p[1], f10 = p[xi], f11 = p[xi + 1];
+    return f00 * (1 - iF) * (1 - jF) + f10 * (1 - iF) * jF + f11 * iF * jF + f01 * iF * (1 - jF);
+}
+
+__device__ __forceinline__ double bil_d(const double *f, int xi, int jI, int iI, double jF, double iF) {
+    const double *p = f + (size_t)jI * xi + iI;
+    return p[0] * (1 - iF) * (1 - jF) + p[xi] * (1 - iF) * jF + p[xi + 1] * iF * jF + p[1] * iF * (1 - jF);
+}
+
+// End of nSub equal substeps of disp/nSub along one axis of [0, maximum): a particle leaving the
+// domain at substep m under repeated reflectDomain alternates its overshoot e and d - e.
+__device__ double pinned_axis(double x0, double disp, double nSub, double maximum, double &m) {
+    const double d = disp / nSub, end = x0 + disp, big = nSub + 1;
+    const bool up = end >= maximum, down = end < 0;
+    if (!up && !down) {
+        m = big;
+        return end;
+    }
+    double mm = up ? (d > 0 ? floor((maximum - x0) / d) + 1 : big) : (d < 0 ? floor(x0 / -d) + 1 : big);
+    mm = fmin(mm, big);
+    const double r = nSub - mm;
+    double e = up ? x0 + mm * d - maximum : -(x0 + mm * d);
+    e = fmax(e, 0.0);
+    if (fmod(r, 2.0) != 0.0) e = fmax(fabs(d) - e, 0.0);
+    double x = up ? maximum - e : e;
+    x = fmin(fmax(x, 0.0), nextafter(maximum, 0.0));
+    m = mm;
+    return x;
+}
+
+__device__ __forceinline__ int dry_in_box(const int *pre, int xi, int ja, int jb, int ia, int ib) {
+    const int w = xi + 1;
+    return pre[(jb + 1) * w + ib + 1] - pre[ja * w + ib + 1] - pre[(jb + 1) * w + ia] + pre[ja * w + ia];
+}
+
+__global__ void __launch_bounds__(STEP_THREADS, 1)
+    surrogate_step_kernel(const StepArgs a, ParticleSoA S, const MoveLaunch L) {
+    using namespace umma;
+    extern __shared__ uint8_t dynSmem[];
+    uint8_t *sA = align1024(dynSmem);
+    uint8_t *ring = sA + HID_KB * KBLOCK_A;
+    __shared__ __align__(8) uint64_t full[RING], empty[RING], aFull, accFull;
+    __shared__ uint32_t tmemSlot;
+    __shared__ int abortFlag, rowStop;
+    __shared__ float w1ps[HID * 4], b2s[HID], b3s[HID], w4s[3 * HID], b4s[4];
+    __shared__ float red[TILE * 3];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        for (int s = 0; s < RING; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&aFull, 1);
+        mbar_init(&accFull, 1);
+        abortFlag = 0;
+        rowStop = 0;
+        fence_barrier_init();
+    }
+    {
+        const float *w1p = reinterpret_cast<const float *>(a.weights + OFF_W1P);
+        const float *b2 = reinterpret_cast<const float *>(a.weights + OFF_B2);
+        const float *b3 = reinterpret_cast<const float *>(a.weights + OFF_B3);
+        const float *w4 = reinterpret_cast<const float *>(a.weights + OFF_W4);
+        const float *b4 = reinterpret_cast<const float *>(a.weights + OFF_B4);
+        for (int c = tid; c < HID * 4; c += STEP_THREADS) w1ps[c] = w1p[c];
+        for (int c = tid; c < HID; c += STEP_THREADS) {
+            b2s[c] = b2[c];
+            b3s[c] = b3[c];
+        }
+        for (int c = tid; c < 3 * HID; c += STEP_THREADS) w4s[c] = w4[c];
+        if (tid < 3) b4s[tid] = b4[tid];
+    }
+    if (warp == 9) tmem_alloc(&tmemSlot, 256);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = tmemSlot;
+    const long long nTiles = ((long long)L.count + TILE - 1) / TILE;
+    const uint32_t idesc = idesc_bf16(TILE, HID);
+
+    if (warp == 8) {
+        // ---------------------------------------------------------- weight producer
+        if (lane == 0) {
+            int issued[RING] = {-1, -1, -1};
+            uint32_t g = 0;
+            bool ok = true;
+            for (long long tile = blockIdx.x; tile < nTiles && ok; tile += gridDim.x) {
+                for (int b = 0; b < 2 * HID_KB && ok; b++, g++) {
+                    const uint32_t s = g % RING, n = g / RING;
+                    if (!mbar_wait(&empty[s], (n & 1) ^ 1, &abortFlag)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], KBLOCK_W);
+                    const uint8_t *src = a.weights + (b < HID_KB ? OFF_W2 + (size_t)b * KBLOCK_W
+                                                                 : OFF_W3 + (size_t)(b - HID_KB) * KBLOCK_W);
+                    bulk_g2s(ring + s * KBLOCK_W, src, KBLOCK_W, &full[s]);
+                    issued[s] = (int)n;
+                }
+            }
+            // copies still in flight land before the block exits
+            for (int s = 0; s < RING; s++)
+                if (issued[s] >= 0) mbar_wait_bounded(&full[s], (uint32_t)issued[s] & 1);
+        }
+        __syncwarp();
+    } else if (warp == 9) {
+        // ---------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            uint32_t g = 0;
+            bool ok = true;
+            for (long long tile = blockIdx.x; tile < nTiles && ok; tile += gridDim.x) {
+                for (int layer = 0; layer < 2 && ok; layer++) {
+                    if (!mbar_wait(&aFull, (uint32_t)layer, &abortFlag)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after_sync();
+                    for (int kb = 0; kb < HID_KB; kb++, g++) {
+                        const uint32_t s = g % RING, n = g / RING;
+                        if (!mbar_wait(&full[s], n & 1, &abortFlag)) {
+                            ok = false;
+                            break;
+                        }
+                        fence_after_sync();
+#pragma unroll
+                        for (int ks = 0; ks < 4; ks++)
+                            mma_bf16(tmem, desc_sw128(smem_u32(sA + kb * KBLOCK_A + ks * 32)),
+                                     desc_sw128(smem_u32(ring + s * KBLOCK_W + ks * 32)), idesc,
+                                     (kb | ks) != 0);
+                        mma_commit(&empty[s]);
+                    }
+                    mma_commit(&accFull);
+                }
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------------- rows (warps 0-7)
+        const int quarter = warp & 3, half = warp >> 2;
+        const int r = quarter * 32 + lane;
+        const uint32_t tlane = (uint32_t)(quarter * 32) << 16;
+        const int cBase = half * 128;
+        const double T0 = a.start, T1 = a.start + a.length;
+        const double kLower = -a.sW + 2;
+        for (long long tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
+            // ---- prologue: state, status, layer 1 from z
+            const long long n = tile * TILE + r;
+            int status = ROW_EMPTY;
+            uint32_t slot = 0;
+            double pj = 0, pi = 0, pk = 0, ptime = 0, phealth = 0, page = 0;
+            int jI = 0, iI = 0, kI = 0;
+            float jF = 0.f, iF = 0.f, kF = 0.f, a0 = 0.f;
+            long long cl = 0;
+            if (n < L.count) {
+                slot = L.order ? L.order[n] : (uint32_t)n;
+                pj = S.j[slot];
+                pi = S.i[slot];
+                pk = S.k[slot];
+                ptime = S.time[slot];
+                phealth = S.health[slot];
+                page = S.age[slot];
+                const int ptype = S.type[slot];
+                status = ROW_NONE;
+                if (phealth > 0 && ptime < T1) {
+                    const double fj = floor(pj), fi = floor(pi), ck = ceil(pk);
+                    const bool cellOk = fj >= 0 && fi >= 0 && fj + 1 < a.eta && fi + 1 < a.xi;
+                    if (a.fallbackAll || phealth < a.survprob || pk > 0 || pk < kLower ||
+                        (a.drift && ptype != 0) || !cellOk) {
+                        status = ROW_FALLBACK;
+                    } else {
+                        status = ROW_RUN;
+                        jI = (int)fj;
+                        iI = (int)fi;
+                        kI = (int)ck;
+                        jF = (float)(pj - fj);
+                        iF = (float)(pi - fi);
+                        kF = (float)(ck - pk);
+                        a0 = ptime > T0 ? (float)((ptime - T0) / a.length) : 0.f;
+                        cl = ((long long)jI * (a.xi - 1) + iI) * (a.sW - 1) + (kI + a.sW - 2);
+                    }
+                }
+            }
+            {
+                const uint4 *zrow = reinterpret_cast<const uint4 *>(a.z + (size_t)cl * HID + cBase);
+#pragma unroll 1
+                for (int q = 0; q < 16; q++) {
+                    uint4 out = make_uint4(0, 0, 0, 0);
+                    if (status == ROW_RUN) {
+                        const uint4 zz = __ldg(zrow + q);
+                        const __half2 *hz = reinterpret_cast<const __half2 *>(&zz);
+                        float h[8];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            const float2 f2 = __half22float2(hz[e]);
+                            h[2 * e] = f2.x;
+                            h[2 * e + 1] = f2.y;
+                        }
+#pragma unroll
+                        for (int e = 0; e < 8; e++) {
+                            const int c = cBase + q * 8 + e;
+                            const float* wp = w1ps + c * 4;
+                            float x = h[e] + wp[0] * jF + wp[1] * iF + wp[2] * kF + wp[3] * a0;
+                            h[e] = gelu_tanh(x);
+                        }
+                        out.x = pack_bf16(h[0], h[1]);
+                        out.y = pack_bf16(h[2], h[3]);
+                        out.z = pack_bf16(h[4], h[5]);
+                        out.w = pack_bf16(h[6], h[7]);
+                    }
+                    const int col = cBase + q * 8;
+                    *reinterpret_cast<uint4 *>(sA + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
+                }
+            }
+            fence_async_shared();
+            fence_before_sync();
+            named_sync(1, 256);
+            if (tid == 0) mbar_arrive(&aFull);
+            // ---- layer 2 epilogue: h2 = GELU(acc + b2) -> A
+            bool ok = mbar_wait(&accFull, 0, &abortFlag);
+            __syncwarp();
+            fence_after_sync();
+#pragma unroll 1
+            for (int t = 0; t < 4; t++) {
+                const int c0 = cBase + 32 * t;
+                float v[32];
+                tmem_ld32(tmem + tlane + (uint32_t)c0, v);
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    uint4 out;
+                    out.x = pack_bf16(gelu_tanh(v[8 * q + 0] + b2s[c0 + 8 * q + 0]), gelu_tanh(v[8 * q + 1] + b2s[c0 + 8 * q + 1]));
+                    out.y = pack_bf16(gelu_tanh(v[8 * q + 2] + b2s[c0 + 8 * q + 2]), gelu_tanh(v[8 * q + 3] + b2s[c0 + 8 * q + 3]));
+                    out.z = pack_bf16(gelu_tanh(v[8 * q + 4] + b2s[c0 + 8 * q + 4]), gelu_tanh(v[8 * q + 5] + b2s[c0 + 8 * q + 5]));
+                    out.w = pack_bf16(gelu_tanh(v[8 * q + 6] + b2s[c0 + 8 * q + 6]), gelu_tanh(v[8 * q + 7] + b2s[c0 + 8 * q + 7]));
+                    const int col = c0 + 8 * q;
+                    *reinterpret_cast<uint4 *>(sA + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
+                }
+            }
+            fence_async_shared();
+            fence_before_sync();
+            named_sync(1, 256);
+            if (tid == 0) mbar_arrive(&aFull);
+            // ---- layer 3 epilogue with layer 4 folded in
+            ok = mbar_wait(&accFull, 1, &abortFlag) && ok;
+            __syncwarp();
+            fence_after_sync();
+            float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+#pragma unroll 1
+            for (int t = 0; t < 4; t++) {
+                const int c0 = cBase + 32 * t;
+                float v[32];
+                tmem_ld32(tmem + tlane + (uint32_t)c0, v);
+#pragma unroll
+                for (int c = 0; c < 32; c++) {
+                    const float x = gelu_tanh(v[c] + b3s[c0 + c]);
+                    o0 = fmaf(x, w4s[c0 + c], o0);
+                    o1 = fmaf(x, w4s[HID + c0 + c], o1);
+                    o2 = fmaf(x, w4s[2 * HID + c0 + c], o2);
+                }
+            }
+            if (half == 1) {
+                red[r * 3 + 0] = o0;
+                red[r * 3 + 1] = o1;
+                red[r * 3 + 2] = o2;
+            }
+            fence_before_sync();
+            named_sync(1, 256);
+            if (half == 0) {
+                // ---- displacement, closures, state
+                long long concCell = -1;
+                int steps = 0;
+                bool run = false;
+                const bool write = ok && !abortFlag;
+                if (status == ROW_RUN && write) {
+                    const float gate = __ldg(a.gate + cl);
+                    const double y0 = (double)((o0 + red[r * 3 + 0] + b4s[0]) * gate);
+                    const double y1 = (double)((o1 + red[r * 3 + 1] + b4s[1]) * gate);
+                    const double y2 = (double)((o2 + red[r * 3 + 2] + b4s[2]) * gate);
+                    const double da0 = ptime > T0 ? (ptime - T0) / a.length : 0.0;
+                    const double amid = 0.5 * (da0 + 1.0), trem = (1.0 - da0) * a.length;
+                    const double nSub = fmax(1.0, ceil(trem / a.dti - 1e-9));
+                    const size_t plane = (size_t)a.eta * a.xi;
+                    const double djF = pj - jI, diF = pi - iI, dkF = (double)kI - pk;
+                    const size_t lr = (size_t)(kI + a.sRho - 1) * plane;
+                    const double ub = (1 - amid) * bil_f(a.u0, lr, a.xi, jI, iI, djF, diF) +
+                                      amid * bil_f(a.u1, lr, a.xi, jI, iI, djF, diF);
+                    const double vb = (1 - amid) * bil_f(a.v0, lr, a.xi, jI, iI, djF, diF) +
+                                      amid * bil_f(a.v1, lr, a.xi, jI, iI, djF, diF);
+                    const size_t lwU = (size_t)(kI + a.sW - 1) * plane, lwL = (size_t)(kI + a.sW - 2) * plane;
+                    const double wb =
+                        (1 - amid) * ((1 - dkF) * bil_f(a.w0, lwU, a.xi, jI, iI, djF, diF) +
+                                      dkF * bil_f(a.w0, lwL, a.xi, jI, iI, djF, diF)) +
+                        amid * ((1 - dkF) * bil_f(a.w1, lwU, a.xi, jI, iI, djF, diF) +
+                                dkF * bil_f(a.w1, lwL, a.xi, jI, iI, djF, diF));
+                    const double hc = bil_d(a.h, a.xi, jI, iI, djF, diF) +
+                                      (1 - amid) * bil_f(a.z0, 0, a.xi, jI, iI, djF, diF) +
+                                      amid * bil_f(a.z1, 0, a.xi, jI, iI, djF, diF);
+                    const double2 met = a.metric[(size_t)jI * a.xi + iI];
+                    const double zdist = hc * a.depthIntervals[kI + a.sW - 2];
+                    const double dI = (ub * trem + OUT_H * y0) / met.x;
+                    const double dJ = (vb * trem + OUT_H * y1) / met.y;
+                    const double dK = ((wb + a.sv) * trem + OUT_V * y2) / zdist;
+                    double mj, mi;
+                    double jn = pinned_axis(pj, dJ, nSub, (double)(a.eta - 1), mj);
+                    double in = pinned_axis(pi, dI, nSub, (double)(a.xi - 1), mi);
+                    const double m = fmin(mj, mi);
+                    const bool crossed = m <= nSub;
+                    bool dead = false;
+                    if (a.horizontal == 1 && crossed) {  // constraint: the last in-domain substep
+                        const double keep = (m - 1) / nSub;
+                        jn = pj + keep * dJ;
+                        in = pi + keep * dI;
+                    } else if (a.horizontal == 2 && crossed) {  // kill
+                        dead = true;
+                        jn = pj;
+                        in = pi;
+                    } else if (a.horizontal == 1) {
+                        jn = pj + dJ;
+                        in = pi + dI;
+                    }
+                    double kn = pk + dK;
+                    if (kn > 0) {
+                        if (a.upper == 1) kn = 0;
+                        else if (a.upper == 2) dead = true;
+                        else if (a.upper == 3) kn = -kn;
+                    }
+                    if (kn < kLower) {
+                        if (a.lower == 1) kn = kLower;
+                        else if (a.lower == 2) dead = true;
+                        else if (a.lower == 3) kn = 2.0 * kLower - kn;
+                    }
+                    int ja = (int)floor(fmin(pj, jn)), jb = (int)floor(fmax(pj, jn)) + 1;
+                    int ia = (int)floor(fmin(pi, in)), ib = (int)floor(fmax(pi, in)) + 1;
+                    ja = ja < 0 ? 0 : (ja > a.eta - 1 ? a.eta - 1 : ja);
+                    jb = jb < 0 ? 0 : (jb > a.eta - 1 ? a.eta - 1 : jb);
+                    ia = ia < 0 ? 0 : (ia > a.xi - 1 ? a.xi - 1 : ia);
+                    ib = ib < 0 ? 0 : (ib > a.xi - 1 ? a.xi - 1 : ib);
+                    if (dry_in_box(a.dry, a.xi, ja, jb, ia, ib) > 0) {
+                        status = ROW_FALLBACK;
+                    } else {
+                        const double age = page + trem;
+                        const double health = exp(-age / a.tau0);
+                        dead = dead || health < a.survprob;
+                        S.j[slot] = jn;
+                        S.i[slot] = in;
+                        S.k[slot] = kn;
+                        S.age[slot] = age;
+                        S.health[slot] = dead ? -1.0 : health;
+                        ParticleState p;
+                        p.j = jn;
+                        p.i = in;
+                        p.k = kn;
+                        p.health = dead ? -1.0 : health;
+                        if (L.conc) concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
+                        steps = (int)nSub;
+                        run = true;
+                    }
+                } else if (status == ROW_NONE && write && L.conc) {
+                    ParticleState p;
+                    p.j = pj;
+                    p.i = pi;
+                    p.k = pk;
+                    p.health = phealth;
+                    concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
+                }
+                if (status == ROW_FALLBACK && write) {
+                    const uint32_t at = atomicAdd(a.fallbackCount, 1u);
+                    a.fallback[at] = slot;
+                }
+                __syncwarp();
+                if (L.steps) warp_sum_steps(L.steps, steps);
+                if (L.conc) warp_count(L.conc, concCell);
+                const unsigned ran = __ballot_sync(0xffffffffu, run);
+                if (lane == 0 && ran) atomicAdd(a.runCount, (unsigned long long)__popc(ran));
+            }
+            // ---- uniform stop decision of the row warps
+            named_sync(1, 256);
+            if (tid == 0) rowStop = abortFlag;
+            named_sync(1, 256);
+            if (rowStop) break;
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 9) {
+        fence_after_sync();
+        tmem_dealloc(tmem, 256);
+    }
+    if (tid == 0 && abortFlag) atomicOr(L.err, ERR_SURROGATE_WAIT);
+}
+
+// ------------------------------------------------------------------ dry-node prefix sums
+
+__global__ void dry_rows_kernel(const double *mask, const double *h, double shore, int eta, int xi,
+                                int *pre) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > eta) return;
+    const int w = xi + 1;
+    int run = 0;
+    pre[j * w] = 0;
+    for (int i = 0; i < xi; i++) {
+        if (j > 0) {
+            const size_t n = (size_t)(j - 1) * xi + i;
+            run += ((mask && mask[n] == 0.0) || h[n] <= shore) ? 1 : 0;
+        }
+        pre[j * w + i + 1] = run;
+    }
+}
+
+__global__ void dry_cols_kernel(int eta, int xi, int *pre) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > xi) return;
+    const int w = xi + 1;
+    int run = 0;
+    for (int j = 0; j <= eta; j++) {
+        run += pre[j * w + i];
+        pre[j * w + i] = run;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host side
+
+size_t surrogate_packed_bytes() { return PACKED_BYTES; }
+
+size_t surrogate_parameter_count() {
+    return (size_t)HID * N_INPUT + HID + 2 * ((size_t)HID * HID + HID) + 3 * HID + 3;
+}
+
+void surrogate_pack(const float *flat, uint8_t *out) {
+    memset(out, 0, PACKED_BYTES);
+    const float *w1 = flat;
+    const float *b1 = w1 + HID * N_INPUT;
+    const float *w2 = b1 + HID;
+    const float *b2 = w2 + HID * HID;
+    const float *w3 = b2 + HID;
+    const float *b3 = w3 + HID * HID;
+    const float *w4 = b3 + HID;
+    const float *b4 = w4 + 3 * HID;
+    auto put = [&](size_t base, int rows, int k, float v) {
+        __nv_bfloat16 b = __float2bfloat16_rn(v);
+        memcpy(out + base + (size_t)(k / 64) * KBLOCK_W + umma::sw128_offset(rows, k % 64), &b, 2);
+    };
+    for (int n = 0; n < HID; n++) {
+        for (int k = 0; k < N_STENCIL; k++) put(OFF_W1, n, k, w1[n * N_INPUT + k]);
+        for (int k = 0; k < HID; k++) {
+            put(OFF_W2, n, k, w2[n * HID + k]);
+            put(OFF_W3, n, k, w3[n * HID + k]);
+        }
+    }
+    float *fb1 = reinterpret_cast<float *>(out + OFF_B1), *fb2 = reinterpret_cast<float *>(out + OFF_B2);
+    float *fb3 = reinterpret_cast<float *>(out + OFF_B3), *fw1p = reinterpret_cast<float *>(out + OFF_W1P);
+    float *fw4 = reinterpret_cast<float *>(out + OFF_W4), *fb4 = reinterpret_cast<float *>(out + OFF_B4);
+    for (int n = 0; n < HID; n++) {
+        fb1[n] = b1[n];
+        fb2[n] = b2[n];
+        fb3[n] = b3[n];
+        for (int e = 0; e < 4; e++) fw1p[n * 4 + e] = w1[n * N_INPUT + N_STENCIL + e];
+    }
+    for (int o = 0; o < 3 * HID; o++) fw4[o] = w4[o];
+    for (int o = 0; o < 3; o++) fb4[o] = b4[o];
+}
+
+long long surrogate_cell_levels(int eta, int xi, int sW) {
+    return (long long)(eta - 1) * (xi - 1) * (sW - 1);
+}
+
+cudaError_t surrogate_cells(int eta, int xi, int sW, int sRho, const FrameDevice &f0,
+                            const FrameDevice &f1, const uint8_t *weights, __half *z, float *gate,
+                            int *err, int smCount, cudaStream_t stream) {
+    CellArgs a;
+    a.eta = eta;
+    a.xi = xi;
+    a.sW = sW;
+    a.sRho = sRho;
+    a.nCL = surrogate_cell_levels(eta, xi, sW);
+    a.u0 = f0.u;
+    a.v0 = f0.v;
+    a.w0 = f0.w;
+    a.u1 = f1.u;
+    a.v1 = f1.v;
+    a.w1 = f1.w;
+    a.weights = weights;
+    a.z = z;
+    a.gate = gate;
+    a.err = err;
+    if (a.nCL <= 0) return cudaSuccess;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(surrogate_cell_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CELL_SMEM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    long long tiles = (a.nCL + TILE - 1) / TILE;
+    int blocks = (int)(tiles < smCount ? tiles : smCount);
+    surrogate_cell_kernel<<<blocks, 128, CELL_SMEM, stream>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const MoveLaunch &L,
+                           int smCount, cudaStream_t stream) {
+    if (L.count <= 0) return cudaSuccess;
+    StepArgs a;
+    a.eta = s.eta;
+    a.xi = s.xi;
+    a.sW = s.sW;
+    a.sRho = s.sRho;
+    a.start = s.start;
+    a.length = s.length;
+    a.dti = s.cfg.dti;
+    a.tau0 = s.cfg.tau0;
+    a.survprob = s.cfg.survprob;
+    a.sv = s.cfg.sv;
+    a.shoreLimit = s.cfg.shoreLimit;
+    a.upper = s.cfg.upperClosure;
+    a.lower = s.cfg.lowerClosure;
+    a.horizontal = s.cfg.horizontalClosure;
+    a.fallbackAll = s.fallbackAll;
+    a.drift = s.cfg.driftModel == 1;
+    a.u0 = s.f0.u;
+    a.v0 = s.f0.v;
+    a.w0 = s.f0.w;
+    a.z0 = s.f0.zeta;
+    a.u1 = s.f1.u;
+    a.v1 = s.f1.v;
+    a.w1 = s.f1.w;
+    a.z1 = s.f1.zeta;
+    a.h = s.h;
+    a.depthIntervals = s.depthIntervals;
+    a.metric = s.metric;
+    a.dry = s.dry;
+    a.z = s.z;
+    a.gate = s.gate;
+    a.weights = s.weights;
+    a.fallback = s.fallback;
+    a.fallbackCount = s.fallbackCount;
+    a.runCount = s.runCount;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(surrogate_step_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)STEP_SMEM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    long long tiles = ((long long)L.count + TILE - 1) / TILE;
+    int blocks = (int)(tiles < smCount ? tiles : smCount);
+    surrogate_step_kernel<<<blocks, STEP_THREADS, STEP_SMEM, stream>>>(a, S, L);
+    return cudaGetLastError();
+}
+
+cudaError_t surrogate_dry_prefix(const double *mask, const double *h, double shore, int eta, int xi,
+                                 int *pre, cudaStream_t stream) {
+    dry_rows_kernel<<<(eta + 1 + 127) / 128, 128, 0, stream>>>(mask, h, shore, eta, xi, pre);
+    dry_cols_kernel<<<(xi + 1 + 127) / 128, 128, 0, stream>>>(eta, xi, pre);
+    return cudaGetLastError();
+}
+
+}  // namespace wb

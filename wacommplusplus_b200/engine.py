@@ -35,7 +35,8 @@ class Engine:
 
     Options (defaults in brackets): semantics ["host"|"device"], arithmetic ["fp32"|"reference"],
     storage ["fp32"|"fp16"|"bf16"], rng ["reference"|"philox"], block_size [256],
-    substeps_per_launch [0 = whole interval], sort_by_cell [True], fuse_concentration [True].
+    substeps_per_launch [0 = whole interval], sort_by_cell [True], fuse_concentration [True],
+    launch_shape [2], surrogate [False] (needs set_surrogate).
     """
 
     _SEM = {"host": 0, "device": 1}
@@ -92,6 +93,27 @@ class Engine:
                 value = table[key][value]
             setattr(o, key, int(value))
         self._check(self._lib.wacomm_b200_set_options(self._ctx, ctypes.byref(o)))
+
+    def set_surrogate(self, weights=None):
+        """Uploads the surrogate's weights: a name -> array mapping (surrogate.PARAMETERS), a
+        path to a weights file, or None for the weights shipped with the package."""
+        from . import surrogate
+        if weights is None or isinstance(weights, str):
+            weights = surrogate.load_weights(weights or surrogate.DEFAULT_WEIGHTS)
+        flat = surrogate.flatten(weights)
+        self._surrogate = flat
+        self._check(self._lib.wacomm_b200_set_surrogate(self._ctx, flat.ctypes.data_as(_fp), len(flat)))
+
+    def surrogate_stats(self):
+        """dict of the last surrogate interval: particles moved by the surrogate, particles handed
+        to the FP32 step, device ms of the per-cell and per-particle kernels."""
+        run, fallback = ctypes.c_size_t(), ctypes.c_size_t()
+        cell_ms, step_ms = ctypes.c_float(), ctypes.c_float()
+        self._check(self._lib.wacomm_b200_last_surrogate_stats(
+            self._ctx, ctypes.byref(run), ctypes.byref(fallback), ctypes.byref(cell_ms),
+            ctypes.byref(step_ms)))
+        return {"run": run.value, "fallback": fallback.value, "cell_ms": cell_ms.value,
+                "step_ms": step_ms.value}
 
     def set_config(self, cfg):
         assert isinstance(cfg, config_data)

@@ -8,7 +8,10 @@ with random off) by one evaluation of a small MLP per particle:
   the interval already elapsed at activation (4 values);
 * layers: 388 -> 256 -> 256 -> 256 -> 3, GELU (tanh form) between them;
 * output: the correction, in metres, to the displacement that the velocity interpolated at the
-  start position and the interval's mid time would give over the remaining time.
+  start position and the interval's mid time would give over the remaining time, scaled by a
+  uniformity gate: min(1, sigma / GATE_SIGMA), sigma the RMS deviation of the stencil's u and v
+  from their value at the cell's own corner (per record and field). In a spatially uniform flow
+  the start-point displacement is exact and the gate makes the correction exactly zero.
 
 The displacement is turned into grid units with the start cell's metric (host rules,
 Particle.cpp:548-579), then the domain-edge closures are applied in closed form for the number of
@@ -36,6 +39,8 @@ N_OUTPUT = 3
 U_SCALE = 1.0             # m/s per unit of the u, v features
 W_SCALE = 1.0e-3          # m/s per unit of the w features
 OUT_SCALE = (100.0, 100.0, 1.0)   # metres per unit of the three outputs (east, north, up)
+GATE_SIGMA = 0.01         # m/s: stencil non-uniformity at which the correction is fully on
+GATE_REF = (1 * 4 + 1) * 4 + 1    # position of the cell's own corner (level c=1, row a=1, column b=1) in a 64-block
 EARTH_RADIUS = 6371000.0
 
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "surrogate_weights.npz")
@@ -153,12 +158,24 @@ def stencil_features(u0, v0, w0, u1, v1, w1, jI, iI, kI):
     return torch.cat(out, dim=1)
 
 
+def uniformity_gate(stencil):
+    """[n] gate in [0, 1] of stencil features [n, 384]: RMS over the u and v blocks of both records
+    (features 0-127 and 192-319) of the deviation from each block's value at GATE_REF, in m/s,
+    divided by GATE_SIGMA and capped at 1."""
+    torch = _torch()
+    blocks = [stencil[:, b * 64:(b + 1) * 64] for b in (0, 1, 3, 4)]
+    total = sum(((x - x[:, GATE_REF:GATE_REF + 1]) ** 2).sum(1) for x in blocks)
+    sigma = torch.sqrt(total / 256.0) * U_SCALE
+    return torch.clamp(sigma / GATE_SIGMA, max=1.0)
+
+
 def mlp(weights, stencil, particle, emulate_kernel=True):
     """[n, 3] outputs of the MLP from stencil [n, 384] and particle [n, 4] features.
 
     With emulate_kernel the operand roundings of the CUDA path are applied: stencil and the
     stencil part of w1 in bfloat16 (the per-cell GEMM), the per-cell partial sum in float16,
-    hidden activations and w2, w3 in bfloat16; w4 and the particle part of w1 stay float32."""
+    hidden activations and w2, w3 in bfloat16; w4 and the particle part of w1 stay float32.
+    The outputs are multiplied by the uniformity gate of the stencil."""
     torch = _torch()
     dev = stencil.device
     W = {k: torch.as_tensor(v, device=dev) for k, v in weights.items()}
@@ -169,11 +186,11 @@ def mlp(weights, stencil, particle, emulate_kernel=True):
         h = bf16_round(gelu(z + particle @ w1p.T))
         h = bf16_round(gelu(h @ bf16_round(W["w2"]).T + W["b2"]))
         h = gelu(h @ bf16_round(W["w3"]).T + W["b3"])
-        return h @ W["w4"].T + W["b4"]
+        return (h @ W["w4"].T + W["b4"]) * uniformity_gate(stencil)[:, None]
     h = gelu(stencil @ w1s.T + particle @ w1p.T + W["b1"])
     h = gelu(h @ W["w2"].T + W["b2"])
     h = gelu(h @ W["w3"].T + W["b3"])
-    return h @ W["w4"].T + W["b4"]
+    return (h @ W["w4"].T + W["b4"]) * uniformity_gate(stencil)[:, None]
 
 
 def _bilinear(field, level, jI, iI, jF, iF):

@@ -140,16 +140,19 @@ class Net:
         w["w4"] *= 0.1
         self.p = {k: torch.tensor(v, device="cuda", requires_grad=True) for k, v in w.items()}
 
-    def forward(self, torch, S, P):
+    def forward(self, torch, S, P, G):
         p = self.p
         h = sg.gelu(S @ p["w1"][:, :sg.N_STENCIL].T + P @ p["w1"][:, sg.N_STENCIL:].T + p["b1"])
         h = sg.gelu(h @ p["w2"].T + p["b2"])
         h = sg.gelu(h @ p["w3"].T + p["b3"])
-        return h @ p["w4"].T + p["b4"]
+        return (h @ p["w4"].T + p["b4"]) * G[:, None]
 
 
 def train(torch, S, P, R, epochs, batch, lr, seed):
     net = Net(torch, seed)
+    G = torch.cat([sg.uniformity_gate(S[c:c + (1 << 20)].float()) for c in range(0, len(S), 1 << 20)])
+    print(f"  gate: {float((G < 1).float().mean()):.3f} of segments below 1, "
+          f"{float((G == 0).float().mean()):.3f} at 0", flush=True)
     opt = torch.optim.Adam(net.p.values(), lr=lr)
     n = len(S)
     steps = epochs * (n // batch)
@@ -165,15 +168,15 @@ def train(torch, S, P, R, epochs, batch, lr, seed):
         for b in range(len(perm) // batch):
             ix = perm[b * batch:(b + 1) * batch]
             with torch.autocast("cuda", dtype=torch.bfloat16):
-                y = net.forward(torch, S[ix].float(), P[ix])
+                y = net.forward(torch, S[ix].float(), P[ix], G[ix])
             loss = torch.mean((y.float() - R[ix]) ** 2)
             opt.zero_grad(set_to_none=True)
             loss.backward()
             opt.step()
             sched.step()
-            tot += float(loss)
+            tot += float(loss.detach())
         with torch.no_grad():
-            y = net.forward(torch, S[hold].float(), P[hold])
+            y = net.forward(torch, S[hold].float(), P[hold], G[hold])
             val = torch.mean((y - R[hold]) ** 2).item()
             base = torch.mean(R[hold] ** 2).item()
         print(f"  epoch {epoch}: train {tot / max(1, len(perm) // batch):.4g} held-out {val:.4g} "
@@ -181,12 +184,20 @@ def train(torch, S, P, R, epochs, batch, lr, seed):
     return {k: v.detach().float().cpu().numpy() for k, v in net.p.items()}
 
 
-def evaluate(weights, n_particles=32768, hours=24, seed=1):
+def evaluate(weights, n_particles=32768, hours=24, seed=1, realistic=False):
     """Great-circle error (metres) after `hours` of the surrogate (PyTorch reference) against the
-    reference-arithmetic kernel on the analytic precision grid; prints and returns the stats."""
+    reference-arithmetic kernel, on the analytic precision grid or on a realistic flow window
+    without land; prints and returns the stats."""
     cfg = training_config()
-    win = syn.config1_window(n_frames=hours + 1)
-    start = syn.uniform_particles(n_particles, win.eta, win.xi, seed=seed, time=win.times[0])
+    if realistic:
+        win = syn.RealisticForcing(eta=256, xi=256, s_rho=12, n_frames=hours + 1, seed=4242,
+                                   dlon=0.0015, dlat=0.0015, land_fraction=0.0,
+                                   water_border=0).window()
+        start = segment_particles(np.random.default_rng(seed), win, 0, n_particles)
+        start["time"] = win.times[0]
+    else:
+        win = syn.config1_window(n_frames=hours + 1)
+        start = syn.uniform_particles(n_particles, win.eta, win.xi, seed=seed, time=win.times[0])
     exact = Engine(0, arithmetic="reference")
     exact.set_config(cfg)
     exact.load_window(win)
@@ -210,7 +221,8 @@ def evaluate(weights, n_particles=32768, hours=24, seed=1):
     err = sg.geo_error_m(win, cur, truth)
     stats = dict(mean=float(err.mean()), p99=float(np.quantile(err, 0.99)), max=float(err.max()),
                  fallbacks=fallbacks)
-    print(f"analytic grid, {hours} h, {n_particles} particles: error mean {stats['mean']:.2f} m, "
+    print(f"{'realistic flow' if realistic else 'analytic grid'}, {hours} h, {n_particles} particles: "
+          f"error mean {stats['mean']:.2f} m, "
           f"p99 {stats['p99']:.2f} m, max {stats['max']:.2f} m, fallback particle-intervals "
           f"{fallbacks}", flush=True)
     return stats
@@ -223,7 +235,7 @@ def main():
     ap.add_argument("--uniform", type=int, default=48)
     ap.add_argument("--frames", type=int, default=25)
     ap.add_argument("--per-interval", type=int, default=250000)
-    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--epochs", type=int, default=20)
     ap.add_argument("--batch", type=int, default=16384)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=7)
@@ -231,6 +243,7 @@ def main():
     args = ap.parse_args()
     if args.evaluate_only:
         evaluate(sg.load_weights(args.out))
+        evaluate(sg.load_weights(args.out), realistic=True)
         return
     import torch
     cfg = training_config()
@@ -246,6 +259,7 @@ def main():
     sg.save_weights(args.out, weights, segments=len(S), epochs=args.epochs, seed=args.seed)
     print(f"weights written to {args.out}")
     evaluate(weights)
+    evaluate(weights, realistic=True)
 
 
 if __name__ == "__main__":
