@@ -10,7 +10,11 @@ interval of every particle. Synthetic, seeded inputs stand in for the unavailabl
 
 Prints one JSON line (rank 0). `value` is device-timed with the particles resident in HBM;
 `e2e` moves the same particles through the public host-buffer entry point with the copies in the
-timed region; `cpu_baseline` times the reference's own CPU path on a bounded sample.
+timed region; `cpu_baseline` times the reference's own CPU path on a bounded sample. `surrogate`
+is the second arm of the metric: the same workload with FP16 forcing storage and the learned
+surrogate (tcgen05 MLP per particle-interval), device-timed the same way, with its position error
+after 24 hours against the FP64 reference-arithmetic kernel on a 1,048,576-particle subset and its
+tensor-core roofline.
 """
 import argparse
 import json
@@ -29,13 +33,17 @@ sys.path.insert(0, ROOT)
 B_ALG = 118.0  # algorithmic bytes per particle-step: one read + one write of the 59-byte state
 
 
-def measured_peaks():
+SURROGATE_FLOP = 2 * 2 * 256 * 256  # tensor-core FLOPs per particle-interval: layers 2 and 3
+
+
+def measured_peaks(key="hbm_gbs", fallback=6650.0):
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
         with open(path) as fh:
             data = json.load(fh)
-        return float(data["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        if key in data:
+            return float(data[key]), "measured"
+    return fallback, "fallback"
 
 
 def profile_traffic():
@@ -179,6 +187,87 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, dist):
+    """The FP16+surrogate arm: device-timed throughput on the same workload, the 24-hour error
+    against the FP64 reference-arithmetic kernel on a subset (rank 0), and the tensor roofline of
+    the per-particle kernel."""
+    import torch
+    from wacommplusplus_b200.engine import Engine
+    from wacommplusplus_b200 import surrogate as sg
+
+    engine = Engine(local_rank, arithmetic="fp32", storage="fp16", surrogate=1)
+    engine.set_config(cfg)
+    engine.load_window(win)
+    engine.set_surrogate()
+    engine.set_particles(particles)
+    n_intervals = win.T - 1
+    for s in range(args.warmup):
+        engine.move_interval(s % n_intervals)
+        engine.stats()
+    ext = torch.cuda.ExternalStream(engine.stream)
+    barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(ext)
+    steps_total, launches, step_ms, cell_ms, run, fallback = 0.0, 0, [], [], 0, 0
+    for s in range(args.steps):
+        engine.move_interval((args.warmup + s) % n_intervals)
+        st = engine.stats()
+        ss = engine.surrogate_stats()
+        steps_total += st["particle_steps"]
+        launches += st["launches"]
+        step_ms.append(ss["step_ms"])
+        cell_ms.append(ss["cell_ms"])
+        run += ss["run"]
+        fallback += ss["fallback"]
+    end.record(ext)
+    torch.cuda.synchronize()
+    barrier()
+    elapsed_ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([elapsed_ms, steps_total], dtype=torch.float64, device="cuda")
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        elapsed_ms, steps_total = float(mx[0]), float(t[1])
+    engine.close()
+    kernel_ms = statistics.mean(step_ms)
+    per_launch_run = run / args.steps
+    achieved = per_launch_run * SURROGATE_FLOP / (kernel_ms / 1000.0) / 1e12
+    peak, peak_kind = measured_peaks("bf16_tflops", 1590.0)
+    out = {"value": steps_total / (elapsed_ms / 1000.0), "unit": "particle-steps/s",
+           "ms_per_step": elapsed_ms / args.steps, "storage": "fp16",
+           "moved_by_surrogate_per_step": per_launch_run, "fallback_per_step": fallback / args.steps,
+           "gpu_launches": launches,
+           "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak, "peak_source": peak_kind,
+                        "kernel": "surrogate_step_kernel", "kernel_ms": kernel_ms,
+                        "flop_per_particle_interval": SURROGATE_FLOP,
+                        "cell_kernel_ms": statistics.mean(cell_ms), "traffic": None}}
+    if rank == 0:
+        n = min(len(particles), 1 << 20)
+        sub = particles[:n].copy()
+        s_eng = Engine(local_rank, arithmetic="fp32", storage="fp16", surrogate=1)
+        x_eng = Engine(local_rank, arithmetic="reference")
+        for e in (s_eng, x_eng):
+            e.set_config(cfg)
+            e.load_window(win)
+            e.set_particles(sub)
+        s_eng.set_surrogate()
+        hours = min(24, n_intervals)
+        for t in range(hours):
+            s_eng.move_interval(t)
+            x_eng.move_interval(t)
+        err = sg.geo_error_m(win, s_eng.get_particles(), x_eng.get_particles())
+        s_eng.close()
+        x_eng.close()
+        err = err[np.isfinite(err)]
+        out["error_m"] = {"mean": float(err.mean()), "p99": float(np.quantile(err, 0.99)),
+                          "max": float(err.max()), "hours": hours, "particles": n,
+                          "against": "FP64 reference-arithmetic kernel (parity-pinned to the oracle)"}
+    return out
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -190,6 +279,7 @@ def main():
     parser.add_argument("--arithmetic", default="fp32", choices=["fp32", "reference"])
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-cpu", action="store_true")
+    parser.add_argument("--no-surrogate", action="store_true")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -305,6 +395,10 @@ def main():
                "h2d_bytes_per_step": n * 64 + frame_bytes, "d2h_bytes_per_step": n * 64,
                "timing": "wall clock around K steps of upload_frame + move_interval_host"}
 
+    surrogate = None
+    if not args.no_surrogate:
+        surrogate = surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, dist)
+
     if rank == 0:
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
@@ -320,6 +414,7 @@ def main():
                        "l2": "inputs larger than L2 (particle state 1 GiB per GPU)",
                        "parallelism": f"particle shards x{world}, no data-path collective"},
             "roofline": roofline,
+            "surrogate": surrogate,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
