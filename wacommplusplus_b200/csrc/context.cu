@@ -92,9 +92,10 @@ struct wacomm_b200_context {
     uint8_t *dSurrogate = nullptr;  // packed weights
     bool hasSurrogate = false;
     __half *dZ = nullptr;           // per-cell-level layer-1 sums [cell-levels][256]
-    float *dGate = nullptr;         // per-cell-level uniformity gate
+    void *dCorners = nullptr;       // per-cell-level corner records (forcing, metric, gate)
     size_t zCap = 0;                // cell-levels held
     int zT0 = -1, zT1 = -1;         // forcing pair z was computed for
+    int zSemantics = -1;            // metric rules of the corner records
     int *dDry = nullptr;            // dry-node prefix sums
     size_t dryCap = 0;
     double dryShore = NAN;
@@ -491,23 +492,24 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     // layer 1 per cell-level
     const long long nCL = surrogate_cell_levels(ctx->eta, ctx->xi, ctx->sW);
     CUDA_TRY(ctx, cudaEventRecord(ctx->evCell0, ctx->stream));
-    if (ctx->zT0 != P.t0 || ctx->zT1 != P.t1) {
+    if (ctx->zT0 != P.t0 || ctx->zT1 != P.t1 || ctx->zSemantics != ctx->metricSemantics) {
         if ((size_t)nCL > ctx->zCap) {
             cudaFree(ctx->dZ);
-            cudaFree(ctx->dGate);
+            cudaFree(ctx->dCorners);
             ctx->dZ = nullptr;
-            ctx->dGate = nullptr;
+            ctx->dCorners = nullptr;
             ctx->zCap = 0;
             CUDA_TRY(ctx, cudaMalloc(&ctx->dZ, (size_t)nCL * 256 * sizeof(__half)));
-            CUDA_TRY(ctx, cudaMalloc(&ctx->dGate, (size_t)nCL * sizeof(float)));
+            CUDA_TRY(ctx, cudaMalloc(&ctx->dCorners, (size_t)nCL * surrogate_corner_bytes()));
             ctx->zCap = (size_t)nCL;
         }
         CUDA_TRY(ctx, surrogate_cells(ctx->eta, ctx->xi, ctx->sW, ctx->sRho, frame_of(a), frame_of(b),
-                                      ctx->dSurrogate, ctx->dZ, ctx->dGate, ctx->dErr, ctx->smCount,
-                                      ctx->stream));
+                                      ctx->dH, ctx->dDepth, ctx->dMetric, ctx->dSurrogate, ctx->dZ,
+                                      ctx->dCorners, ctx->dErr, ctx->smCount, ctx->stream));
         launches++;
         ctx->zT0 = P.t0;
         ctx->zT1 = P.t1;
+        ctx->zSemantics = ctx->metricSemantics;
     }
     CUDA_TRY(ctx, cudaEventRecord(ctx->evCell1, ctx->stream));
     // work order and fallback list
@@ -537,14 +539,9 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     const bool diffuse = ctx->cfg.random && (P.direction > 0 || ctx->cfg.backwardDiffusion);
     st.fallbackAll = diffuse || P.direction < 0 || P.elapsed0 != 0 || P.length <= 0 ||
                      ctx->cfg.leewayJibeProbabilityHourly > 0;
-    st.f0 = frame_of(a);
-    st.f1 = frame_of(b);
-    st.h = ctx->dH;
-    st.depthIntervals = ctx->dDepth;
-    st.metric = ctx->dMetric;
     st.dry = ctx->dDry;
     st.z = ctx->dZ;
-    st.gate = ctx->dGate;
+    st.corners = ctx->dCorners;
     st.weights = ctx->dSurrogate;
     st.fallback = ctx->dFallback;
     st.fallbackCount = reinterpret_cast<uint32_t *>(ctx->dSurrCounts);
@@ -694,7 +691,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dConc);
     cudaFree(ctx->dSurrogate);
     cudaFree(ctx->dZ);
-    cudaFree(ctx->dGate);
+    cudaFree(ctx->dCorners);
     cudaFree(ctx->dDry);
     cudaFree(ctx->dFallback);
     cudaFree(ctx->dSurrCounts);

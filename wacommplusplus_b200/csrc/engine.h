@@ -120,33 +120,31 @@ cudaError_t geo_positions(const ParticleSoA &S, int n, int eta, int xi, int sW, 
 
 // surrogate.cu -----------------------------------------------------------------------------
 
-// One surrogate interval: grid, interval, run parameters, the bracketing records (FP32 reference
-// layout), the static grid tables, the per-cell layer-1 sums and gate, the packed weights and the
-// fallback outputs.
+// One surrogate interval: grid, interval, run parameters, the dry-node table, the per-cell layer-1
+// sums and corner records, the packed weights and the fallback outputs.
 struct SurrogateStep {
     int eta, xi, sW, sRho;
     double start, length;
     wacomm_b200_config cfg;
     int fallbackAll;
-    FrameDevice f0, f1;
-    const double *h, *depthIntervals;
-    const double2 *metric;
     const int *dry;
     const __half *z;
-    const float *gate;
+    const void *corners;  // per-cell-level corner records (surrogate_corner_bytes each)
     const uint8_t *weights;
     uint32_t *fallback, *fallbackCount;
     unsigned long long *runCount;
 };
 
 size_t surrogate_packed_bytes();
+size_t surrogate_corner_bytes();
 size_t surrogate_parameter_count();
 // Packs the flat FP32 parameters (w1 [256][388], b1, w2 [256][256], b2, w3, b3, w4 [3][256], b4)
 // into the device image: BF16 swizzled K-blocks of the GEMM weights, FP32 vectors.
 void surrogate_pack(const float *flat, uint8_t *out);
 long long surrogate_cell_levels(int eta, int xi, int sW);
 cudaError_t surrogate_cells(int eta, int xi, int sW, int sRho, const FrameDevice &f0,
-                            const FrameDevice &f1, const uint8_t *weights, __half *z, float *gate,
+                            const FrameDevice &f1, const double *h, const double *depthIntervals,
+                            const double2 *metric, const uint8_t *weights, __half *z, void *corners,
                             int *err, int smCount, cudaStream_t stream);
 cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const MoveLaunch &L,
                            int smCount, cudaStream_t stream);

@@ -38,7 +38,6 @@ constexpr uint32_t KBLOCK_A = TILE * 128;  // 16 KB: 128 rows x 64 BF16
 constexpr uint32_t KBLOCK_W = HID * 128;   // 32 KB: 256 rows x 64 BF16
 constexpr int CELL_KB = N_STENCIL / 64;    // 6
 constexpr int HID_KB = HID / 64;           // 4
-constexpr int RING = 3;
 constexpr float W_FEATURE = 1000.f;        // 1 / (w feature scale, m/s)
 constexpr float OUT_H = 100.f, OUT_V = 1.f;
 constexpr float GATE_SIGMA = 0.01f;
@@ -56,11 +55,13 @@ constexpr size_t OFF_W4 = OFF_W1P + 4096;
 constexpr size_t OFF_B4 = OFF_W4 + 3072;
 constexpr size_t PACKED_BYTES = OFF_B4 + 1024;
 
+// GELU, tanh form: h = x/2 + (x/2) tanh(x (c0 + c1 x^2)), c0 = sqrt(2/pi), c1 = 0.044715 c0.
 __device__ __forceinline__ float gelu_tanh(float x) {
-    float inner = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+    const float inner = x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f);
     float t;
     asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(inner));
-    return 0.5f * x * (1.f + t);
+    const float h = 0.5f * x;
+    return fmaf(h, t, h);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
@@ -74,13 +75,27 @@ __device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
 
 // ------------------------------------------------------------------ per-cell layer 1
 
+// What the displacement step needs from the forcing at a start cell-level, in one contiguous
+// record: corners in the order (j,i), (j+1,i), (j+1,i+1), (j,i+1) of records t0 and t1.
+struct alignas(16) CellCorners {
+    float u[2][4], v[2][4];    // rho level kI
+    float wU[2][4], wL[2][4];  // w levels kI and kI-1
+    float zeta[2][4];
+    float h[4];
+    double xdist, ydist, depth;  // cell metric, depthIntervals(kI)
+    float gate, pad;
+};
+static_assert(sizeof(CellCorners) == 208, "corner record layout");
+
 struct CellArgs {
     int eta, xi, sW, sRho;
     long long nCL;  // (eta-1) * (xi-1) * (sW-1) cell-levels, index ((j*(xi-1)) + i)*(sW-1) + kI+sW-2
-    const float *u0, *v0, *w0, *u1, *v1, *w1;
+    const float *u0, *v0, *w0, *u1, *v1, *w1, *z0, *z1;
+    const double *h, *depthIntervals;
+    const double2 *metric;
     const uint8_t *weights;
-    __half *z;      // [nCL][256]
-    float *gate;    // [nCL]
+    __half *z;             // [nCL][256]
+    CellCorners *corners;  // [nCL]
     int *err;
 };
 
@@ -242,7 +257,38 @@ __global__ void __launch_bounds__(128, 1) surrogate_cell_kernel(const CellArgs a
                 }
             }
         }
-        if (write) a.gate[cl] = fminf(sqrtf(gsum / 256.f) / GATE_SIGMA, 1.f);
+        if (write) {
+            const int lev = (int)(cl % levels);
+            const long long cell = cl / levels;
+            const int j = (int)(cell / (a.xi - 1)), i = (int)(cell % (a.xi - 1));
+            const int kI = lev - (a.sW - 2);
+            const size_t plane = (size_t)a.eta * a.xi, c00 = (size_t)j * a.xi + i;
+            const size_t corner[4] = {c00, c00 + a.xi, c00 + a.xi + 1, c00 + 1};
+            const size_t lr = (size_t)(kI + a.sRho - 1) * plane, lu = (size_t)(kI + a.sW - 1) * plane,
+                         ll = (size_t)(kI + a.sW - 2) * plane;
+            CellCorners c;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                c.u[0][q] = a.u0[lr + corner[q]];
+                c.u[1][q] = a.u1[lr + corner[q]];
+                c.v[0][q] = a.v0[lr + corner[q]];
+                c.v[1][q] = a.v1[lr + corner[q]];
+                c.wU[0][q] = a.w0[lu + corner[q]];
+                c.wU[1][q] = a.w1[lu + corner[q]];
+                c.wL[0][q] = a.w0[ll + corner[q]];
+                c.wL[1][q] = a.w1[ll + corner[q]];
+                c.zeta[0][q] = a.z0[corner[q]];
+                c.zeta[1][q] = a.z1[corner[q]];
+                c.h[q] = (float)a.h[corner[q]];
+            }
+            const double2 m = a.metric[c00];
+            c.xdist = m.x;
+            c.ydist = m.y;
+            c.depth = a.depthIntervals[kI + a.sW - 2];
+            c.gate = fminf(sqrtf(gsum / 256.f) / GATE_SIGMA, 1.f);
+            c.pad = 0.f;
+            a.corners[cl] = c;
+        }
         fence_before_sync();
         __syncthreads();
         if (abortFlag) break;
@@ -264,36 +310,36 @@ __global__ void __launch_bounds__(128, 1) surrogate_cell_kernel(const CellArgs a
 
 struct StepArgs {
     int eta, xi, sW, sRho;
-    double start, length, dti, tau0, survprob, sv, shoreLimit;
+    double start, length, dti, tau0, survprob, sv;
     int upper, lower, horizontal;
     int fallbackAll;  // run parameters outside the surrogate: every active particle falls back
     int drift;        // driftModel == 1: drifting objects fall back
-    const float *u0, *v0, *w0, *z0, *u1, *v1, *w1, *z1;
-    const double *h, *depthIntervals;
-    const double2 *metric;
-    const int *dry;        // inclusive 2-D prefix sums of dry nodes, [(eta+1)][(xi+1)]
-    const __half *z;       // [nCL][256]
-    const float *gate;     // [nCL]
+    const int *dry;   // inclusive 2-D prefix sums of dry nodes, [(eta+1)][(xi+1)]
+    const __half *z;  // [nCL][256]
+    const CellCorners *corners;
     const uint8_t *weights;
     uint32_t *fallback, *fallbackCount;
     unsigned long long *runCount;
 };
 
 constexpr int STEP_THREADS = 320;
-constexpr size_t STEP_SMEM = (size_t)HID_KB * KBLOCK_A + RING * (size_t)KBLOCK_W + 1024;
+constexpr int WRING = 2;
+constexpr uint32_t A_BYTES = HID_KB * KBLOCK_A;  // 64 KB: one tile's activations
+constexpr size_t STEP_SMEM = 2 * (size_t)A_BYTES + WRING * (size_t)KBLOCK_W + 1024;
 
 enum : int { ROW_NONE = 0, ROW_RUN = 1, ROW_FALLBACK = 2, ROW_EMPTY = 3 };
 
-__device__ __forceinline__ double bil_f(const float *f, size_t plane, int xi, int jI, int iI,
-                                        double jF, double iF) {
-    const float *p = f + plane + (size_t)jI * xi + iI;
-    const double f00 = p[0], f01 = p[1], f10 = p[xi], f11 = p[xi + 1];
-    return f00 * (1 - iF) * (1 - jF) + f10 * (1 - iF) * jF + f11 * iF * jF + f01 * iF * (1 - jF);
-}
+// A tile's row as the prologue classified it.
+struct RowTag {
+    uint32_t slot;
+    int status;
+    int cl;
+};
 
-__device__ __forceinline__ double bil_d(const double *f, int xi, int jI, int iI, double jF, double iF) {
-    const double *p = f + (size_t)jI * xi + iI;
-    return p[0] * (1 - iF) * (1 - jF) + p[xi] * (1 - iF) * jF + p[xi + 1] * iF * jF + p[1] * iF * (1 - jF);
+// Bilinear value from the four corners (j,i), (j+1,i), (j+1,i+1), (j,i+1) held in x, y, z, w.
+__device__ __forceinline__ double bil4(const float4 c, double jF, double iF) {
+    return (double)c.x * (1 - iF) * (1 - jF) + (double)c.y * (1 - iF) * jF + (double)c.z * iF * jF +
+           (double)c.w * iF * (1 - jF);
 }
 
 // End of nSub equal substeps of disp/nSub along one axis of [0, maximum): a particle leaving the
@@ -322,25 +368,42 @@ __device__ __forceinline__ int dry_in_box(const int *pre, int xi, int ja, int jb
     return pre[(jb + 1) * w + ib + 1] - pre[ja * w + ib + 1] - pre[(jb + 1) * w + ia] + pre[ja * w + ia];
 }
 
+// The MMA jobs of a block in the order the row warps make their operands ready: layer 2 of tiles
+// 0 and 1, layer 3 of tile 0, then for each tile k layer 3 of tile k+1 and layer 2 of tile k+2.
+// fn(tile, layer) returns false to stop.
+template <class Fn>
+__device__ __forceinline__ void for_each_job(int nT, Fn fn) {
+    if (nT > 0 && !fn(0, 0)) return;
+    if (nT > 1 && !fn(1, 0)) return;
+    if (nT > 0 && !fn(0, 1)) return;
+    for (int k = 0; k < nT; k++) {
+        if (k + 1 < nT && !fn(k + 1, 1)) return;
+        if (k + 2 < nT && !fn(k + 2, 0)) return;
+    }
+}
+
 __global__ void __launch_bounds__(STEP_THREADS, 1)
     surrogate_step_kernel(const StepArgs a, ParticleSoA S, const MoveLaunch L) {
     using namespace umma;
     extern __shared__ uint8_t dynSmem[];
-    uint8_t *sA = align1024(dynSmem);
-    uint8_t *ring = sA + HID_KB * KBLOCK_A;
-    __shared__ __align__(8) uint64_t full[RING], empty[RING], aFull, accFull;
+    uint8_t *sA0 = align1024(dynSmem);
+    uint8_t *ring = sA0 + 2 * A_BYTES;
+    __shared__ __align__(8) uint64_t full[WRING], empty[WRING], aFull[2], accFull[2];
     __shared__ uint32_t tmemSlot;
     __shared__ int abortFlag, rowStop;
-    __shared__ float w1ps[HID * 4], b2s[HID], b3s[HID], w4s[3 * HID], b4s[4];
+    __shared__ __align__(16) float w1ps[HID * 4];  // read as float4 per hidden unit
+    __shared__ float b2s[HID], b3s[HID], w4s[3 * HID], b4s[4];
     __shared__ float red[TILE * 3];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
-        for (int s = 0; s < RING; s++) {
+        for (int s = 0; s < WRING; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(&aFull, 1);
-        mbar_init(&accFull, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&aFull[b], 1);
+            mbar_init(&accFull[b], 1);
+        }
         abortFlag = 0;
         rowStop = 0;
         fence_barrier_init();
@@ -359,68 +422,61 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
         for (int c = tid; c < 3 * HID; c += STEP_THREADS) w4s[c] = w4[c];
         if (tid < 3) b4s[tid] = b4[tid];
     }
-    if (warp == 9) tmem_alloc(&tmemSlot, 256);
+    if (warp == 9) tmem_alloc(&tmemSlot, 512);
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = tmemSlot;
     const long long nTiles = ((long long)L.count + TILE - 1) / TILE;
+    const int nT = blockIdx.x < nTiles ? (int)((nTiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
     const uint32_t idesc = idesc_bf16(TILE, HID);
 
     if (warp == 8) {
         // ---------------------------------------------------------- weight producer
         if (lane == 0) {
-            int issued[RING] = {-1, -1, -1};
+            int issued0 = -1, issued1 = -1;
             uint32_t g = 0;
-            bool ok = true;
-            for (long long tile = blockIdx.x; tile < nTiles && ok; tile += gridDim.x) {
-                for (int b = 0; b < 2 * HID_KB && ok; b++, g++) {
-                    const uint32_t s = g % RING, n = g / RING;
-                    if (!mbar_wait(&empty[s], (n & 1) ^ 1, &abortFlag)) {
-                        ok = false;
-                        break;
-                    }
+            for_each_job(nT, [&](int, int layer) {
+                for (int b = 0; b < HID_KB; b++, g++) {
+                    const uint32_t s = g % WRING, n = g / WRING;
+                    if (!mbar_wait(&empty[s], (n & 1) ^ 1, &abortFlag)) return false;
                     mbar_expect_tx(&full[s], KBLOCK_W);
-                    const uint8_t *src = a.weights + (b < HID_KB ? OFF_W2 + (size_t)b * KBLOCK_W
-                                                                 : OFF_W3 + (size_t)(b - HID_KB) * KBLOCK_W);
-                    bulk_g2s(ring + s * KBLOCK_W, src, KBLOCK_W, &full[s]);
-                    issued[s] = (int)n;
+                    const size_t off = (layer == 0 ? OFF_W2 : OFF_W3) + (size_t)b * KBLOCK_W;
+                    bulk_g2s(ring + s * KBLOCK_W, a.weights + off, KBLOCK_W, &full[s]);
+                    if (s == 0) issued0 = (int)n;
+                    else issued1 = (int)n;
                 }
-            }
+                return true;
+            });
             // copies still in flight land before the block exits
-            for (int s = 0; s < RING; s++)
-                if (issued[s] >= 0) mbar_wait_bounded(&full[s], (uint32_t)issued[s] & 1);
+            if (issued0 >= 0) mbar_wait_bounded(&full[0], (uint32_t)issued0 & 1);
+            if (issued1 >= 0) mbar_wait_bounded(&full[1], (uint32_t)issued1 & 1);
         }
         __syncwarp();
     } else if (warp == 9) {
         // ---------------------------------------------------------- MMA issuer
         if (lane == 0) {
             uint32_t g = 0;
-            bool ok = true;
-            for (long long tile = blockIdx.x; tile < nTiles && ok; tile += gridDim.x) {
-                for (int layer = 0; layer < 2 && ok; layer++) {
-                    if (!mbar_wait(&aFull, (uint32_t)layer, &abortFlag)) {
-                        ok = false;
-                        break;
-                    }
+            for_each_job(nT, [&](int tile, int layer) {
+                const int buf = tile & 1;
+                if (!mbar_wait(&aFull[buf], (uint32_t)layer, &abortFlag)) return false;
+                fence_after_sync();
+                const uint32_t d = tmem + (uint32_t)(buf * HID);
+                const uint8_t *A = sA0 + buf * A_BYTES;
+                for (int kb = 0; kb < HID_KB; kb++, g++) {
+                    const uint32_t s = g % WRING, n = g / WRING;
+                    if (!mbar_wait(&full[s], n & 1, &abortFlag)) return false;
                     fence_after_sync();
-                    for (int kb = 0; kb < HID_KB; kb++, g++) {
-                        const uint32_t s = g % RING, n = g / RING;
-                        if (!mbar_wait(&full[s], n & 1, &abortFlag)) {
-                            ok = false;
-                            break;
-                        }
-                        fence_after_sync();
 #pragma unroll
-                        for (int ks = 0; ks < 4; ks++)
-                            mma_bf16(tmem, desc_sw128(smem_u32(sA + kb * KBLOCK_A + ks * 32)),
-                                     desc_sw128(smem_u32(ring + s * KBLOCK_W + ks * 32)), idesc,
-                                     (kb | ks) != 0);
-                        mma_commit(&empty[s]);
-                    }
-                    mma_commit(&accFull);
+                    for (int ks = 0; ks < 4; ks++)
+                        mma_bf16(d, desc_sw128(smem_u32(A + kb * KBLOCK_A + ks * 32)),
+                                 desc_sw128(smem_u32(ring + s * KBLOCK_W + ks * 32)), idesc,
+                                 (kb | ks) != 0);
+                    mma_commit(&empty[s]);
                 }
-            }
+                mma_commit(&accFull[buf]);
+                return true;
+            });
         }
         __syncwarp();
     } else {
@@ -431,52 +487,55 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
         const int cBase = half * 128;
         const double T0 = a.start, T1 = a.start + a.length;
         const double kLower = -a.sW + 2;
-        for (long long tile = blockIdx.x; tile < nTiles; tile += gridDim.x) {
-            // ---- prologue: state, status, layer 1 from z
-            const long long n = tile * TILE + r;
-            int status = ROW_EMPTY;
-            uint32_t slot = 0;
-            double pj = 0, pi = 0, pk = 0, ptime = 0, phealth = 0, page = 0;
-            int jI = 0, iI = 0, kI = 0;
+        auto tileOf = [&](int x) { return (long long)blockIdx.x + (long long)x * gridDim.x; };
+        auto arrive = [&](int buf) {
+            fence_async_shared();
+            fence_before_sync();
+            named_sync(1, 256);
+            if (tid == 0) mbar_arrive(&aFull[buf]);
+        };
+
+        // layer 1 of tile x from the per-cell sums -> A[x & 1]
+        auto prologue = [&](int x) {
+            RowTag tag{0u, ROW_EMPTY, 0};
+            const long long n = tileOf(x) * TILE + r;
             float jF = 0.f, iF = 0.f, kF = 0.f, a0 = 0.f;
-            long long cl = 0;
             if (n < L.count) {
-                slot = L.order ? L.order[n] : (uint32_t)n;
-                pj = S.j[slot];
-                pi = S.i[slot];
-                pk = S.k[slot];
-                ptime = S.time[slot];
-                phealth = S.health[slot];
-                page = S.age[slot];
-                const int ptype = S.type[slot];
-                status = ROW_NONE;
+                tag.slot = L.order ? L.order[n] : (uint32_t)n;
+                const double pj = S.j[tag.slot], pi = S.i[tag.slot], pk = S.k[tag.slot];
+                const double ptime = S.time[tag.slot], phealth = S.health[tag.slot];
+                const int ptype = S.type[tag.slot];
+                tag.status = ROW_NONE;
                 if (phealth > 0 && ptime < T1) {
                     const double fj = floor(pj), fi = floor(pi), ck = ceil(pk);
                     const bool cellOk = fj >= 0 && fi >= 0 && fj + 1 < a.eta && fi + 1 < a.xi;
                     if (a.fallbackAll || phealth < a.survprob || pk > 0 || pk < kLower ||
                         (a.drift && ptype != 0) || !cellOk) {
-                        status = ROW_FALLBACK;
+                        tag.status = ROW_FALLBACK;
                     } else {
-                        status = ROW_RUN;
-                        jI = (int)fj;
-                        iI = (int)fi;
-                        kI = (int)ck;
+                        tag.status = ROW_RUN;
+                        const int jI = (int)fj, iI = (int)fi, kI = (int)ck;
                         jF = (float)(pj - fj);
                         iF = (float)(pi - fi);
                         kF = (float)(ck - pk);
                         a0 = ptime > T0 ? (float)((ptime - T0) / a.length) : 0.f;
-                        cl = ((long long)jI * (a.xi - 1) + iI) * (a.sW - 1) + (kI + a.sW - 2);
+                        tag.cl = (jI * (a.xi - 1) + iI) * (a.sW - 1) + (kI + a.sW - 2);
                     }
                 }
             }
-            {
-                const uint4 *zrow = reinterpret_cast<const uint4 *>(a.z + (size_t)cl * HID + cBase);
+            uint8_t *A = sA0 + (x & 1) * A_BYTES;
+            const uint4 *zrow = reinterpret_cast<const uint4 *>(a.z + (size_t)tag.cl * HID + cBase);
 #pragma unroll 1
-                for (int q = 0; q < 16; q++) {
+            for (int q0 = 0; q0 < 16; q0 += 8) {
+                uint4 zz[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    zz[q] = tag.status == ROW_RUN ? __ldg(zrow + q0 + q) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
                     uint4 out = make_uint4(0, 0, 0, 0);
-                    if (status == ROW_RUN) {
-                        const uint4 zz = __ldg(zrow + q);
-                        const __half2 *hz = reinterpret_cast<const __half2 *>(&zz);
+                    if (tag.status == ROW_RUN) {
+                        const __half2 *hz = reinterpret_cast<const __half2 *>(&zz[q]);
                         float h[8];
 #pragma unroll
                         for (int e = 0; e < 4; e++) {
@@ -486,33 +545,36 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                         }
 #pragma unroll
                         for (int e = 0; e < 8; e++) {
-                            const int c = cBase + q * 8 + e;
-                            const float* wp = w1ps + c * 4;
-                            float x = h[e] + wp[0] * jF + wp[1] * iF + wp[2] * kF + wp[3] * a0;
-                            h[e] = gelu_tanh(x);
+                            const float4 wp =
+                                *reinterpret_cast<const float4 *>(w1ps + (cBase + (q0 + q) * 8 + e) * 4);
+                            h[e] = gelu_tanh(h[e] + wp.x * jF + wp.y * iF + wp.z * kF + wp.w * a0);
                         }
                         out.x = pack_bf16(h[0], h[1]);
                         out.y = pack_bf16(h[2], h[3]);
                         out.z = pack_bf16(h[4], h[5]);
                         out.w = pack_bf16(h[6], h[7]);
                     }
-                    const int col = cBase + q * 8;
-                    *reinterpret_cast<uint4 *>(sA + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
+                    const int col = cBase + (q0 + q) * 8;
+                    *reinterpret_cast<uint4 *>(A + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
                 }
             }
-            fence_async_shared();
-            fence_before_sync();
-            named_sync(1, 256);
-            if (tid == 0) mbar_arrive(&aFull);
-            // ---- layer 2 epilogue: h2 = GELU(acc + b2) -> A
-            bool ok = mbar_wait(&accFull, 0, &abortFlag);
+            arrive(x & 1);
+            return tag;
+        };
+
+        // layer-2 epilogue of tile x: GELU(acc + b2) -> A[x & 1]
+        auto epilogue2 = [&](int x) {
+            const int buf = x & 1;
+            const bool ok = mbar_wait(&accFull[buf], 0, &abortFlag);
             __syncwarp();
             fence_after_sync();
+            uint8_t *A = sA0 + buf * A_BYTES;
+            const uint32_t acc = tmem + (uint32_t)(buf * HID) + tlane;
 #pragma unroll 1
             for (int t = 0; t < 4; t++) {
                 const int c0 = cBase + 32 * t;
                 float v[32];
-                tmem_ld32(tmem + tlane + (uint32_t)c0, v);
+                tmem_ld32(acc + (uint32_t)c0, v);
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     uint4 out;
@@ -521,29 +583,33 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                     out.z = pack_bf16(gelu_tanh(v[8 * q + 4] + b2s[c0 + 8 * q + 4]), gelu_tanh(v[8 * q + 5] + b2s[c0 + 8 * q + 5]));
                     out.w = pack_bf16(gelu_tanh(v[8 * q + 6] + b2s[c0 + 8 * q + 6]), gelu_tanh(v[8 * q + 7] + b2s[c0 + 8 * q + 7]));
                     const int col = c0 + 8 * q;
-                    *reinterpret_cast<uint4 *>(sA + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
+                    *reinterpret_cast<uint4 *>(A + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
                 }
             }
-            fence_async_shared();
-            fence_before_sync();
-            named_sync(1, 256);
-            if (tid == 0) mbar_arrive(&aFull);
-            // ---- layer 3 epilogue with layer 4 folded in
-            ok = mbar_wait(&accFull, 1, &abortFlag) && ok;
+            arrive(buf);
+            return ok;
+        };
+
+        // layer-3 epilogue of tile x with layer 4 folded in; the upper column half leaves its
+        // partial sums in red[]
+        auto epilogue3 = [&](int x, float &o0, float &o1, float &o2) {
+            const int buf = x & 1;
+            const bool ok = mbar_wait(&accFull[buf], 1, &abortFlag);
             __syncwarp();
             fence_after_sync();
-            float o0 = 0.f, o1 = 0.f, o2 = 0.f;
+            const uint32_t acc = tmem + (uint32_t)(buf * HID) + tlane;
+            o0 = o1 = o2 = 0.f;
 #pragma unroll 1
             for (int t = 0; t < 4; t++) {
                 const int c0 = cBase + 32 * t;
                 float v[32];
-                tmem_ld32(tmem + tlane + (uint32_t)c0, v);
+                tmem_ld32(acc + (uint32_t)c0, v);
 #pragma unroll
                 for (int c = 0; c < 32; c++) {
-                    const float x = gelu_tanh(v[c] + b3s[c0 + c]);
-                    o0 = fmaf(x, w4s[c0 + c], o0);
-                    o1 = fmaf(x, w4s[HID + c0 + c], o1);
-                    o2 = fmaf(x, w4s[2 * HID + c0 + c], o2);
+                    const float h = gelu_tanh(v[c] + b3s[c0 + c]);
+                    o0 = fmaf(h, w4s[c0 + c], o0);
+                    o1 = fmaf(h, w4s[HID + c0 + c], o1);
+                    o2 = fmaf(h, w4s[2 * HID + c0 + c], o2);
                 }
             }
             if (half == 1) {
@@ -553,38 +619,46 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             }
             fence_before_sync();
             named_sync(1, 256);
-            if (half == 0) {
-                // ---- displacement, closures, state
-                long long concCell = -1;
-                int steps = 0;
-                bool run = false;
-                const bool write = ok && !abortFlag;
-                if (status == ROW_RUN && write) {
-                    const float gate = __ldg(a.gate + cl);
+            return ok;
+        };
+
+        // displacement, closures and state of a row of tile x (lower column half)
+        auto post = [&](const RowTag &tag, float o0, float o1, float o2, bool ok) {
+            long long concCell = -1;
+            int steps = 0;
+            bool run = false;
+            int status = tag.status;
+            const bool write = ok && !abortFlag;
+            if (status != ROW_EMPTY && write) {
+                const uint32_t slot = tag.slot;
+                const double pj = S.j[slot], pi = S.i[slot], pk = S.k[slot];
+                const double ptime = S.time[slot], page = S.age[slot], phealth = S.health[slot];
+                if (status == ROW_RUN) {
+                    // the corner record: u[0],u[1],v[0],v[1],wU[0],wU[1],wL[0],wL[1],zeta[0],zeta[1],h
+                    // as float4s, then {xdist, ydist}, then {depth, gate}
+                    const float4 *cf = reinterpret_cast<const float4 *>(a.corners + tag.cl);
+                    const float4 cu0 = __ldg(cf + 0), cu1 = __ldg(cf + 1), cv0 = __ldg(cf + 2),
+                                 cv1 = __ldg(cf + 3), cwU0 = __ldg(cf + 4), cwU1 = __ldg(cf + 5),
+                                 cwL0 = __ldg(cf + 6), cwL1 = __ldg(cf + 7), cz0 = __ldg(cf + 8),
+                                 cz1 = __ldg(cf + 9), ch = __ldg(cf + 10);
+                    const double2 met = __ldg(reinterpret_cast<const double2 *>(cf + 11));
+                    const double depth = __ldg(reinterpret_cast<const double *>(cf + 12));
+                    const float gate = __ldg(reinterpret_cast<const float *>(cf + 12) + 2);
                     const double y0 = (double)((o0 + red[r * 3 + 0] + b4s[0]) * gate);
                     const double y1 = (double)((o1 + red[r * 3 + 1] + b4s[1]) * gate);
                     const double y2 = (double)((o2 + red[r * 3 + 2] + b4s[2]) * gate);
+                    const double fj = floor(pj), fi = floor(pi), ck = ceil(pk);
+                    const double jF = pj - fj, iF = pi - fi, kF = ck - pk;
                     const double da0 = ptime > T0 ? (ptime - T0) / a.length : 0.0;
                     const double amid = 0.5 * (da0 + 1.0), trem = (1.0 - da0) * a.length;
                     const double nSub = fmax(1.0, ceil(trem / a.dti - 1e-9));
-                    const size_t plane = (size_t)a.eta * a.xi;
-                    const double djF = pj - jI, diF = pi - iI, dkF = (double)kI - pk;
-                    const size_t lr = (size_t)(kI + a.sRho - 1) * plane;
-                    const double ub = (1 - amid) * bil_f(a.u0, lr, a.xi, jI, iI, djF, diF) +
-                                      amid * bil_f(a.u1, lr, a.xi, jI, iI, djF, diF);
-                    const double vb = (1 - amid) * bil_f(a.v0, lr, a.xi, jI, iI, djF, diF) +
-                                      amid * bil_f(a.v1, lr, a.xi, jI, iI, djF, diF);
-                    const size_t lwU = (size_t)(kI + a.sW - 1) * plane, lwL = (size_t)(kI + a.sW - 2) * plane;
-                    const double wb =
-                        (1 - amid) * ((1 - dkF) * bil_f(a.w0, lwU, a.xi, jI, iI, djF, diF) +
-                                      dkF * bil_f(a.w0, lwL, a.xi, jI, iI, djF, diF)) +
-                        amid * ((1 - dkF) * bil_f(a.w1, lwU, a.xi, jI, iI, djF, diF) +
-                                dkF * bil_f(a.w1, lwL, a.xi, jI, iI, djF, diF));
-                    const double hc = bil_d(a.h, a.xi, jI, iI, djF, diF) +
-                                      (1 - amid) * bil_f(a.z0, 0, a.xi, jI, iI, djF, diF) +
-                                      amid * bil_f(a.z1, 0, a.xi, jI, iI, djF, diF);
-                    const double2 met = a.metric[(size_t)jI * a.xi + iI];
-                    const double zdist = hc * a.depthIntervals[kI + a.sW - 2];
+                    const double ub = (1 - amid) * bil4(cu0, jF, iF) + amid * bil4(cu1, jF, iF);
+                    const double vb = (1 - amid) * bil4(cv0, jF, iF) + amid * bil4(cv1, jF, iF);
+                    const double wb = (1 - amid) * ((1 - kF) * bil4(cwU0, jF, iF) + kF * bil4(cwL0, jF, iF)) +
+                                      amid * ((1 - kF) * bil4(cwU1, jF, iF) + kF * bil4(cwL1, jF, iF));
+                    const double hc = bil4(ch, jF, iF) + (1 - amid) * bil4(cz0, jF, iF) +
+                                      amid * bil4(cz1, jF, iF);
+                    const double zdist = hc * depth;
                     const double dI = (ub * trem + OUT_H * y0) / met.x;
                     const double dJ = (vb * trem + OUT_H * y1) / met.y;
                     const double dK = ((wb + a.sv) * trem + OUT_V * y2) / zdist;
@@ -594,17 +668,14 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                     const double m = fmin(mj, mi);
                     const bool crossed = m <= nSub;
                     bool dead = false;
-                    if (a.horizontal == 1 && crossed) {  // constraint: the last in-domain substep
-                        const double keep = (m - 1) / nSub;
+                    if (a.horizontal == 1) {  // constraint: the last in-domain substep
+                        const double keep = crossed ? (m - 1) / nSub : 1.0;
                         jn = pj + keep * dJ;
                         in = pi + keep * dI;
                     } else if (a.horizontal == 2 && crossed) {  // kill
                         dead = true;
                         jn = pj;
                         in = pi;
-                    } else if (a.horizontal == 1) {
-                        jn = pj + dJ;
-                        in = pi + dI;
                     }
                     double kn = pk + dK;
                     if (kn > 0) {
@@ -643,7 +714,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                         steps = (int)nSub;
                         run = true;
                     }
-                } else if (status == ROW_NONE && write && L.conc) {
+                } else if (status == ROW_NONE && L.conc) {
                     ParticleState p;
                     p.j = pj;
                     p.i = pi;
@@ -651,28 +722,45 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                     p.health = phealth;
                     concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
                 }
-                if (status == ROW_FALLBACK && write) {
+                if (status == ROW_FALLBACK) {
                     const uint32_t at = atomicAdd(a.fallbackCount, 1u);
                     a.fallback[at] = slot;
                 }
-                __syncwarp();
-                if (L.steps) warp_sum_steps(L.steps, steps);
-                if (L.conc) warp_count(L.conc, concCell);
-                const unsigned ran = __ballot_sync(0xffffffffu, run);
-                if (lane == 0 && ran) atomicAdd(a.runCount, (unsigned long long)__popc(ran));
             }
-            // ---- uniform stop decision of the row warps
+            __syncwarp();
+            if (L.steps) warp_sum_steps(L.steps, steps);
+            if (L.conc) warp_count(L.conc, concCell);
+            const unsigned ran = __ballot_sync(0xffffffffu, run);
+            if (lane == 0 && ran) atomicAdd(a.runCount, (unsigned long long)__popc(ran));
+        };
+
+        RowTag cur{0u, ROW_EMPTY, 0}, next{0u, ROW_EMPTY, 0}, after{0u, ROW_EMPTY, 0};
+        bool okCur = true, okNext = true;
+        if (nT > 0) cur = prologue(0);
+        if (nT > 1) next = prologue(1);
+        if (nT > 0) okCur = epilogue2(0);
+        for (int k = 0; k < nT; k++) {
+            if (k + 1 < nT) okNext = epilogue2(k + 1);
+            float o0, o1, o2;
+            okCur = epilogue3(k, o0, o1, o2) && okCur;
+            if (k + 2 < nT) after = prologue(k + 2);
+            if (half == 0) post(cur, o0, o1, o2, okCur);
+            // uniform stop decision of the row warps
             named_sync(1, 256);
             if (tid == 0) rowStop = abortFlag;
             named_sync(1, 256);
             if (rowStop) break;
+            cur = next;
+            okCur = okNext;
+            next = after;
+            okNext = true;
         }
     }
     fence_before_sync();
     __syncthreads();
     if (warp == 9) {
         fence_after_sync();
-        tmem_dealloc(tmem, 256);
+        tmem_dealloc(tmem, 512);
     }
     if (tid == 0 && abortFlag) atomicOr(L.err, ERR_SURROGATE_WAIT);
 }
@@ -711,6 +799,8 @@ __global__ void dry_cols_kernel(int eta, int xi, int *pre) {
 // ------------------------------------------------------------------ host side
 
 size_t surrogate_packed_bytes() { return PACKED_BYTES; }
+
+size_t surrogate_corner_bytes() { return sizeof(CellCorners); }
 
 size_t surrogate_parameter_count() {
     return (size_t)HID * N_INPUT + HID + 2 * ((size_t)HID * HID + HID) + 3 * HID + 3;
@@ -755,7 +845,8 @@ long long surrogate_cell_levels(int eta, int xi, int sW) {
 }
 
 cudaError_t surrogate_cells(int eta, int xi, int sW, int sRho, const FrameDevice &f0,
-                            const FrameDevice &f1, const uint8_t *weights, __half *z, float *gate,
+                            const FrameDevice &f1, const double *h, const double *depthIntervals,
+                            const double2 *metric, const uint8_t *weights, __half *z, void *corners,
                             int *err, int smCount, cudaStream_t stream) {
     CellArgs a;
     a.eta = eta;
@@ -769,9 +860,14 @@ cudaError_t surrogate_cells(int eta, int xi, int sW, int sRho, const FrameDevice
     a.u1 = f1.u;
     a.v1 = f1.v;
     a.w1 = f1.w;
+    a.z0 = f0.zeta;
+    a.z1 = f1.zeta;
+    a.h = h;
+    a.depthIntervals = depthIntervals;
+    a.metric = metric;
     a.weights = weights;
     a.z = z;
-    a.gate = gate;
+    a.corners = static_cast<CellCorners *>(corners);
     a.err = err;
     if (a.nCL <= 0) return cudaSuccess;
     static bool attr = false;
@@ -801,26 +897,14 @@ cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const M
     a.tau0 = s.cfg.tau0;
     a.survprob = s.cfg.survprob;
     a.sv = s.cfg.sv;
-    a.shoreLimit = s.cfg.shoreLimit;
     a.upper = s.cfg.upperClosure;
     a.lower = s.cfg.lowerClosure;
     a.horizontal = s.cfg.horizontalClosure;
     a.fallbackAll = s.fallbackAll;
     a.drift = s.cfg.driftModel == 1;
-    a.u0 = s.f0.u;
-    a.v0 = s.f0.v;
-    a.w0 = s.f0.w;
-    a.z0 = s.f0.zeta;
-    a.u1 = s.f1.u;
-    a.v1 = s.f1.v;
-    a.w1 = s.f1.w;
-    a.z1 = s.f1.zeta;
-    a.h = s.h;
-    a.depthIntervals = s.depthIntervals;
-    a.metric = s.metric;
     a.dry = s.dry;
     a.z = s.z;
-    a.gate = s.gate;
+    a.corners = static_cast<const CellCorners *>(s.corners);
     a.weights = s.weights;
     a.fallback = s.fallback;
     a.fallbackCount = s.fallbackCount;
