@@ -187,7 +187,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, dist):
+def surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, dist, exchange):
     """The FP16+surrogate arm: device-timed throughput on the same workload, the 24-hour error
     against the FP64 reference-arithmetic kernel on a subset (rank 0), and the tensor roofline of
     the per-particle kernel."""
@@ -200,9 +200,11 @@ def surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, d
     engine.load_window(win)
     engine.set_surrogate()
     engine.set_particles(particles)
+    engine.concentration_reset(win.T)
     n_intervals = win.T - 1
     for s in range(args.warmup):
         engine.move_interval(s % n_intervals)
+        exchange(engine, s % n_intervals)
         engine.stats()
     ext = torch.cuda.ExternalStream(engine.stream)
     barrier()
@@ -211,7 +213,9 @@ def surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, d
     start.record(ext)
     steps_total, launches, step_ms, cell_ms, run, fallback = 0.0, 0, [], [], 0, 0
     for s in range(args.steps):
-        engine.move_interval((args.warmup + s) % n_intervals)
+        t = (args.warmup + s) % n_intervals
+        engine.move_interval(t)
+        exchange(engine, t)
         st = engine.stats()
         ss = engine.surrogate_stats()
         steps_total += st["particle_steps"]
@@ -313,18 +317,27 @@ def main():
                          f"median of 3 after a warm-up",
                "value_1core": rate1}
 
+    from wacommplusplus_b200 import sharding
+
     engine = Engine(local_rank, arithmetic=args.arithmetic, storage=args.storage)
     engine.load_window(win)
     engine.set_config(cfg)
     engine.set_particles(particles)
+    engine.concentration_reset(win.T)
     n_intervals = win.T - 1
 
     def barrier():
         if world > 1:
             dist.barrier()
 
+    def exchange(eng, t):
+        # the interval's concentration slice summed over the particle shards (N > 1)
+        if world > 1:
+            sharding.allreduce_concentration(eng, t + 1)
+
     for s in range(args.warmup):
         engine.move_interval(s % n_intervals)
+        exchange(engine, s % n_intervals)
         engine.stats()
     ext = torch.cuda.ExternalStream(engine.stream)
     sampler = ClockSampler(physical_gpu(local_rank))
@@ -335,7 +348,9 @@ def main():
     start.record(ext)
     steps_total, launches, move_ms, move_steps = 0.0, 0, [], []
     for s in range(args.steps):
-        engine.move_interval((args.warmup + s) % n_intervals)
+        t = (args.warmup + s) % n_intervals
+        engine.move_interval(t)
+        exchange(engine, t)
         st = engine.stats()
         steps_total += st["particle_steps"]
         launches += st["launches"]
@@ -373,6 +388,7 @@ def main():
         frame_bytes = win.nbytes_frame
         for s in range(2):
             engine.move_interval_host_ptr(s % n_intervals, host.data_ptr(), n)
+            exchange(engine, s % n_intervals)
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -382,6 +398,7 @@ def main():
             f = win.frame(t + 1)
             engine.upload_frame(t + 1, f["zeta"], f["u"], f["v"], f["w"], f["akt"])
             engine.move_interval_host_ptr(t, host.data_ptr(), n)
+            exchange(engine, t)
             e2e_steps += engine.stats()["particle_steps"]
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
@@ -397,7 +414,8 @@ def main():
 
     surrogate = None
     if not args.no_surrogate:
-        surrogate = surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, dist)
+        surrogate = surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, dist,
+                                  exchange)
 
     if rank == 0:
         line = {
@@ -412,7 +430,11 @@ def main():
                                    f"dt=30 s, forcing storage {args.storage}, arithmetic "
                                    f"{args.arithmetic}",
                        "l2": "inputs larger than L2 (particle state 1 GiB per GPU)",
-                       "parallelism": f"particle shards x{world}, no data-path collective"},
+                       "concentration": "fused uint32 counts each interval; for N > 1 the "
+                                        "interval's grid slice is summed over the shards by an "
+                                        "NCCL all-reduce inside the timed region",
+                       "parallelism": f"particle shards x{world}, one concentration all-reduce "
+                                      "per interval"},
             "roofline": roofline,
             "surrogate": surrogate,
             "cpu_baseline": cpu,

@@ -233,6 +233,13 @@ int wacomm_b200_concentration_get(wacomm_b200_context *ctx, uint32_t *out, size_
 int wacomm_b200_concentration_get_float(wacomm_b200_context *ctx, float *out, size_t n,
                                         int mask_land);
 
+/* The device address of the context's uint32 concentration grid and its cell count, so that
+ * particle shards held by several contexts (one per GPU) can sum their grids with a collective of
+ * the caller's (the counts add modulo 2^32, so a signed 32-bit sum gives the same bits). The
+ * memory stays owned by the context and valid until the next concentration_reset or destroy; the
+ * context's stream (wacomm_b200_stream) orders the kernels that write it. */
+int wacomm_b200_concentration_device(wacomm_b200_context *ctx, void **device_ptr, size_t *cells);
+
 int wacomm_b200_synchronize(wacomm_b200_context *ctx);
 
 /* Statistics of the last move_interval: device milliseconds of all its kernels (CUDA events on

@@ -67,6 +67,7 @@ SIGNATURES = {
     "wacomm_b200_concentration_count": (_i, [_vp, _i]),
     "wacomm_b200_concentration_get": (_i, [_vp, _vp, _sz]),
     "wacomm_b200_concentration_get_float": (_i, [_vp, _vp, _sz, _i]),
+    "wacomm_b200_concentration_device": (_i, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_sz)]),
     "wacomm_b200_synchronize": (_i, [_vp]),
     "wacomm_b200_last_interval_stats": (_i, [_vp, _fp, _fp, ctypes.POINTER(_i), _dp]),
     "wacomm_b200_stream": (_i, [_vp, ctypes.POINTER(_vp)]),

@@ -1158,6 +1158,14 @@ int wacomm_b200_concentration_get(wacomm_b200_context *ctx, uint32_t *out, size_
     return WACOMM_B200_OK;
 }
 
+int wacomm_b200_concentration_device(wacomm_b200_context *ctx, void **device_ptr, size_t *cells) {
+    if (!ctx || !device_ptr || !cells) return WACOMM_B200_ERR_ARGUMENT;
+    if (!ctx->dConc) return fail(ctx, WACOMM_B200_ERR_STATE, "concentration_reset has not been called");
+    *device_ptr = ctx->dConc;
+    *cells = (size_t)ctx->concTimes * ctx->sRho * ctx->eta * ctx->xi;
+    return WACOMM_B200_OK;
+}
+
 int wacomm_b200_concentration_get_float(wacomm_b200_context *ctx, float *out, size_t n,
                                         int mask_land) {
     if (!ctx || !out) return WACOMM_B200_ERR_ARGUMENT;

@@ -52,6 +52,7 @@ class Engine:
             raise WacommError(status, f"cannot create a context on CUDA device {device} "
                                       f"({self._lib.wacomm_b200_device_count()} visible)")
         self._ctx = handle
+        self.device = device
         self.window = None
         if options:
             self.set_options(**options)
@@ -249,6 +250,31 @@ class Engine:
         out = np.zeros(self._conc_shape(), dtype=np.uint32)
         self._check(self._lib.wacomm_b200_concentration_get(self._ctx, out.ctypes.data, out.size))
         return out
+
+    def concentration_device(self):
+        """(device address, cell count) of the context's uint32 concentration grid."""
+        ptr, cells = ctypes.c_void_p(), ctypes.c_size_t()
+        self._check(self._lib.wacomm_b200_concentration_device(self._ctx, ctypes.byref(ptr),
+                                                               ctypes.byref(cells)))
+        return ptr.value, cells.value
+
+    def concentration_view(self, conc_time_index=None):
+        """A torch int32 tensor on the context's device aliasing the uint32 concentration grid
+        [n_times][s_rho][eta][xi] (or one time slice of it), for collectives across shards; the
+        bits are the uint32 counts."""
+        import torch
+        ptr, cells = self.concentration_device()
+        shape = self._conc_shape()
+        plane = int(np.prod(shape[1:]))
+        if conc_time_index is not None:
+            ptr += 4 * plane * conc_time_index
+            shape = shape[1:]
+        device = torch.device("cuda", self.device)
+
+        class _Grid:
+            __cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<i4",
+                                        "data": (ptr, False), "version": 3, "strides": None}
+        return torch.as_tensor(_Grid(), device=device)
 
     def concentration_float(self, mask_land=False):
         out = np.zeros(self._conc_shape(), dtype=np.float32)
