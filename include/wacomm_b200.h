@@ -170,6 +170,18 @@ int wacomm_b200_upload_frame(wacomm_b200_context *ctx, int t, const float *zeta,
                              const float *wind_u10, const float *wind_v10, const float *stokes_u,
                              const float *stokes_v);
 
+/* The same upload without waiting: the copies run on the context's copy stream, after the kernels
+ * already enqueued on its compute stream (which may still read record t), and the next interval
+ * that uses record t waits for them on the device. The host arrays must stay unchanged until the
+ * copies have completed (wacomm_b200_synchronize); from page-locked memory the call returns at
+ * once, so the next record crosses PCIe while the current interval computes (the reference
+ * re-uploads its whole window each interval, Wacomm.cpp:424-477). */
+int wacomm_b200_upload_frame_async(wacomm_b200_context *ctx, int t, const float *zeta,
+                                   const float *u, const float *v, const float *w,
+                                   const float *akt, const float *wind_u10,
+                                   const float *wind_v10, const float *stokes_u,
+                                   const float *stokes_v);
+
 /* Particle records in and out (reference particle_data layout, host memory). set replaces the
  * resident set, append adds after it, get copies the resident records (in their order) into
  * out (capacity n), and count reports how many are resident. */

@@ -53,6 +53,7 @@ SIGNATURES = {
     "wacomm_b200_set_grid": (_i, [_vp, _i, _i, _i, _i, _dp, _dp, _dp, _dp, _dp]),
     "wacomm_b200_set_times": (_i, [_vp, _i, _dp]),
     "wacomm_b200_upload_frame": (_i, [_vp, _i] + [_fp] * 9),
+    "wacomm_b200_upload_frame_async": (_i, [_vp, _i] + [_fp] * 9),
     "wacomm_b200_set_particles": (_i, [_vp, _vp, _sz]),
     "wacomm_b200_append_particles": (_i, [_vp, _vp, _sz]),
     "wacomm_b200_get_particles": (_i, [_vp, _vp, _sz]),

@@ -25,6 +25,8 @@ struct FrameSlot {
     float *zeta = nullptr, *u = nullptr, *v = nullptr, *w = nullptr, *akt = nullptr;
     float *windU = nullptr, *windV = nullptr, *stokesU = nullptr, *stokesV = nullptr;
     bool loaded = false;
+    bool pending = false;           // an asynchronous upload the compute stream has not waited on
+    cudaEvent_t ready = nullptr;    // recorded on the copy stream after an asynchronous upload
 };
 
 struct SoABuffers {
@@ -116,6 +118,7 @@ struct wacomm_b200_context {
     unsigned long long *dSteps = nullptr;
     int *dErr = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evMove0 = nullptr, evMove1 = nullptr;
+    cudaEvent_t evComputeMark = nullptr;  // orders asynchronous frame copies after enqueued kernels
     bool moveTimed = false;
     float lastMs = 0;
     int lastLaunches = 0;
@@ -295,6 +298,7 @@ void release_frames(wacomm_b200_context *ctx) {
         cudaFree(s.windV);
         cudaFree(s.stokesU);
         cudaFree(s.stokesV);
+        if (s.ready) cudaEventDestroy(s.ready);
         s = FrameSlot{};
     }
     ctx->pairT0 = ctx->pairT1 = -1;
@@ -464,6 +468,13 @@ int prepare_interval(wacomm_b200_context *ctx, int time_index, IntervalParams &P
     if (!ctx->slots[P.t0].loaded || !ctx->slots[P.t1].loaded)
         return fail(ctx, WACOMM_B200_ERR_STATE, "forcing records %d and %d must be uploaded", P.t0,
                     P.t1);
+    for (int t : {P.t0, P.t1}) {
+        FrameSlot &slot = ctx->slots[t];
+        if (slot.pending) {
+            CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, slot.ready, 0));
+            slot.pending = false;
+        }
+    }
     if ((rc = ensure_metric(ctx))) return rc;
     if ((rc = ensure_pair(ctx, P.t0, P.t1, launches))) return rc;
     return WACOMM_B200_OK;
@@ -639,6 +650,7 @@ int wacomm_b200_context_create(int device, wacomm_b200_context **out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->evComputeMark, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->evMove0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->evMove1);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->dSteps, sizeof(unsigned long long));
@@ -663,6 +675,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     if (!ctx) return WACOMM_B200_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->h2d) cudaStreamSynchronize(ctx->h2d);
     release_frames(ctx);
     cudaFree(ctx->dMask);
     cudaFree(ctx->dLon);
@@ -710,6 +723,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dCfg);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->evComputeMark) cudaEventDestroy(ctx->evComputeMark);
     if (ctx->evMove0) cudaEventDestroy(ctx->evMove0);
     if (ctx->evMove1) cudaEventDestroy(ctx->evMove1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -768,6 +782,7 @@ int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, i
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null grid array");
     cudaSetDevice(ctx->device);
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
     size_t plane = (size_t)eta * xi;
     cudaFree(ctx->dMask);
     cudaFree(ctx->dLon);
@@ -839,10 +854,17 @@ int wacomm_b200_set_times(wacomm_b200_context *ctx, int n_times, const double *o
     return WACOMM_B200_OK;
 }
 
-int wacomm_b200_upload_frame(wacomm_b200_context *ctx, int t, const float *zeta, const float *u,
-                             const float *v, const float *w, const float *akt,
-                             const float *wind_u10, const float *wind_v10, const float *stokes_u,
-                             const float *stokes_v) {
+}  // extern "C"
+
+namespace {
+
+// Copies forcing record t from host arrays into its device slot on the copy stream. Synchronous:
+// the compute stream is drained first and the copies are waited for. Asynchronous: the copy
+// stream waits for the work enqueued so far on the compute stream (which may still read the
+// slot), and the slot's ready event is recorded for the next interval to wait on.
+int stage_frame(wacomm_b200_context *ctx, int t, const float *zeta, const float *u, const float *v,
+                const float *w, const float *akt, const float *wind_u10, const float *wind_v10,
+                const float *stokes_u, const float *stokes_v, bool async) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     if (!ctx->hasGrid) return fail(ctx, WACOMM_B200_ERR_STATE, "set_grid has not been called");
     if (t < 0 || t >= (int)ctx->times.size())
@@ -855,7 +877,11 @@ int wacomm_b200_upload_frame(wacomm_b200_context *ctx, int t, const float *zeta,
     FrameSlot &s = ctx->slots[t];
     auto put = [&](float *&dst, const float *src, size_t count) -> int {
         if (!src) {
-            cudaFree(dst);
+            if (dst) {
+                CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+                CUDA_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
+                cudaFree(dst);
+            }
             dst = nullptr;
             return WACOMM_B200_OK;
         }
@@ -864,8 +890,15 @@ int wacomm_b200_upload_frame(wacomm_b200_context *ctx, int t, const float *zeta,
                                       ctx->h2d));
         return WACOMM_B200_OK;
     };
-    // The pair cache may reference this slot: finish kernels that read it first.
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (async) {
+        if (!s.ready) CUDA_TRY(ctx, cudaEventCreateWithFlags(&s.ready, cudaEventDisableTiming));
+        // kernels already enqueued may read this slot (through the pair packing): copy after them
+        CUDA_TRY(ctx, cudaEventRecord(ctx->evComputeMark, ctx->stream));
+        CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->h2d, ctx->evComputeMark, 0));
+    } else {
+        // The pair cache may reference this slot: finish kernels that read it first.
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    }
     int rc;
     if ((rc = put(s.zeta, zeta, plane))) return rc;
     if ((rc = put(s.u, u, plane * ctx->sRho))) return rc;
@@ -876,11 +909,36 @@ int wacomm_b200_upload_frame(wacomm_b200_context *ctx, int t, const float *zeta,
     if ((rc = put(s.windV, wind_v10, plane))) return rc;
     if ((rc = put(s.stokesU, stokes_u, plane))) return rc;
     if ((rc = put(s.stokesV, stokes_v, plane))) return rc;
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
+    if (async) {
+        CUDA_TRY(ctx, cudaEventRecord(s.ready, ctx->h2d));
+        s.pending = true;
+    } else {
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
+        s.pending = false;
+    }
     s.loaded = true;
     if (ctx->pairT0 == t || ctx->pairT1 == t) ctx->pairT0 = ctx->pairT1 = -1;
     if (ctx->zT0 == t || ctx->zT1 == t) ctx->zT0 = ctx->zT1 = -1;
     return WACOMM_B200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wacomm_b200_upload_frame(wacomm_b200_context *ctx, int t, const float *zeta, const float *u,
+                             const float *v, const float *w, const float *akt,
+                             const float *wind_u10, const float *wind_v10, const float *stokes_u,
+                             const float *stokes_v) {
+    return stage_frame(ctx, t, zeta, u, v, w, akt, wind_u10, wind_v10, stokes_u, stokes_v, false);
+}
+
+int wacomm_b200_upload_frame_async(wacomm_b200_context *ctx, int t, const float *zeta,
+                                   const float *u, const float *v, const float *w,
+                                   const float *akt, const float *wind_u10,
+                                   const float *wind_v10, const float *stokes_u,
+                                   const float *stokes_v) {
+    return stage_frame(ctx, t, zeta, u, v, w, akt, wind_u10, wind_v10, stokes_u, stokes_v, true);
 }
 
 int wacomm_b200_set_particles(wacomm_b200_context *ctx, const wacomm_b200_particle *host,
@@ -1191,6 +1249,7 @@ int wacomm_b200_synchronize(wacomm_b200_context *ctx) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     cudaSetDevice(ctx->device);
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
     return check_errors(ctx);
 }
 

@@ -136,6 +136,17 @@ class Engine:
                   _f(stokes_u), _f(stokes_v)]
         self._check(self._lib.wacomm_b200_upload_frame(self._ctx, t, *[p for _, p in fields]))
 
+    def upload_frame_async(self, t, zeta, u, v, w, akt, wind_u10=None, wind_v10=None,
+                           stokes_u=None, stokes_v=None):
+        """Asynchronous upload of record t (copy stream, ordered after the enqueued kernels). The
+        host arrays are kept referenced until synchronize(); pass page-locked arrays (e.g. numpy
+        views of pinned torch tensors) for the copy to overlap the kernels."""
+        fields = [_f(zeta), _f(u), _f(v), _f(w), _f(akt), _f(wind_u10), _f(wind_v10),
+                  _f(stokes_u), _f(stokes_v)]
+        self._in_flight = getattr(self, "_in_flight", {})
+        self._in_flight.setdefault(t, []).append(fields)
+        self._check(self._lib.wacomm_b200_upload_frame_async(self._ctx, t, *[p for _, p in fields]))
+
     def load_window(self, win, frames=None):
         """Grid, times and forcing records of a ``synthetic.Window``-like object."""
         self.window = win
@@ -214,6 +225,7 @@ class Engine:
 
     def synchronize(self):
         self._check(self._lib.wacomm_b200_synchronize(self._ctx))
+        self._in_flight = {}
 
     def stats(self):
         """dict of the last interval: device ms of all kernels, ms of the move launches, kernel
