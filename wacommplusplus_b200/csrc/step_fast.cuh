@@ -53,10 +53,16 @@ __device__ __forceinline__ float blend(const QuadPair &q, const Weights8 &w) {
     return x + y;
 }
 
-// Water column height h + zeta at a fractional position of a cell (FP32).
+// Bilinear h, zeta@t0 and zeta@t1 at a fractional position of a cell (FP32); the water column
+// height at time weight a is h + at_f32(z0, z1, a).
+struct SurfaceSums {
+    float h, z0, z1;
+    __device__ __forceinline__ float height(float a) const { return h + at_f32(z0, z1, a); }
+};
+
 template <int STORE>
-__device__ __forceinline__ float column_height(const CellView<STORE> &C, int jI, int iI, float jF,
-                                               float iF, float a) {
+__device__ __forceinline__ SurfaceSums surface_sums(const CellView<STORE> &C, int jI, int iI,
+                                                    float jF, float iF) {
     CellSurface s = C.surf(jI, iI);
     float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
     float h = s.h.x * w1, z0 = s.z0.x * w1, z1 = s.z1.x * w1;
@@ -69,7 +75,14 @@ __device__ __forceinline__ float column_height(const CellView<STORE> &C, int jI,
     h = fmaf(s.h.w, w4, h);
     z0 = fmaf(s.z0.w, w4, z0);
     z1 = fmaf(s.z1.w, w4, z1);
-    return h + at_f32(z0, z1, a);
+    return SurfaceSums{h, z0, z1};
+}
+
+// Water column height h + zeta at a fractional position of a cell (FP32).
+template <int STORE>
+__device__ __forceinline__ float column_height(const CellView<STORE> &C, int jI, int iI, float jF,
+                                               float iF, float a) {
+    return surface_sums(C, jI, iI, jF, iF).height(a);
 }
 
 // Current (u, v, w) and, when wanted, AKT at a fractional position: one stencil read.
@@ -79,7 +92,8 @@ __device__ __forceinline__ void current_cell(const CellView<STORE> &C, int kI, f
                                              bool wantAkt, float &uu, float &vv, float &ww,
                                              float &aa) {
     QuadPair u, v, wUp, aUp, wLo, aLo;
-    C.stencil(kI, jI, iI, u, v, wUp, aUp, wLo, aLo);
+    if (wantAkt) C.stencil(kI, jI, iI, u, v, wUp, aUp, wLo, aLo);
+    else C.stencil_w(kI, jI, iI, u, v, wUp, wLo);
     Weights8 w = weights8(jF, iF, a);
     uu = blend(u, w);
     vv = blend(v, w);
@@ -190,6 +204,9 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
     const uint64_t prefix = fold(fold(mix64(cfg.randomSeed), p.id), (uint64_t)P.intervalKey);
     const uint64_t philoxKey = p.id ^ mix64(cfg.randomSeed);
     const double stop = P.chunkEnd < length ? P.chunkEnd : length;
+    // surface sums at the previous step's destination, valid while the particle still sits there
+    SurfaceSums carried{0.f, 0.f, 0.f};
+    bool haveCarried = false;
 
     while (elapsed < stop) {
         double stepDt = fmin(cfg.dti, length - elapsed);
@@ -220,7 +237,9 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         const float dt = (float)stepDt;
         const float alpha = (float)((elapsed + 0.5 * stepDt) * invLength);
         const float alphaStart = (float)(elapsed * invLength);
-        const float hc = column_height(C, jI, iI, jF, iF, alpha);
+        const SurfaceSums here = haveCarried ? carried : surface_sums(C, jI, iI, jF, iF);
+        haveCarried = false;
+        const float hc = here.height(alpha);
         if (hc <= shore && cfg.horizontalClosure == CLOSURE_KILL) {
             p.health = -1;
             lazy = false;
@@ -263,6 +282,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         }
         const float2 inv = __ldg(F.X.invMetric + (size_t)jI * xi + iI);
         const float zdist = hc * __ldg(F.X.depthIntervals + (kM + sW - 2));
+        const float rzdist = __frcp_rn(zdist);
         // index increments (i, j) and the vertical leap in metres
         float dI, dJ, zleap;
         if (midpoint) {
@@ -270,7 +290,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
             if (fabsf(kHalf) > zdist) kHalf = signf_of(zdist, kHalf);
             double iMid = p.i + (double)(dirf * uu * 0.5f * dt * inv.x);
             double jMid = p.j + (double)(dirf * vv * 0.5f * dt * inv.y);
-            double kMid = fmin(0.0, fmax(kLower, p.k + (double)(kHalf / zdist)));
+            double kMid = fmin(0.0, fmax(kLower, p.k + (double)(kHalf * rzdist)));
             double fim = floor(iMid), fjm = floor(jMid);
             int iMI = to_index<SEM>(fim), jMI = to_index<SEM>(fjm);
             bool midValid = valid_cell(jMI, iMI, eta, xi);
@@ -299,7 +319,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 float zdistMid = hcMid * __ldg(F.X.depthIntervals + (kMI + sW - 2));
                 dI = dirf * um * dt * im.x;
                 dJ = dirf * vm * dt * im.y;
-                detZ = dirf * (sv + wm) * dt * zdist / zdistMid;
+                detZ = dirf * (sv + wm) * dt * zdist * __frcp_rn(zdistMid);
             } else {
                 float ue, ve, we, unused;
                 current_cell(C, kM, kF, jI, jF, iI, iF, alpha, alpha, false, ue, ve, we, unused);
@@ -325,14 +345,18 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         if (fabsf(zleap) > zdist) zleap = signf_of(zdist, zleap);
         double jdet = p.j + (double)dJ;
         double idet = p.i + (double)dI;
-        double kdet = p.k + (double)(zleap / zdist);
+        double kdet = p.k + (double)(zleap * rzdist);
         if (kdet > 0.) close_upper(cfg, kdet, p.health, lazy);
         if (kdet < kLower) close_lower(cfg, kLower, kdet, p.health, lazy);
 
         double fjd = floor(jdet), fid = floor(idet);
         int jdetI = to_index<SEM>(fjd), idetI = to_index<SEM>(fid);
         if (valid_cell(jdetI, idetI, eta, xi)) {
-            float hcdet = column_height(C, jdetI, idetI, (float)(jdet - fjd), (float)(idet - fid), alpha);
+            const SurfaceSums there = surface_sums(C, jdetI, idetI, (float)(jdet - fjd), (float)(idet - fid));
+            float hcdet = there.height(alpha);
+            // the next step starts here unless a closure moves the particle
+            carried = there;
+            haveCarried = hcdet > shore;
             if (hcdet <= shore) {
                 if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
                     idet = p.i;

@@ -227,6 +227,31 @@ __device__ __forceinline__ void load_quad<STORE_BF16>(const CellQuad<STORE_BF16>
     b.t1 = quad_bf(y.z, y.w);
 }
 
+// The first field of a CellQuad only (w of a B record, without akt).
+template <int STORE>
+__device__ __forceinline__ void load_first(const CellQuad<STORE> *p, QuadPair &a);
+
+template <>
+__device__ __forceinline__ void load_first<STORE_F32>(const CellQuad<STORE_F32> *p, QuadPair &a) {
+    const float4 *q = reinterpret_cast<const float4 *>(p);
+    a.t0 = quad_of(__ldg(q));
+    a.t1 = quad_of(__ldg(q + 1));
+}
+
+template <>
+__device__ __forceinline__ void load_first<STORE_F16>(const CellQuad<STORE_F16> *p, QuadPair &a) {
+    uint4 x = __ldg(reinterpret_cast<const uint4 *>(p));
+    a.t0 = quad_h(x.x, x.y);
+    a.t1 = quad_h(x.z, x.w);
+}
+
+template <>
+__device__ __forceinline__ void load_first<STORE_BF16>(const CellQuad<STORE_BF16> *p, QuadPair &a) {
+    uint4 x = __ldg(reinterpret_cast<const uint4 *>(p));
+    a.t0 = quad_bf(x.x, x.y);
+    a.t1 = quad_bf(x.z, x.w);
+}
+
 struct CellSurface {  // FP32: h, zeta@t0, zeta@t1 at the 4 corners
     float4 h, z0, z1;
 };
@@ -247,6 +272,15 @@ struct CellView {
         load_quad<STORE>(col - 1, wLo, aLo);  // B(L-1)
         load_quad<STORE>(col, u, v);          // A(L)
         load_quad<STORE>(col + 1, wUp, aUp);  // B(L)
+    }
+    // The same without the diffusivity (deterministic steps).
+    __device__ __forceinline__ void stencil_w(int kI, int j, int i, QuadPair &u, QuadPair &v,
+                                              QuadPair &wUp, QuadPair &wLo) const {
+        size_t L = (size_t)(kI + sW - 1);
+        const CellQuad<STORE> *col = columns + (((size_t)j * xi + i) * sW + L) * 2;
+        load_first<STORE>(col - 1, wLo);  // B(L-1)
+        load_quad<STORE>(col, u, v);      // A(L)
+        load_first<STORE>(col + 1, wUp);  // B(L)
     }
     __device__ __forceinline__ CellSurface surf(int j, int i) const {
         const float4 *q = reinterpret_cast<const float4 *>(surface + ((size_t)j * xi + i));
