@@ -42,11 +42,18 @@ static cudaError_t by_shape(int shape, const wacomm_b200_config &cfg, const Inte
                             const PackedArgs &A, const ParticleSoA &S, const MoveLaunch &L,
                             cudaStream_t stream) {
     FastView<STORE> F = fast_view<STORE>(A);
+    // deterministic passive tracking: no diffusion, no drifting objects, no jibing
+    const bool lean = !(cfg.random && (P.direction > 0 || cfg.backwardDiffusion)) &&
+                      cfg.driftModel != 1 && !(cfg.leewayJibeProbabilityHourly > 0);
     switch (shape) {
-        case 0: return launch_move_fast<SEM, STORE, 0>(cfg, P, F, S, L, stream);
-        case 2: return launch_move_fast<SEM, STORE, 2>(cfg, P, F, S, L, stream);
-        case 3: return launch_move_fast<SEM, STORE, 3>(cfg, P, F, S, L, stream);
-        default: return launch_move_fast<SEM, STORE, 1>(cfg, P, F, S, L, stream);
+        case 0: return launch_move_fast<SEM, STORE, 0, false>(cfg, P, F, S, L, stream);
+        case 2:
+            return lean ? launch_move_fast<SEM, STORE, 2, true>(cfg, P, F, S, L, stream)
+                        : launch_move_fast<SEM, STORE, 2, false>(cfg, P, F, S, L, stream);
+        case 3: return launch_move_fast<SEM, STORE, 3, false>(cfg, P, F, S, L, stream);
+        default:
+            return lean ? launch_move_fast<SEM, STORE, 1, true>(cfg, P, F, S, L, stream)
+                        : launch_move_fast<SEM, STORE, 1, false>(cfg, P, F, S, L, stream);
     }
 }
 

@@ -177,7 +177,9 @@ __device__ __forceinline__ float signf_of(float a, float b) {
     return fabsf(a) * (float)((b > 0.f) - (b < 0.f));
 }
 
-template <int SEM, int STORE>
+// LEAN: the run parameters exclude diffusion, drifting objects and jibing (deterministic passive
+// tracking), so those branches are compiled out.
+template <int SEM, int STORE, bool LEAN>
 __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalParams &P,
                                   const FastView<STORE> &F, ParticleState &p, double &elapsed,
                                   int *err) {
@@ -190,9 +192,9 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
     const float dirf = (float)direction;
     const float sv = (float)cfg.sv, shore = (float)cfg.shoreLimit;
     const bool midpoint = cfg.integrator == INTEGRATOR_MIDPOINT;
-    const bool diffuse = cfg.random && (direction > 0 || cfg.backwardDiffusion);
-    const bool drift = cfg.driftModel == 1 && p.type != 0;
-    const bool jibe = cfg.leewayJibeProbabilityHourly > 0 && p.type != 0;
+    const bool diffuse = !LEAN && cfg.random && (direction > 0 || cfg.backwardDiffusion);
+    const bool drift = !LEAN && cfg.driftModel == 1 && p.type != 0;
+    const bool jibe = !LEAN && cfg.leewayJibeProbabilityHourly > 0 && p.type != 0;
     if (drift && SEM == SEM_HOST && (p.type < 0 || p.type > 22)) atomicOr(err, ERR_DRIFT_OBJECT);
     bool lazy = false;
     int steps = 0;
