@@ -495,16 +495,36 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             if (tid == 0) mbar_arrive(&aFull[buf]);
         };
 
-        // layer 1 of tile x from the per-cell sums -> A[x & 1]
-        auto prologue = [&](int x) {
-            RowTag tag{0u, ROW_EMPTY, 0};
+        // A row's particle state, gathered ahead of the prologue that classifies it.
+        struct RowState {
+            uint32_t slot;
+            bool valid;
+            double pj, pi, pk, ptime, phealth;
+            int ptype;
+        };
+        auto fetch = [&](int x) {
+            RowState st{0u, false, 0.0, 0.0, 0.0, 0.0, 0.0, 0};
             const long long n = tileOf(x) * TILE + r;
-            float jF = 0.f, iF = 0.f, kF = 0.f, a0 = 0.f;
             if (n < L.count) {
-                tag.slot = L.order ? L.order[n] : (uint32_t)n;
-                const double pj = S.j[tag.slot], pi = S.i[tag.slot], pk = S.k[tag.slot];
-                const double ptime = S.time[tag.slot], phealth = S.health[tag.slot];
-                const int ptype = S.type[tag.slot];
+                st.valid = true;
+                st.slot = L.order ? L.order[n] : (uint32_t)n;
+                st.pj = S.j[st.slot];
+                st.pi = S.i[st.slot];
+                st.pk = S.k[st.slot];
+                st.ptime = S.time[st.slot];
+                st.phealth = S.health[st.slot];
+                st.ptype = S.type[st.slot];
+            }
+            return st;
+        };
+        auto prologue = [&](int x, const RowState &st) {
+            RowTag tag{0u, ROW_EMPTY, 0};
+            float jF = 0.f, iF = 0.f, kF = 0.f, a0 = 0.f;
+            if (st.valid) {
+                tag.slot = st.slot;
+                const double pj = st.pj, pi = st.pi, pk = st.pk;
+                const double ptime = st.ptime, phealth = st.phealth;
+                const int ptype = st.ptype;
                 tag.status = ROW_NONE;
                 if (phealth > 0 && ptime < T1) {
                     const double fj = floor(pj), fi = floor(pi), ck = ceil(pk);
@@ -736,14 +756,16 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
 
         RowTag cur{0u, ROW_EMPTY, 0}, next{0u, ROW_EMPTY, 0}, after{0u, ROW_EMPTY, 0};
         bool okCur = true, okNext = true;
-        if (nT > 0) cur = prologue(0);
-        if (nT > 1) next = prologue(1);
+        if (nT > 0) cur = prologue(0, fetch(0));
+        if (nT > 1) next = prologue(1, fetch(1));
         if (nT > 0) okCur = epilogue2(0);
         for (int k = 0; k < nT; k++) {
+            // the state gather of tile k+2 overlaps the epilogues below
+            const RowState ahead = fetch(k + 2);
             if (k + 1 < nT) okNext = epilogue2(k + 1);
             float o0, o1, o2;
             okCur = epilogue3(k, o0, o1, o2) && okCur;
-            if (k + 2 < nT) after = prologue(k + 2);
+            if (k + 2 < nT) after = prologue(k + 2, ahead);
             if (half == 0) post(cur, o0, o1, o2, okCur);
             // uniform stop decision of the row warps
             named_sync(1, 256);
