@@ -46,13 +46,13 @@ def measured_peaks(key="hbm_gbs", fallback=6650.0):
     return fallback, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per particle-step of the move kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "move_kernel_config3.md")
+def profile_traffic(summary="move_kernel_config3.md", key="traffic_bytes_per_particle_step"):
+    """DRAM bytes per unit of work of a kernel from its committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", summary)
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("traffic_bytes_per_particle_step:"):
+        if line.startswith(key + ":"):
             return float(line.split(":", 1)[1].strip().split()[0])
     return None
 
@@ -239,6 +239,9 @@ def surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, d
     per_launch_run = run / args.steps
     achieved = per_launch_run * SURROGATE_FLOP / (kernel_ms / 1000.0) / 1e12
     peak, peak_kind = measured_peaks("bf16_tflops", 1590.0)
+    per_particle = profile_traffic("surrogate_step_kernel_config3.md",
+                                   "traffic_bytes_per_particle_interval")
+    traffic = None if per_particle is None else per_particle * per_launch_run
     out = {"value": steps_total / (elapsed_ms / 1000.0), "unit": "particle-steps/s",
            "ms_per_step": elapsed_ms / args.steps, "storage": "fp16",
            "moved_by_surrogate_per_step": per_launch_run, "fallback_per_step": fallback / args.steps,
@@ -247,7 +250,8 @@ def surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, d
                         "frac": achieved / peak, "peak_source": peak_kind,
                         "kernel": "surrogate_step_kernel", "kernel_ms": kernel_ms,
                         "flop_per_particle_interval": SURROGATE_FLOP,
-                        "cell_kernel_ms": statistics.mean(cell_ms), "traffic": None}}
+                        "cell_kernel_ms": statistics.mean(cell_ms),
+                        "traffic": traffic}}
     if rank == 0:
         n = min(len(particles), 1 << 20)
         sub = particles[:n].copy()
