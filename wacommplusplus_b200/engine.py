@@ -121,6 +121,7 @@ class Engine:
         self._check(self._lib.wacomm_b200_set_config(self._ctx, ctypes.byref(cfg)))
 
     def set_grid(self, eta, xi, s_rho, s_w, lon_rad, lat_rad, h, depth_intervals, mask=None):
+        self._grid_shape = (s_rho, eta, xi)
         keep = [_d(lon_rad), _d(lat_rad), _d(h), _d(depth_intervals), _d(mask)]
         ptrs = [None if k is None else k[1] for k in keep]
         self._check(self._lib.wacomm_b200_set_grid(self._ctx, eta, xi, s_rho, s_w, ptrs[4], ptrs[0],
@@ -255,8 +256,7 @@ class Engine:
         self._check(self._lib.wacomm_b200_concentration_count(self._ctx, conc_time_index))
 
     def _conc_shape(self):
-        w = self.window
-        return (self._conc_times, w.sRho, w.eta, w.xi)
+        return (self._conc_times,) + self._grid_shape
 
     def concentration(self):
         out = np.zeros(self._conc_shape(), dtype=np.uint32)
