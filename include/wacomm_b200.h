@@ -17,6 +17,9 @@
  *                                                               Sources.cpp:233-249 (wacomm_b200_emit)
  *   - OceanModelAdapter::kji2deplatlon                          OceanModelAdapter.cpp:271-327
  *                                                               (wacomm_b200_geo_positions)
+ *   - EnvironmentalRegridder::bilinearGeographic /              EnvironmentalRegridder.cpp:239-334,
+ *     bilinearCurvilinearGeographic of wind and Stokes fields   WacommPlusPlus.cpp:162-173
+ *                                                               (wacomm_b200_regrid_environment)
  * The drop-in C++ launcher with the reference's exact signature is declared in
  * include/wacomm_b200_kernel.h.
  */
@@ -233,6 +236,40 @@ int wacomm_b200_set_geo_grid(wacomm_b200_context *ctx, const double *lon, const 
  * outside the grid or its valid levels. Requires set_grid and set_geo_grid. */
 int wacomm_b200_geo_positions(wacomm_b200_context *ctx, double *depth, double *lat, double *lon,
                               size_t n);
+
+/* Wind (10 m) and Stokes drift fields on their own grids and times, regridded on the device to the
+ * rho nodes of set_geo_grid and aligned to the set_times forcing times. Replaces the host
+ * regridding the reference runs before its move loop (WacommPlusPlus.cpp:162-173, reaching
+ * EnvironmentalRegridder::bilinearGeographic / bilinearCurvilinearGeographic,
+ * EnvironmentalRegridder.cpp:239-334) and its same-grid, same-times requirement
+ * (Wacomm.cpp:70-84).
+ *   method GEOGRAPHIC: rectilinear source (lon depends on i only, lat on j only, 1e-10);
+ *   method CURVILINEAR: any non-folded source grid, each target found by Newton inversion in the
+ *   reference's cell index.
+ * src_lon/src_lat [src_eta][src_xi] degrees; u, v [src_times][src_eta][src_xi]; times
+ * [src_times] seconds, strictly increasing. A forcing time equal to a source time (1e-6 s) takes
+ * that record; one between two source times blends the two regridded values linearly in time
+ * (no reference counterpart: the reference requires equal times). Errors, as the reference
+ * throws: a target outside the source grid or times (no extrapolation), a non-rectilinear
+ * source for GEOGRAPHIC, a folded cell holding a target, non-finite values; also longitudes more
+ * than 3600 degrees apart, where the reference's wrapping loop would not end. On error the field
+ * is left unset. The regridded fields stay resident ([T][eta][xi] float per component) and feed
+ * every interval whose records were uploaded without that field; an upload with the field takes
+ * precedence for its record. Synchronous. */
+#define WACOMM_B200_FIELD_WIND 0
+#define WACOMM_B200_FIELD_STOKES 1
+#define WACOMM_B200_REGRID_BILINEAR_GEOGRAPHIC 0
+#define WACOMM_B200_REGRID_BILINEAR_CURVILINEAR_GEOGRAPHIC 1
+int wacomm_b200_regrid_environment(wacomm_b200_context *ctx, int field, int method, int src_eta,
+                                   int src_xi, const double *src_lon, const double *src_lat,
+                                   int src_times, const double *times, const float *u,
+                                   const float *v);
+
+/* Drops a regridded field (wind or Stokes). */
+int wacomm_b200_clear_environment(wacomm_b200_context *ctx, int field);
+
+/* Copies forcing time t of a regridded field into host arrays of eta*xi values. */
+int wacomm_b200_get_environment(wacomm_b200_context *ctx, int field, int t, float *u, float *v);
 
 /* Concentration grid of n_conc_times records [n_conc_times][s_rho][eta][xi] as uint32 counts.
  * reset zeroes it; count adds the resident alive particles at conc_time_index

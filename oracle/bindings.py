@@ -272,3 +272,75 @@ def deplatlon2kji(grid, dep, lat, lon):
     if status != 0:
         return None
     return k.value, j.value, i.value
+
+
+REF_REGRID_SO = os.path.join(HERE, "_ref", "libwacomm_ref_regrid.so")
+REGRID_METHODS = ("geographic", "curvilinear")
+_ref_regrid = None
+
+
+def _regrid_argtypes(fn):
+    i32, lng = ctypes.c_int, ctypes.c_long
+    fn.restype = i32
+    fn.argtypes = [i32, i32, _c_double_p, _c_double_p, i32, _c_float_p, lng, _c_double_p,
+                   _c_double_p, _c_float_p]
+
+
+def ref_regrid_available():
+    return os.path.exists(REF_REGRID_SO)
+
+
+def ref_regrid_lib():
+    global _ref_regrid
+    if _ref_regrid is None:
+        if not ref_regrid_available():
+            raise RuntimeError(f"reference regridder build missing: {REF_REGRID_SO}")
+        lib = ctypes.CDLL(REF_REGRID_SO)
+        _regrid_argtypes(lib.ref_regrid_geographic)
+        _regrid_argtypes(lib.ref_regrid_curvilinear)
+        _ref_regrid = lib
+    return _ref_regrid
+
+
+def regrid(lib_kind, method, lon, lat, src, target_lon, target_lat):
+    """Bilinear regridding of src[T, eta, xi] (or [eta, xi]) from the source grid lon/lat
+    [eta, xi] (degrees) to the targets; returns (code, out[T, *target.shape]). lib_kind is
+    "oracle" (the restatement) or "ref" (the reference's EnvironmentalRegridder)."""
+    lon = np.ascontiguousarray(lon, dtype=np.float64)
+    lat = np.ascontiguousarray(lat, dtype=np.float64)
+    src = np.ascontiguousarray(src, dtype=np.float32)
+    squeeze = src.ndim == 2
+    if squeeze:
+        src = src[None]
+    tshape = np.shape(target_lon)
+    tlon = np.ascontiguousarray(target_lon, dtype=np.float64).ravel()
+    tlat = np.ascontiguousarray(target_lat, dtype=np.float64).ravel()
+    out = np.zeros((src.shape[0], tlon.size), dtype=np.float32)
+    if lib_kind == "oracle":
+        fn = getattr(oracle_lib(), f"wo_regrid_{method}")
+        if fn.argtypes is None:
+            _regrid_argtypes(fn)
+    else:
+        fn = getattr(ref_regrid_lib(), f"ref_regrid_{method}")
+    eta, xi = lon.shape
+    rc = fn(eta, xi, _dptr(lon), _dptr(lat), src.shape[0], _fptr(src), tlon.size, _dptr(tlon),
+            _dptr(tlat), _fptr(out))
+    out = out.reshape((src.shape[0],) + tshape)
+    return rc, (out[0] if squeeze else out)
+
+
+def align_times(src_times, src, dst_times):
+    """wo_align_times: src[nSrc, ...] at src_times to dst_times; returns (code, out)."""
+    lib = oracle_lib()
+    fn = lib.wo_align_times
+    if fn.argtypes is None:
+        fn.restype = ctypes.c_int
+        fn.argtypes = [ctypes.c_int, _c_double_p, ctypes.c_long, _c_float_p, ctypes.c_int,
+                       _c_double_p, _c_float_p]
+    st = np.ascontiguousarray(src_times, dtype=np.float64)
+    dt = np.ascontiguousarray(dst_times, dtype=np.float64)
+    src = np.ascontiguousarray(src, dtype=np.float32)
+    plane = int(np.prod(src.shape[1:]))
+    out = np.zeros((dt.size,) + src.shape[1:], dtype=np.float32)
+    rc = fn(st.size, _dptr(st), plane, _fptr(src), dt.size, _dptr(dt), _fptr(out))
+    return rc, out

@@ -1009,3 +1009,333 @@ int wo_deplatlon2kji(int eta, int xi, int sW, const double *lon, const double *l
 #undef AT
     return 0;
 }
+
+/* ------------------------------------------------------------------------------------------
+ * Environmental regridding (EnvironmentalRegridder.cpp)
+ * ------------------------------------------------------------------------------------------ */
+
+/* nearLongitude / longitudeBranch (EnvironmentalRegridder.cpp:37-48) */
+static double rg_near(double value, double reference) {
+    while (value - reference > 180) value -= 360;
+    while (value - reference < -180) value += 360;
+    return value;
+}
+
+/* bilinear (EnvironmentalRegridder.cpp:50-52) */
+static double rg_bilinear(double f00, double f10, double f01, double f11, double x, double y) {
+    return (1 - x) * (1 - y) * f00 + x * (1 - y) * f10 + (1 - x) * y * f01 + x * y * f11;
+}
+
+/* bracket (EnvironmentalRegridder.cpp:14-28): the first interval of a strictly monotonic axis
+ * that holds value within 1e-10. */
+static int rg_bracket(const double *axis, int n, double value, int *lower, double *weight) {
+    int increasing = axis[n - 1] > axis[0];
+    for (int i = 1; i < n; i++)
+        if ((increasing && axis[i] <= axis[i - 1]) || (!increasing && axis[i] >= axis[i - 1]))
+            return WO_REGRID_GRID;
+    double minimum = increasing ? axis[0] : axis[n - 1];
+    double maximum = increasing ? axis[n - 1] : axis[0];
+    if (value < minimum - 1.e-10 || value > maximum + 1.e-10) return WO_REGRID_OUTSIDE;
+    for (int i = 0; i + 1 < n; i++) {
+        if ((increasing && value >= axis[i] - 1.e-10 && value <= axis[i + 1] + 1.e-10) ||
+            (!increasing && value <= axis[i] + 1.e-10 && value >= axis[i + 1] - 1.e-10)) {
+            *lower = i;
+            *weight = (value - axis[i]) / (axis[i + 1] - axis[i]);
+            return 0;
+        }
+    }
+    return WO_REGRID_OUTSIDE;
+}
+
+/* std::max(0.0, std::min(1.0, v)), signed zeros included */
+static double rg_unit(double v) {
+    double m = v < 1.0 ? v : 1.0;
+    return 0.0 < m ? m : 0.0;
+}
+
+static int rg_fields_finite(int T, long plane, const float *src) {
+    for (long n = 0; n < (long)T * plane; n++)
+        if (!isfinite(src[n])) return WO_REGRID_FIELD;
+    return 0;
+}
+
+int wo_regrid_geographic(int eta, int xi, const double *lon, const double *lat, int T,
+                         const float *src, long nTarget, const double *tLon, const double *tLat,
+                         float *out) {
+    if (eta < 2 || xi < 2) return WO_REGRID_GRID;
+    double *axisX = malloc(sizeof(double) * (size_t)xi);
+    double *axisY = malloc(sizeof(double) * (size_t)eta);
+    int rc = 0;
+    for (int i = 0; i < xi; i++) axisX[i] = lon[i];
+    for (int j = 0; j < eta; j++) axisY[j] = lat[(size_t)j * xi];
+    for (int j = 0; j < eta && !rc; j++)
+        for (int i = 0; i < xi && !rc; i++) {
+            double x = lon[(size_t)j * xi + i], y = lat[(size_t)j * xi + i];
+            if (!isfinite(x) || !isfinite(y) || fabs(x - axisX[i]) > 1.e-10 ||
+                fabs(y - axisY[j]) > 1.e-10)
+                rc = WO_REGRID_GRID;
+        }
+    /* unwrapLongitude (EnvironmentalRegridder.cpp:30-35) */
+    for (int i = 1; i < xi && !rc; i++) {
+        while (axisX[i] - axisX[i - 1] > 180) axisX[i] -= 360;
+        while (axisX[i] - axisX[i - 1] < -180) axisX[i] += 360;
+    }
+    if (!rc && fabs(axisX[xi - 1] - axisX[0]) > 360 + 1.e-10) rc = WO_REGRID_GRID;
+    const long plane = (long)eta * xi;
+    if (!rc) rc = rg_fields_finite(T, plane, src);
+    double center = .5 * (axisX[0] + axisX[xi - 1]);
+    for (long n = 0; n < nTarget && !rc; n++) {
+        if (!isfinite(tLon[n]) || !isfinite(tLat[n])) {
+            rc = WO_REGRID_TARGET;
+            break;
+        }
+        int xl = 0, yl = 0;
+        double wx = 0, wy = 0;
+        rc = rg_bracket(axisX, xi, rg_near(tLon[n], center), &xl, &wx);
+        if (!rc) rc = rg_bracket(axisY, eta, tLat[n], &yl, &wy);
+        if (rc) break;
+        for (int t = 0; t < T; t++) {
+            const float *s = src + (size_t)t * plane;
+            double lower = s[(size_t)yl * xi + xl] * (1 - wx) + s[(size_t)yl * xi + xl + 1] * wx;
+            double upper = s[(size_t)(yl + 1) * xi + xl] * (1 - wx) +
+                           s[(size_t)(yl + 1) * xi + xl + 1] * wx;
+            out[(size_t)t * nTarget + n] = (float)(lower * (1 - wy) + upper * wy);
+        }
+    }
+    free(axisX);
+    free(axisY);
+    return rc;
+}
+
+/* CurvilinearCellIndex (EnvironmentalRegridder.cpp:170-236), cyclic longitude */
+typedef struct rg_index {
+    long cells;
+    double *box;        /* [cells][4] minimumX, maximumX, minimumY, maximumY */
+    long *binStart;     /* [bins + 1] */
+    long *binCells;
+    double minX, maxX, minY, maxY, reference;
+    int binsX, binsY;
+} rg_index;
+
+static int rg_xbin(const rg_index *ix, double v) {
+    if (ix->maxX == ix->minX) return 0;
+    int b = (int)((v - ix->minX) / (ix->maxX - ix->minX) * ix->binsX);
+    return b < 0 ? 0 : (b > ix->binsX - 1 ? ix->binsX - 1 : b);
+}
+
+static int rg_ybin(const rg_index *ix, double v) {
+    if (ix->maxY == ix->minY) return 0;
+    int b = (int)((v - ix->minY) / (ix->maxY - ix->minY) * ix->binsY);
+    return b < 0 ? 0 : (b > ix->binsY - 1 ? ix->binsY - 1 : b);
+}
+
+static double rg_min4(double a, double b, double c, double d) {
+    double l = b < a ? b : a, r = d < c ? d : c;  /* std::min(std::min(a,b),std::min(c,d)) */
+    return r < l ? r : l;
+}
+
+static double rg_max4(double a, double b, double c, double d) {
+    double l = a < b ? b : a, r = c < d ? d : c;  /* std::max(std::max(a,b),std::max(c,d)) */
+    return l < r ? r : l;
+}
+
+static int rg_index_build(rg_index *ix, int eta, int xi, const double *lon, const double *lat) {
+    memset(ix, 0, sizeof *ix);
+    double reference = lon[0];
+    if (!isfinite(reference)) return WO_REGRID_GRID;
+    ix->cells = (long)(eta - 1) * (xi - 1);
+    ix->box = malloc(sizeof(double) * 4 * (size_t)ix->cells);
+    for (int j = 0; j + 1 < eta; j++)
+        for (int i = 0; i + 1 < xi; i++) {
+#define L(jj, ii) lon[(size_t)(jj) * xi + (ii)]
+#define A(jj, ii) lat[(size_t)(jj) * xi + (ii)]
+            double x00 = L(j, i), x10 = rg_near(L(j, i + 1), x00);
+            double x01 = rg_near(L(j + 1, i), x00), x11 = rg_near(L(j + 1, i + 1), x00);
+            double y00 = A(j, i), y10 = A(j, i + 1), y01 = A(j + 1, i), y11 = A(j + 1, i + 1);
+#undef L
+#undef A
+            if (!isfinite(x00) || !isfinite(x10) || !isfinite(x01) || !isfinite(x11) ||
+                !isfinite(y00) || !isfinite(y10) || !isfinite(y01) || !isfinite(y11))
+                return WO_REGRID_GRID;
+            double center = .25 * (x00 + x10 + x01 + x11);
+            double shift = 360 * round((reference - center) / 360);
+            double *b = ix->box + 4 * ((size_t)j * (xi - 1) + i);
+            b[0] = rg_min4(x00, x10, x01, x11) + shift;
+            b[1] = rg_max4(x00, x10, x01, x11) + shift;
+            b[2] = rg_min4(y00, y10, y01, y11);
+            b[3] = rg_max4(y00, y10, y01, y11);
+        }
+    ix->minX = ix->box[0];
+    ix->maxX = ix->box[1];
+    ix->minY = ix->box[2];
+    ix->maxY = ix->box[3];
+    for (long c = 0; c < ix->cells; c++) {
+        const double *b = ix->box + 4 * c;
+        ix->minX = b[0] < ix->minX ? b[0] : ix->minX;  /* std::min(minimumX, cell) */
+        ix->maxX = ix->maxX < b[1] ? b[1] : ix->maxX;
+        ix->minY = b[2] < ix->minY ? b[2] : ix->minY;
+        ix->maxY = ix->maxY < b[3] ? b[3] : ix->maxY;
+    }
+    double width = ix->maxX - ix->minX, height = ix->maxY - ix->minY;
+    width = width < 1.e-12 ? 1.e-12 : width;
+    height = height < 1.e-12 ? 1.e-12 : height;
+    double scale = sqrt((double)ix->cells);
+    int bx = (int)round(scale * sqrt(width / height)), by = (int)round(scale * sqrt(height / width));
+    bx = bx < 1 ? 1 : bx;
+    by = by < 1 ? 1 : by;
+    ix->binsX = bx < ix->cells ? bx : (int)ix->cells;
+    ix->binsY = by < ix->cells ? by : (int)ix->cells;
+    long bins = (long)ix->binsX * ix->binsY;
+    ix->binStart = calloc((size_t)bins + 1, sizeof(long));
+    for (int pass = 0; pass < 2; pass++) {
+        long *fill = pass ? calloc((size_t)bins, sizeof(long)) : NULL;
+        for (long c = 0; c < ix->cells; c++) {
+            const double *b = ix->box + 4 * c;
+            int i0 = rg_xbin(ix, b[0]), i1 = rg_xbin(ix, b[1]);
+            int j0 = rg_ybin(ix, b[2]), j1 = rg_ybin(ix, b[3]);
+            for (int jj = j0; jj <= j1; jj++)
+                for (int ii = i0; ii <= i1; ii++) {
+                    long bin = (long)jj * ix->binsX + ii;
+                    if (pass) ix->binCells[ix->binStart[bin] + fill[bin]++] = c;
+                    else ix->binStart[bin + 1]++;
+                }
+        }
+        if (!pass) {
+            for (long b = 0; b < bins; b++) ix->binStart[b + 1] += ix->binStart[b];
+            ix->binCells = malloc(sizeof(long) * ((size_t)ix->binStart[bins] + 1));
+        }
+        free(fill);
+    }
+    ix->reference = reference;
+    return 0;
+}
+
+static void rg_index_free(rg_index *ix) {
+    free(ix->box);
+    free(ix->binStart);
+    free(ix->binCells);
+}
+
+int wo_regrid_curvilinear(int eta, int xi, const double *lon, const double *lat, int T,
+                          const float *src, long nTarget, const double *tLon, const double *tLat,
+                          float *out) {
+    if (eta < 2 || xi < 2) return WO_REGRID_GRID;
+    const long plane = (long)eta * xi;
+    int rc = rg_fields_finite(T, plane, src);
+    if (rc) return rc;
+    rg_index ix;
+    rc = rg_index_build(&ix, eta, xi, lon, lat);
+    for (long n = 0; n < nTarget && !rc; n++) {
+        double targetX = tLon[n], targetY = tLat[n];
+        if (!isfinite(targetX) || !isfinite(targetY)) {
+            rc = WO_REGRID_TARGET;
+            break;
+        }
+        /* candidates(): the longitude is moved to the branch of the index reference first */
+        targetX = rg_near(targetX, ix.reference);
+        long first = 0, last = 0;
+        if (!(targetX < ix.minX - 1.e-10 || targetX > ix.maxX + 1.e-10 ||
+              targetY < ix.minY - 1.e-10 || targetY > ix.maxY + 1.e-10)) {
+            long bin = (long)rg_ybin(&ix, targetY) * ix.binsX + rg_xbin(&ix, targetX);
+            first = ix.binStart[bin];
+            last = ix.binStart[bin + 1];
+        }
+        int foundJ = -1, foundI = -1;
+        double foundX = 0, foundY = 0;
+        for (long c = first; c < last; c++) {
+            long cell = ix.binCells[c];
+            int j = (int)(cell / (xi - 1)), i = (int)(cell % (xi - 1));
+#define L(jj, ii) lon[(size_t)(jj) * xi + (ii)]
+#define A(jj, ii) lat[(size_t)(jj) * xi + (ii)]
+            double x00 = rg_near(L(j, i), targetX), x10 = rg_near(L(j, i + 1), targetX);
+            double x01 = rg_near(L(j + 1, i), targetX), x11 = rg_near(L(j + 1, i + 1), targetX);
+            double y00 = A(j, i), y10 = A(j, i + 1), y01 = A(j + 1, i), y11 = A(j + 1, i + 1);
+#undef L
+#undef A
+            if (!isfinite(x00) || !isfinite(x10) || !isfinite(x01) || !isfinite(x11) ||
+                !isfinite(y00) || !isfinite(y10) || !isfinite(y01) || !isfinite(y11)) {
+                rc = WO_REGRID_GRID;
+                break;
+            }
+            const double *b = ix.box + 4 * cell;
+            if (targetX < b[0] - 1.e-10 || targetX > b[1] + 1.e-10 || targetY < b[2] - 1.e-10 ||
+                targetY > b[3] + 1.e-10)
+                continue;
+            double x = .5, y = .5;
+            for (int iteration = 0; iteration < 20; iteration++) {
+                double mappedX = rg_bilinear(x00, x10, x01, x11, x, y);
+                double mappedY = rg_bilinear(y00, y10, y01, y11, x, y);
+                double dXdx = (1 - y) * (x10 - x00) + y * (x11 - x01);
+                double dXdy = (1 - x) * (x01 - x00) + x * (x11 - x10);
+                double dYdx = (1 - y) * (y10 - y00) + y * (y11 - y01);
+                double dYdy = (1 - x) * (y01 - y00) + x * (y11 - y10);
+                double determinant = dXdx * dYdy - dXdy * dYdx;
+                if (fabs(determinant) < 1.e-14) break;
+                double residualX = mappedX - targetX, residualY = mappedY - targetY;
+                x -= (dYdy * residualX - dXdy * residualY) / determinant;
+                y -= (-dYdx * residualX + dXdx * residualY) / determinant;
+            }
+            double residual = hypot(rg_bilinear(x00, x10, x01, x11, x, y) - targetX,
+                                    rg_bilinear(y00, y10, y01, y11, x, y) - targetY);
+            if (x >= -1.e-9 && x <= 1 + 1.e-9 && y >= -1.e-9 && y <= 1 + 1.e-9 &&
+                residual < 1.e-8) {
+                double d00 = (x10 - x00) * (y01 - y00) - (x01 - x00) * (y10 - y00);
+                double d10 = (x10 - x00) * (y11 - y10) - (x11 - x10) * (y10 - y00);
+                double d01 = (x11 - x01) * (y01 - y00) - (x01 - x00) * (y11 - y01);
+                double d11 = (x11 - x01) * (y11 - y10) - (x11 - x10) * (y11 - y01);
+                if (fabs(d00) < 1.e-14 || d00 * d10 <= 0 || d00 * d01 <= 0 || d00 * d11 <= 0) {
+                    rc = WO_REGRID_FOLDED;
+                    break;
+                }
+                foundJ = j;
+                foundI = i;
+                foundX = rg_unit(x);
+                foundY = rg_unit(y);
+                break;
+            }
+        }
+        if (rc) break;
+        if (foundJ < 0) {
+            rc = WO_REGRID_OUTSIDE;
+            break;
+        }
+        for (int t = 0; t < T; t++) {
+            const float *s = src + (size_t)t * plane;
+            size_t o = (size_t)foundJ * xi + foundI;
+            out[(size_t)t * nTarget + n] =
+                (float)rg_bilinear(s[o], s[o + 1], s[o + xi], s[o + xi + 1], foundX, foundY);
+        }
+    }
+    rg_index_free(&ix);
+    return rc;
+}
+
+int wo_align_times(int nSrc, const double *srcTimes, long plane, const float *src, int nDst,
+                   const double *dstTimes, float *out) {
+    if (nSrc < 1) return WO_REGRID_TIME;
+    for (int s = 1; s < nSrc; s++)
+        if (!(srcTimes[s] > srcTimes[s - 1])) return WO_REGRID_TIME;
+    for (int d = 0; d < nDst; d++) {
+        double t = dstTimes[d];
+        int k0 = -1, k1 = -1;
+        for (int s = 0; s < nSrc && k0 < 0; s++)
+            if (fabs(t - srcTimes[s]) <= 1.e-6) k0 = k1 = s;
+        for (int s = 0; s + 1 < nSrc && k0 < 0; s++)
+            if (t > srcTimes[s] && t < srcTimes[s + 1]) {
+                k0 = s;
+                k1 = s + 1;
+            }
+        if (k0 < 0) return WO_REGRID_TIME;
+        /* timeWeight (NumericalHelpers.hpp:30-33) */
+        double alpha = 0.0;
+        if (k1 != k0) {
+            alpha = (t - srcTimes[k0]) / (srcTimes[k1] - srcTimes[k0]);
+            alpha = rg_unit(alpha);
+        }
+        const float *a = src + (size_t)k0 * plane, *b = src + (size_t)k1 * plane;
+        float *o = out + (size_t)d * plane;
+        for (long n = 0; n < plane; n++)
+            o[n] = k1 == k0 ? a[n] : (float)((1.0 - alpha) * a[n] + alpha * b[n]);
+    }
+    return 0;
+}

@@ -144,6 +144,36 @@ int wo_deplatlon2kji(int eta, int xi, int sW, const double *lon, const double *l
                      const double *h, const double *sWValues, double dep, double latIn,
                      double lonIn, double *k, double *j, double *i);
 
+/* Environmental regridding to target nodes (EnvironmentalRegridder.cpp). Source coordinates
+ * lon/lat [eta][xi] in degrees, source fields src[T][eta][xi], targets tLon/tLat[nTarget],
+ * results out[T][nTarget]. Return 0, or a negative code where the reference throws:
+ * WO_REGRID_GRID (source grid invalid: dimensions, not rectilinear, non-monotonic axis, span),
+ * WO_REGRID_OUTSIDE (a target outside the source grid: extrapolation is prohibited),
+ * WO_REGRID_FIELD (a non-finite source value), WO_REGRID_FOLDED (a folded or singular cell),
+ * WO_REGRID_TARGET (a non-finite target coordinate). */
+#define WO_REGRID_GRID (-1)
+#define WO_REGRID_OUTSIDE (-2)
+#define WO_REGRID_FIELD (-3)
+#define WO_REGRID_FOLDED (-4)
+#define WO_REGRID_TARGET (-5)
+#define WO_REGRID_TIME (-6)
+/* bilinearGeographic (EnvironmentalRegridder.cpp:239-275): rectilinear source axes. */
+int wo_regrid_geographic(int eta, int xi, const double *lon, const double *lat, int T,
+                         const float *src, long nTarget, const double *tLon, const double *tLat,
+                         float *out);
+/* bilinearCurvilinearGeographic (EnvironmentalRegridder.cpp:277-334) with the cell index of
+ * CurvilinearCellIndex (:170-236): first cell in index order that holds the target. */
+int wo_regrid_curvilinear(int eta, int xi, const double *lon, const double *lat, int T,
+                          const float *src, long nTarget, const double *tLon, const double *tLat,
+                          float *out);
+/* Aligns records at srcTimes[nSrc] (strictly increasing) to dstTimes[nDst]: each destination
+ * time between two source times (1e-6 s tolerance at the ends, the tolerance of the reference's
+ * time check, Wacomm.cpp:70-84) takes (float)((1-a)*x0 + a*x1) with a = timeWeight
+ * (NumericalHelpers.hpp:30-39); a destination time equal to a source time copies that record.
+ * plane values per record; out[nDst][plane]. The reference requires equal times instead. */
+int wo_align_times(int nSrc, const double *srcTimes, long plane, const float *src, int nDst,
+                   const double *dstTimes, float *out);
+
 #ifdef __cplusplus
 }
 #endif

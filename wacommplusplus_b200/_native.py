@@ -24,6 +24,8 @@ ARITH_REFERENCE, ARITH_FP32 = 0, 1
 STORAGE_FP32, STORAGE_FP16, STORAGE_BF16 = 0, 1, 2
 RNG_REFERENCE, RNG_PHILOX = 0, 1
 EMISSION_UNIFORM_RATE, EMISSION_FORCING_INTERVAL_BATCH, EMISSION_SINGLE_PULSE = 0, 1, 2
+FIELD_WIND, FIELD_STOKES = 0, 1
+REGRID_BILINEAR_GEOGRAPHIC, REGRID_BILINEAR_CURVILINEAR_GEOGRAPHIC = 0, 1
 
 
 class options_t(ctypes.Structure):
@@ -64,6 +66,9 @@ SIGNATURES = {
     "wacomm_b200_emit": (_i, [_vp, _vp, _i, _d, _d, _d, ctypes.POINTER(_sz)]),
     "wacomm_b200_set_geo_grid": (_i, [_vp, _dp, _dp, _dp]),
     "wacomm_b200_geo_positions": (_i, [_vp, _dp, _dp, _dp, _sz]),
+    "wacomm_b200_regrid_environment": (_i, [_vp, _i, _i, _i, _i, _dp, _dp, _i, _dp, _fp, _fp]),
+    "wacomm_b200_clear_environment": (_i, [_vp, _i]),
+    "wacomm_b200_get_environment": (_i, [_vp, _i, _i, _fp, _fp]),
     "wacomm_b200_concentration_reset": (_i, [_vp, _i]),
     "wacomm_b200_concentration_count": (_i, [_vp, _i]),
     "wacomm_b200_concentration_get": (_i, [_vp, _vp, _sz]),

@@ -36,6 +36,10 @@ struct SoABuffers {
 
 constexpr size_t MAX_PARTICLES = (size_t)1 << 31;  // uint32 work indices
 
+struct EnvField {
+    float *u = nullptr, *v = nullptr;
+};
+
 }  // namespace
 
 struct wacomm_b200_context {
@@ -113,6 +117,9 @@ struct wacomm_b200_context {
     double *dGeoLon = nullptr, *dGeoLat = nullptr, *dSWValues = nullptr;  // kji2deplatlon grid
     bool hasGeo = false;
     double *dGeoOut = nullptr;  // [3][n] depth, lat, lon
+    // Wind (0) and Stokes (1) fields regridded to the rho nodes and the forcing times, [T][eta][xi]
+    // each; a frame's own uploaded fields take precedence over these.
+    EnvField env[2];
     size_t geoOutCap = 0;
 
     unsigned long long *dSteps = nullptr;
@@ -305,12 +312,33 @@ void release_frames(wacomm_b200_context *ctx) {
     ctx->zT0 = ctx->zT1 = -1;
 }
 
-FrameDevice frame_of(const FrameSlot &s) {
-    return FrameDevice{s.zeta, s.u, s.v, s.w, s.akt, s.windU, s.windV, s.stokesU, s.stokesV};
+// Forcing record t: the slot's own fields, with the wind and Stokes pairs taken from the regridded
+// environment where the record was uploaded without them.
+FrameDevice frame_of(const wacomm_b200_context *ctx, int t) {
+    const FrameSlot &s = ctx->slots[t];
+    FrameDevice f{s.zeta, s.u, s.v, s.w, s.akt, s.windU, s.windV, s.stokesU, s.stokesV};
+    const size_t at = (size_t)t * ctx->eta * ctx->xi;
+    if (!s.windU && !s.windV && ctx->env[0].u) {
+        f.windU = ctx->env[0].u + at;
+        f.windV = ctx->env[0].v + at;
+    }
+    if (!s.stokesU && ctx->env[1].u) {
+        f.stokesU = ctx->env[1].u + at;
+        f.stokesV = ctx->env[1].v + at;
+    }
+    return f;
+}
+
+void release_environment(wacomm_b200_context *ctx) {
+    for (EnvField &e : ctx->env) {
+        cudaFree(e.u);
+        cudaFree(e.v);
+        e = EnvField{};
+    }
 }
 
 int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
-    const FrameSlot &a = ctx->slots[t0], &b = ctx->slots[t1];
+    const FrameDevice a = frame_of(ctx, t0), b = frame_of(ctx, t1);
     bool env = a.windU || a.windV || a.stokesU || b.windU || b.windV || b.stokesU;
     bool cells = ctx->opt.arithmetic == WACOMM_B200_ARITH_FP32;
     if (ctx->pairT0 == t0 && ctx->pairT1 == t1 && ctx->pairStorage == ctx->opt.storage &&
@@ -326,7 +354,7 @@ int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
         ctx->nodesBytes = need;
     }
     if (env && !ctx->dEnv) CUDA_TRY(ctx, cudaMalloc(&ctx->dEnv, plane * sizeof(EnvPair)));
-    CUDA_TRY(ctx, pack_pair(ctx->opt.storage, ctx->eta, ctx->xi, ctx->sW, frame_of(a), frame_of(b),
+    CUDA_TRY(ctx, pack_pair(ctx->opt.storage, ctx->eta, ctx->xi, ctx->sW, a, b,
                             ctx->dH, ctx->dNodes, ctx->dSurf, env ? ctx->dEnv : nullptr,
                             ctx->stream));
     launches += 2;
@@ -347,8 +375,8 @@ int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
             CUDA_TRY(ctx, cudaMalloc(&ctx->dCellSurface, sneed));
             ctx->cellSurfaceBytes = sneed;
         }
-        CUDA_TRY(ctx, pack_cells(ctx->opt.storage, ctx->eta, ctx->xi, ctx->sW, frame_of(a),
-                                 frame_of(b), ctx->dH, ctx->dCells, ctx->dCellSurface, ctx->stream));
+        CUDA_TRY(ctx, pack_cells(ctx->opt.storage, ctx->eta, ctx->xi, ctx->sW, a, b, ctx->dH,
+                                 ctx->dCells, ctx->dCellSurface, ctx->stream));
         launches += 2;
     }
     ctx->pairT0 = t0;
@@ -368,7 +396,7 @@ PackedArgs packed_args(wacomm_b200_context *ctx) {
     A.nodes = ctx->dNodes;
     A.surf = ctx->dSurf;
     A.env = ctx->pairEnv ? ctx->dEnv : nullptr;
-    const FrameSlot &a = ctx->slots[ctx->pairT0];
+    const FrameDevice a = frame_of(ctx, ctx->pairT0);
     A.hasWindU = ctx->pairEnv && a.windU;
     A.hasWindV = ctx->pairEnv && a.windV;
     A.hasStokes = ctx->pairEnv && a.stokesU && a.stokesV;
@@ -488,7 +516,7 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     const size_t count = ctx->n;
     if (count == 0) return WACOMM_B200_OK;
     int rc;
-    const FrameSlot &a = ctx->slots[P.t0], &b = ctx->slots[P.t1];
+    const FrameDevice a = frame_of(ctx, P.t0), b = frame_of(ctx, P.t1);
     // dry-node table
     const size_t dryNeed = (size_t)(ctx->eta + 1) * (ctx->xi + 1);
     if (!ctx->dryValid || !(ctx->dryShore == ctx->cfg.shoreLimit)) {
@@ -514,7 +542,7 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
             CUDA_TRY(ctx, cudaMalloc(&ctx->dCorners, (size_t)nCL * surrogate_corner_bytes()));
             ctx->zCap = (size_t)nCL;
         }
-        CUDA_TRY(ctx, surrogate_cells(ctx->eta, ctx->xi, ctx->sW, ctx->sRho, frame_of(a), frame_of(b),
+        CUDA_TRY(ctx, surrogate_cells(ctx->eta, ctx->xi, ctx->sW, ctx->sRho, a, b,
                                       ctx->dH, ctx->dDepth, ctx->dMetric, ctx->dSurrogate, ctx->dZ,
                                       ctx->dCorners, ctx->dErr, ctx->smCount, ctx->stream));
         launches++;
@@ -718,6 +746,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dGeoLat);
     cudaFree(ctx->dSWValues);
     cudaFree(ctx->dGeoOut);
+    release_environment(ctx);
     cudaFree(ctx->dSteps);
     cudaFree(ctx->dErr);
     cudaFree(ctx->dCfg);
@@ -806,6 +835,7 @@ int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, i
     cudaFree(ctx->dSWValues);
     ctx->dGeoLon = ctx->dGeoLat = ctx->dSWValues = nullptr;
     ctx->hasGeo = false;
+    release_environment(ctx);
     CUDA_TRY(ctx, cudaMalloc(&ctx->dLon, plane * sizeof(double)));
     CUDA_TRY(ctx, cudaMalloc(&ctx->dLat, plane * sizeof(double)));
     CUDA_TRY(ctx, cudaMalloc(&ctx->dH, plane * sizeof(double)));
@@ -847,6 +877,14 @@ int wacomm_b200_set_times(wacomm_b200_context *ctx, int n_times, const double *o
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     if (n_times < 1 || !ocean_time) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "need >= 1 time");
     cudaSetDevice(ctx->device);
+    if (ctx->env[0].u || ctx->env[1].u) {
+        // regridded fields were aligned to the previous times
+        if (ctx->times.size() != (size_t)n_times ||
+            !std::equal(ctx->times.begin(), ctx->times.end(), ocean_time)) {
+            CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+            release_environment(ctx);
+        }
+    }
     ctx->times.assign(ocean_time, ocean_time + n_times);
     if ((int)ctx->slots.size() < n_times) ctx->slots.resize(n_times);
     ctx->pairT0 = ctx->pairT1 = -1;
@@ -1307,6 +1345,337 @@ int wacomm_b200_last_interval_stats(const wacomm_b200_context *ctx, float *devic
 int wacomm_b200_stream(const wacomm_b200_context *ctx, void **out) {
     if (!ctx || !out) return WACOMM_B200_ERR_ARGUMENT;
     *out = (void *)ctx->stream;
+    return WACOMM_B200_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Source longitudes and target longitudes farther than this from the grid's reference longitude
+// are refused (the reference steps them by 360 degrees in an unbounded loop).
+constexpr double LONGITUDE_REACH = 3600.0;
+
+double near_longitude_host(double value, double reference) {
+    while (value - reference > 180) value -= 360;
+    while (value - reference < -180) value += 360;
+    return value;
+}
+
+int cell_bin_host(double v, double minimum, double maximum, int bins) {
+    if (maximum == minimum) return 0;
+    return std::max(0, std::min(bins - 1, (int)((v - minimum) / (maximum - minimum) * bins)));
+}
+
+// Device buffers of one call, freed on every return path.
+struct Scratch {
+    std::vector<void *> held;
+    ~Scratch() {
+        for (void *p : held) cudaFree(p);
+    }
+    template <class T> cudaError_t get(T *&p, size_t count) {
+        p = nullptr;
+        cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) held.push_back(p);
+        return e;
+    }
+};
+
+// Rectilinear source checks of bilinearGeographic (EnvironmentalRegridder.cpp:243-258) and the
+// axis checks of bracket (:14-19); fills the unwrapped axes.
+const char *geographic_axes(int eta, int xi, const double *lon, const double *lat,
+                            std::vector<double> &ax, std::vector<double> &ay) {
+    ax.assign(xi, 0.0);
+    ay.assign(eta, 0.0);
+    for (int i = 0; i < xi; i++) ax[i] = lon[i];
+    for (int j = 0; j < eta; j++) ay[j] = lat[(size_t)j * xi];
+    for (int j = 0; j < eta; j++)
+        for (int i = 0; i < xi; i++) {
+            double x = lon[(size_t)j * xi + i], y = lat[(size_t)j * xi + i];
+            if (!std::isfinite(x) || !std::isfinite(y) || std::abs(x - ax[i]) > 1.e-10 ||
+                std::abs(y - ay[j]) > 1.e-10)
+                return "bilinear geographic regridding requires a finite rectilinear source grid";
+        }
+    for (int i = 1; i < xi; i++) {
+        if (!(std::abs(ax[i] - ax[i - 1]) <= LONGITUDE_REACH))
+            return "source longitudes lie more than 3600 degrees apart";
+        while (ax[i] - ax[i - 1] > 180) ax[i] -= 360;
+        while (ax[i] - ax[i - 1] < -180) ax[i] += 360;
+    }
+    if (std::abs(ax.back() - ax.front()) > 360 + 1.e-10)
+        return "the source longitude axis spans more than one revolution";
+    for (const std::vector<double> *axis : {&ax, &ay}) {
+        const std::vector<double> &a = *axis;
+        bool rising = a.back() > a.front();
+        for (size_t i = 1; i < a.size(); i++)
+            if ((rising && a[i] <= a[i - 1]) || (!rising && a[i] >= a[i - 1]))
+                return "a source axis is not strictly monotonic";
+    }
+    return nullptr;
+}
+
+struct CellIndexHost {
+    std::vector<double4> box;
+    std::vector<int> binStart, binCells;
+    double minX = 0, maxX = 0, minY = 0, maxY = 0, reference = 0;
+    int binsX = 1, binsY = 1;
+};
+
+// CurvilinearCellIndex (EnvironmentalRegridder.cpp:170-236) with cyclic longitudes: per-cell
+// boxes on the branch of lon(0,0), bins about as many as cells with the aspect of the grid's box,
+// and every cell listed, in index order, in each bin its box touches.
+const char *build_cell_index(int eta, int xi, const double *lon, const double *lat,
+                             CellIndexHost &ix) {
+    const double reference = lon[0];
+    if (!std::isfinite(reference)) return "curvilinear source coordinates must be finite";
+    for (size_t n = 0; n < (size_t)eta * xi; n++) {
+        if (!std::isfinite(lon[n]) || !std::isfinite(lat[n]))
+            return "curvilinear source coordinates must be finite";
+        if (!(std::abs(lon[n] - reference) <= LONGITUDE_REACH))
+            return "source longitudes lie more than 3600 degrees apart";
+    }
+    const size_t cells = (size_t)(eta - 1) * (xi - 1);
+    ix.box.resize(cells);
+    for (int j = 0; j + 1 < eta; j++)
+        for (int i = 0; i + 1 < xi; i++) {
+            auto L = [&](int jj, int ii) { return lon[(size_t)jj * xi + ii]; };
+            auto A = [&](int jj, int ii) { return lat[(size_t)jj * xi + ii]; };
+            double x00 = L(j, i), x10 = near_longitude_host(L(j, i + 1), x00);
+            double x01 = near_longitude_host(L(j + 1, i), x00);
+            double x11 = near_longitude_host(L(j + 1, i + 1), x00);
+            double y00 = A(j, i), y10 = A(j, i + 1), y01 = A(j + 1, i), y11 = A(j + 1, i + 1);
+            double center = .25 * (x00 + x10 + x01 + x11);
+            double shift = 360 * std::round((reference - center) / 360);
+            ix.box[(size_t)j * (xi - 1) + i] =
+                make_double4(std::min(std::min(x00, x10), std::min(x01, x11)) + shift,
+                             std::max(std::max(x00, x10), std::max(x01, x11)) + shift,
+                             std::min(std::min(y00, y10), std::min(y01, y11)),
+                             std::max(std::max(y00, y10), std::max(y01, y11)));
+        }
+    ix.minX = ix.box[0].x;
+    ix.maxX = ix.box[0].y;
+    ix.minY = ix.box[0].z;
+    ix.maxY = ix.box[0].w;
+    for (const double4 &b : ix.box) {
+        ix.minX = std::min(ix.minX, b.x);
+        ix.maxX = std::max(ix.maxX, b.y);
+        ix.minY = std::min(ix.minY, b.z);
+        ix.maxY = std::max(ix.maxY, b.w);
+    }
+    double width = std::max(ix.maxX - ix.minX, 1.e-12), height = std::max(ix.maxY - ix.minY, 1.e-12);
+    double scale = std::sqrt((double)cells);
+    ix.binsX = std::max(1, (int)std::round(scale * std::sqrt(width / height)));
+    ix.binsY = std::max(1, (int)std::round(scale * std::sqrt(height / width)));
+    ix.binsX = std::min(ix.binsX, (int)cells);
+    ix.binsY = std::min(ix.binsY, (int)cells);
+    const size_t bins = (size_t)ix.binsX * ix.binsY;
+    std::vector<size_t> start(bins + 1, 0);
+    auto span = [&](const double4 &b, int &i0, int &i1, int &j0, int &j1) {
+        i0 = cell_bin_host(b.x, ix.minX, ix.maxX, ix.binsX);
+        i1 = cell_bin_host(b.y, ix.minX, ix.maxX, ix.binsX);
+        j0 = cell_bin_host(b.z, ix.minY, ix.maxY, ix.binsY);
+        j1 = cell_bin_host(b.w, ix.minY, ix.maxY, ix.binsY);
+    };
+    int i0, i1, j0, j1;
+    for (const double4 &b : ix.box) {
+        span(b, i0, i1, j0, j1);
+        for (int jj = j0; jj <= j1; jj++)
+            for (int ii = i0; ii <= i1; ii++) start[(size_t)jj * ix.binsX + ii + 1]++;
+    }
+    for (size_t b = 0; b < bins; b++) start[b + 1] += start[b];
+    if (start[bins] >= ((size_t)1 << 31) || bins >= ((size_t)1 << 31) - 1)
+        return "the source grid's cell index exceeds 2^31 entries";
+    ix.binCells.assign(start[bins], 0);
+    std::vector<size_t> fill(start.begin(), start.end() - 1);
+    for (size_t c = 0; c < cells; c++) {
+        span(ix.box[c], i0, i1, j0, j1);
+        for (int jj = j0; jj <= j1; jj++)
+            for (int ii = i0; ii <= i1; ii++) ix.binCells[fill[(size_t)jj * ix.binsX + ii]++] = (int)c;
+    }
+    ix.binStart.assign(start.begin(), start.end());
+    ix.reference = reference;
+    return nullptr;
+}
+
+// Source records for each forcing time: an equal time (1e-6 s) copies the record, a time strictly
+// between two records blends them with timeWeight (NumericalHelpers.hpp:30-33).
+const char *align_times(int nSrc, const double *src, const std::vector<double> &dst,
+                        std::vector<RegridTime> &out) {
+    for (int k = 0; k < nSrc; k++)
+        if (!std::isfinite(src[k]) || (k && !(src[k] > src[k - 1])))
+            return "source times must be finite and strictly increasing";
+    out.clear();
+    for (double t : dst) {
+        int k0 = -1, k1 = -1;
+        for (int k = 0; k < nSrc && k0 < 0; k++)
+            if (std::abs(t - src[k]) <= 1.e-6) k0 = k1 = k;
+        for (int k = 0; k + 1 < nSrc && k0 < 0; k++)
+            if (t > src[k] && t < src[k + 1]) {
+                k0 = k;
+                k1 = k + 1;
+            }
+        if (k0 < 0) return "a forcing time lies outside the source times; extrapolation is prohibited";
+        double alpha = 0.0;
+        if (k1 != k0)
+            alpha = std::max(0.0, std::min(1.0, (t - src[k0]) / (src[k1] - src[k0])));
+        out.push_back(RegridTime{k0, k1, alpha});
+    }
+    return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wacomm_b200_regrid_environment(wacomm_b200_context *ctx, int field, int method, int src_eta,
+                                   int src_xi, const double *src_lon, const double *src_lat,
+                                   int src_times, const double *times, const float *u,
+                                   const float *v) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (field != WACOMM_B200_FIELD_WIND && field != WACOMM_B200_FIELD_STOKES)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "field %d: wind (0) or Stokes (1)", field);
+    if (method != WACOMM_B200_REGRID_BILINEAR_GEOGRAPHIC &&
+        method != WACOMM_B200_REGRID_BILINEAR_CURVILINEAR_GEOGRAPHIC)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "regridding method %d out of range", method);
+    if (!ctx->hasGrid || !ctx->hasGeo || ctx->times.empty())
+        return fail(ctx, WACOMM_B200_ERR_STATE,
+                    "regridding needs set_grid, set_geo_grid (the target nodes) and set_times");
+    if (src_eta < 2 || src_xi < 2 || src_times < 1)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT,
+                    "source grid %dx%d with %d records: need at least 2x2 and one record", src_eta,
+                    src_xi, src_times);
+    if (!src_lon || !src_lat || !times || !u || !v)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null source array");
+    const size_t srcPlane = (size_t)src_eta * src_xi;
+    if (srcPlane >= ((size_t)1 << 31) - 1)
+        return fail(ctx, WACOMM_B200_ERR_CAPACITY, "source grid of %zu nodes exceeds 2^31", srcPlane);
+    const bool curvilinear = method == WACOMM_B200_REGRID_BILINEAR_CURVILINEAR_GEOGRAPHIC;
+    std::vector<RegridTime> plan;
+    if (const char *why = align_times(src_times, times, ctx->times, plan))
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "%s", why);
+    std::vector<double> ax, ay;
+    CellIndexHost ix;
+    const char *why = curvilinear ? build_cell_index(src_eta, src_xi, src_lon, src_lat, ix)
+                                  : geographic_axes(src_eta, src_xi, src_lon, src_lat, ax, ay);
+    if (why) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "%s", why);
+
+    cudaSetDevice(ctx->device);
+    // intervals already enqueued may read the previous fields
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    const size_t plane = (size_t)ctx->eta * ctx->xi, T = ctx->times.size();
+    EnvField &out = ctx->env[field];
+    if (!out.u) {
+        CUDA_TRY(ctx, cudaMalloc(&out.u, T * plane * sizeof(float)));
+        CUDA_TRY(ctx, cudaMalloc(&out.v, T * plane * sizeof(float)));
+    }
+    Scratch scratch;
+    float *dSrc;
+    RegridPlan *dPlan;
+    RegridTime *dTimes;
+    int *dErr;
+    const size_t values = srcPlane * (size_t)src_times;
+    CUDA_TRY(ctx, scratch.get(dSrc, 2 * values));
+    CUDA_TRY(ctx, scratch.get(dPlan, plane));
+    CUDA_TRY(ctx, scratch.get(dTimes, T));
+    CUDA_TRY(ctx, scratch.get(dErr, 1));
+    CUDA_TRY(ctx, cudaMemcpyAsync(dSrc, u, values * sizeof(float), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(dSrc + values, v, values * sizeof(float), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(dTimes, plan.data(), T * sizeof(RegridTime),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(dErr, 0, sizeof(int), ctx->stream));
+    CUDA_TRY(ctx, regrid_check_finite(dSrc, (long long)(2 * values), dErr, ctx->stream));
+    if (curvilinear) {
+        double *dLon, *dLat;
+        double4 *dBox;
+        int *dStart, *dCells;
+        CUDA_TRY(ctx, scratch.get(dLon, srcPlane));
+        CUDA_TRY(ctx, scratch.get(dLat, srcPlane));
+        CUDA_TRY(ctx, scratch.get(dBox, ix.box.size()));
+        CUDA_TRY(ctx, scratch.get(dStart, ix.binStart.size()));
+        CUDA_TRY(ctx, scratch.get(dCells, ix.binCells.size()));
+        CUDA_TRY(ctx, cudaMemcpyAsync(dLon, src_lon, srcPlane * sizeof(double),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(dLat, src_lat, srcPlane * sizeof(double),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(dBox, ix.box.data(), ix.box.size() * sizeof(double4),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(dStart, ix.binStart.data(), ix.binStart.size() * sizeof(int),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        if (!ix.binCells.empty())
+            CUDA_TRY(ctx, cudaMemcpyAsync(dCells, ix.binCells.data(),
+                                          ix.binCells.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                          ctx->stream));
+        RegridCurvilinear C{dLon, dLat, dBox, dStart, dCells, ix.minX, ix.maxX, ix.minY, ix.maxY,
+                            ix.reference, ix.binsX, ix.binsY, src_xi, src_eta};
+        CUDA_TRY(ctx, regrid_plan_curvilinear(C, (long long)plane, ctx->dGeoLon, ctx->dGeoLat,
+                                              dPlan, dErr, ctx->stream));
+    } else {
+        double *dAx, *dAy;
+        CUDA_TRY(ctx, scratch.get(dAx, ax.size()));
+        CUDA_TRY(ctx, scratch.get(dAy, ay.size()));
+        CUDA_TRY(ctx, cudaMemcpyAsync(dAx, ax.data(), ax.size() * sizeof(double),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(dAy, ay.data(), ay.size() * sizeof(double),
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        RegridGeographic G{dAx, dAy, src_xi, src_eta, ax.back() > ax.front(),
+                           ay.back() > ay.front(), .5 * (ax.front() + ax.back())};
+        CUDA_TRY(ctx, regrid_plan_geographic(G, (long long)plane, ctx->dGeoLon, ctx->dGeoLat,
+                                             dPlan, dErr, ctx->stream));
+    }
+    CUDA_TRY(ctx, regrid_apply(curvilinear, dPlan, (long long)plane, src_xi, (long long)srcPlane,
+                               dSrc, dSrc + values, dTimes, (int)T, out.u, out.v, ctx->stream));
+    int err = 0;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&err, dErr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->pairT0 = ctx->pairT1 = -1;
+    ctx->zT0 = ctx->zT1 = -1;
+    if (err) {
+        cudaFree(out.u);
+        cudaFree(out.v);
+        out = EnvField{};
+        const char *what = (err & REGRID_ERR_FIELD)    ? "the source field holds a non-finite value"
+                           : (err & REGRID_ERR_TARGET) ? "a target coordinate is not finite or "
+                                                         "lies more than 3600 degrees away"
+                           : (err & REGRID_ERR_FOLDED) ? "the curvilinear source holds a folded or "
+                                                         "singular cell"
+                                                       : "a target node lies outside the source "
+                                                         "grid; extrapolation is prohibited";
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "%s", what);
+    }
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_clear_environment(wacomm_b200_context *ctx, int field) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (field != WACOMM_B200_FIELD_WIND && field != WACOMM_B200_FIELD_STOKES)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "field %d: wind (0) or Stokes (1)", field);
+    cudaSetDevice(ctx->device);
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->env[field].u);
+    cudaFree(ctx->env[field].v);
+    ctx->env[field] = EnvField{};
+    ctx->pairT0 = ctx->pairT1 = -1;
+    ctx->zT0 = ctx->zT1 = -1;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_get_environment(wacomm_b200_context *ctx, int field, int t, float *u, float *v) {
+    if (!ctx || !u || !v) return WACOMM_B200_ERR_ARGUMENT;
+    if (field != WACOMM_B200_FIELD_WIND && field != WACOMM_B200_FIELD_STOKES)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "field %d: wind (0) or Stokes (1)", field);
+    if (!ctx->env[field].u)
+        return fail(ctx, WACOMM_B200_ERR_STATE, "no regridded field %d", field);
+    if (t < 0 || t >= (int)ctx->times.size())
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "frame %d out of [0, %zu)", t, ctx->times.size());
+    cudaSetDevice(ctx->device);
+    const size_t plane = (size_t)ctx->eta * ctx->xi;
+    CUDA_TRY(ctx, cudaMemcpyAsync(u, ctx->env[field].u + t * plane, plane * sizeof(float),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(v, ctx->env[field].v + t * plane, plane * sizeof(float),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return WACOMM_B200_OK;
 }
 

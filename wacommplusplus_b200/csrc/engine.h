@@ -118,6 +118,56 @@ cudaError_t geo_positions(const ParticleSoA &S, int n, int eta, int xi, int sW, 
                           const double *lat, const double *h, const double *sWValues, double *dep,
                           double *latOut, double *lonOut, cudaStream_t stream);
 
+// regrid.cu --------------------------------------------------------------------------------
+
+// Error bits of the regridding kernels.
+constexpr int REGRID_ERR_OUTSIDE = 1, REGRID_ERR_FIELD = 2, REGRID_ERR_FOLDED = 4,
+              REGRID_ERR_TARGET = 8;
+
+// A target's source cell (row-major index of its lower-left source node; -1: none) and weights.
+struct RegridPlan {
+    int node;
+    double wx, wy;
+};
+
+// Rectilinear source: the longitude axis already unwrapped, `center` the midpoint of its ends.
+struct RegridGeographic {
+    const double *axisX, *axisY;
+    int xi, eta;
+    bool risingX, risingY;
+    double center;
+};
+
+// Curvilinear source: coordinates [eta][xi], the per-cell boxes (minimumX, maximumX, minimumY,
+// maximumY, shifted to the branch of `reference`) and the bins as offsets + cell lists.
+struct RegridCurvilinear {
+    const double *lon, *lat;
+    const double4 *box;
+    const int *binStart, *binCells;
+    double minX, maxX, minY, maxY, reference;
+    int binsX, binsY, xi, eta;
+};
+
+// A forcing time: source records k0 and k1 blended with weight alpha (k0 == k1: a copy).
+struct RegridTime {
+    int k0, k1;
+    double alpha;
+};
+
+cudaError_t regrid_check_finite(const float *values, long long count, int *err,
+                                cudaStream_t stream);
+cudaError_t regrid_plan_geographic(const RegridGeographic &G, long long nTarget,
+                                   const double *tLon, const double *tLat, RegridPlan *plan,
+                                   int *err, cudaStream_t stream);
+cudaError_t regrid_plan_curvilinear(const RegridCurvilinear &C, long long nTarget,
+                                    const double *tLon, const double *tLat, RegridPlan *plan,
+                                    int *err, cudaStream_t stream);
+// outU/outV: nTimes planes of nTarget values each.
+cudaError_t regrid_apply(bool curvilinear, const RegridPlan *plan, long long nTarget, int srcXi,
+                         long long srcPlane, const float *srcU, const float *srcV,
+                         const RegridTime *times, int nTimes, float *outU, float *outV,
+                         cudaStream_t stream);
+
 // surrogate.cu -----------------------------------------------------------------------------
 
 // One surrogate interval: grid, interval, run parameters, the dry-node table, the per-cell layer-1

@@ -224,6 +224,39 @@ class Engine:
                                                         lon.ctypes.data_as(_dp), n))
         return dep, lat, lon
 
+    REGRID_METHODS = {"geographic": _native.REGRID_BILINEAR_GEOGRAPHIC,
+                      "curvilinear": _native.REGRID_BILINEAR_CURVILINEAR_GEOGRAPHIC}
+    FIELDS = {"wind": _native.FIELD_WIND, "stokes": _native.FIELD_STOKES}
+
+    def regrid_environment(self, field, method, lon, lat, times, u, v):
+        """Regrids a wind or Stokes field ("wind"/"stokes") from its own grid lon/lat
+        [eta', xi'] (degrees) and times [T'] to the rho nodes of set_geo_grid and the forcing
+        times, on the device; u, v [T', eta', xi'] float32. method "geographic" (rectilinear
+        source) or "curvilinear"."""
+        lon, lat = np.ascontiguousarray(lon, np.float64), np.ascontiguousarray(lat, np.float64)
+        times = np.ascontiguousarray(times, np.float64)
+        u, v = np.ascontiguousarray(u, np.float32), np.ascontiguousarray(v, np.float32)
+        if lon.ndim != 2 or lat.shape != lon.shape or u.shape != (times.size,) + lon.shape or \
+                v.shape != u.shape:
+            raise ValueError(f"shapes lon {lon.shape} lat {lat.shape} times {times.shape} "
+                             f"u {u.shape} v {v.shape}")
+        self._check(self._lib.wacomm_b200_regrid_environment(
+            self._ctx, self.FIELDS[field], self.REGRID_METHODS[method], lon.shape[0], lon.shape[1],
+            lon.ctypes.data_as(_dp), lat.ctypes.data_as(_dp), times.size, times.ctypes.data_as(_dp),
+            u.ctypes.data_as(_fp), v.ctypes.data_as(_fp)))
+
+    def clear_environment(self, field):
+        self._check(self._lib.wacomm_b200_clear_environment(self._ctx, self.FIELDS[field]))
+
+    def environment(self, field, t):
+        """(u, v) float32 [eta, xi] of the regridded field at forcing time t."""
+        eta, xi = self._grid_shape[1:]
+        u, v = (np.empty((eta, xi), np.float32) for _ in range(2))
+        self._check(self._lib.wacomm_b200_get_environment(self._ctx, self.FIELDS[field], t,
+                                                          u.ctypes.data_as(_fp),
+                                                          v.ctypes.data_as(_fp)))
+        return u, v
+
     def synchronize(self):
         self._check(self._lib.wacomm_b200_synchronize(self._ctx))
         self._in_flight = {}

@@ -258,3 +258,60 @@ class RealisticForcing:
         out["i"] = src[s_idx, 2] + spread * rng.standard_normal(len(order))
         out["health"] = 1.0
         return out
+
+
+# ------------------------------------------------------------------ wind and Stokes on own grids
+
+
+def wind_grid(n=340, spacing_m=3000.0, lon0=14.1, lat0=40.8, rotation_deg=8.0):
+    """A weather-model grid of n x n nodes ``spacing_m`` apart (340 x 340 at 3 km: ~1,000 km
+    across), rotated by ``rotation_deg`` and centred on (lon0, lat0): node positions on a local
+    tangent plane mapped to degrees with the latitude-dependent longitude scale, so that lon and
+    lat both vary along both index directions (curvilinear, like a Lambert-conformal WRF grid).
+    Returns lon, lat [n, n] in degrees."""
+    R = 6371000.0
+    c = (n - 1) / 2.0
+    j, i = np.mgrid[0:n, 0:n].astype(np.float64)
+    x, y = (i - c) * spacing_m, (j - c) * spacing_m
+    r = math.radians(rotation_deg)
+    xr, yr = x * math.cos(r) - y * math.sin(r), x * math.sin(r) + y * math.cos(r)
+    lat = lat0 + np.degrees(yr / R)
+    lon = lon0 + np.degrees(xr / (R * np.cos(np.radians(lat))))
+    return lon, lat
+
+
+def stokes_grid(lon0=13.5, lon1=14.7, lat0=40.2, lat1=41.4, step=0.05):
+    """A rectilinear wave-model grid at ``step`` degrees (0.05 by default) around the analytic
+    ocean domain. Returns lon, lat [eta, xi] in degrees."""
+    lon1d = lon0 + step * np.arange(int(round((lon1 - lon0) / step)) + 1)
+    lat1d = lat0 + step * np.arange(int(round((lat1 - lat0) / step)) + 1)
+    return np.meshgrid(lon1d, lat1d)
+
+
+def vector_series(shape, n_times, rms, seed, length_cells, period_records=24.0):
+    """(u, v) float32 [n_times, *shape]: smooth random vector fields of rms ``rms`` per component
+    turning slowly in time (two random fields per component mixed with phases advancing
+    2*pi/period_records per record)."""
+    rng = np.random.default_rng(seed)
+    eta, xi = shape
+    a, b, c, d = (_smooth_field(rng, eta, xi, length_cells) for _ in range(4))
+    out_u = np.empty((n_times,) + shape, np.float32)
+    out_v = np.empty((n_times,) + shape, np.float32)
+    for t in range(n_times):
+        ph = 2 * np.pi * t / period_records
+        out_u[t] = rms * (math.cos(ph) * a + math.sin(ph) * b)
+        out_v[t] = rms * (math.cos(ph) * c + math.sin(ph) * d)
+    return out_u, out_v
+
+
+def environment(t0, hours, wind_n=340, seed=11):
+    """The batched workload's native environmental forcing over ``hours`` hours from t0: wind on
+    the curvilinear 3 km grid, hourly, rms 8 m/s; Stokes drift on the 0.05-degree grid,
+    3-hourly, rms 0.1 m/s. dict of (lon, lat, times, u, v) per field."""
+    wlon, wlat = wind_grid(wind_n)
+    wt = t0 + 3600.0 * np.arange(hours + 1)
+    wu, wv = vector_series(wlon.shape, len(wt), 8.0, seed, wind_n / 12.0)
+    slon, slat = stokes_grid()
+    st = t0 + 10800.0 * np.arange(hours // 3 + 1 + (hours % 3 > 0))
+    su, sv = vector_series(slon.shape, len(st), 0.1, seed + 1, 3.0, period_records=8.0)
+    return {"wind": (wlon, wlat, wt, wu, wv), "stokes": (slon, slat, st, su, sv)}
