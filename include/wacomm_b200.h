@@ -201,6 +201,27 @@ int wacomm_b200_particle_count(const wacomm_b200_context *ctx, size_t *out);
  * concentration grid at time index time_index + direction (Wacomm.cpp:713-722). */
 int wacomm_b200_move_interval(wacomm_b200_context *ctx, int time_index);
 
+/* A run of n_intervals intervals from first_time_index on, in the tracking direction, recorded
+ * once as a CUDA graph (pair packing, cell sort, move and fused count of every interval) and
+ * launched as one unit by wacomm_b200_graph_launch; the solver's per-interval loop
+ * (Wacomm.cpp:386-739) becomes one host call. Every buffer is sized before the capture. The graph
+ * holds the particle count, the buffer addresses, the forcing times, the config and the options
+ * of the capture: new record values (upload_frame into existing slots, set_particles with the
+ * same count, a new batch of scenarios) are picked up by the next launch, while any change of
+ * those is refused at launch with WACOMM_B200_ERR_STATE (capture again). Not with the surrogate
+ * option (its fallback list returns to the host). last_interval_stats after a launch reports
+ * the whole run (device ms, particle-steps). No reference counterpart. */
+int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, int n_intervals);
+int wacomm_b200_graph_launch(wacomm_b200_context *ctx);
+int wacomm_b200_graph_release(wacomm_b200_context *ctx);
+
+/* Times the interval at time_index once per launch configuration of the move kernel (FP32
+ * arithmetic: launch_shape 0..3; reference arithmetic: block_size 64, 128, 192, 256), each from
+ * the same resident records and concentration after a warm-up pass, keeps the fastest in the
+ * options and restores records and concentration: only the options change. Writes the chosen
+ * value and its device ms. No reference counterpart. */
+int wacomm_b200_autotune(wacomm_b200_context *ctx, int time_index, int *best, float *best_ms);
+
 /* The same interval through host buffers: uploads n records from `particles` (pinned or
  * pageable host memory), moves them, and writes them back in place. Copies are pipelined
  * against the kernels in slabs; the resident set is replaced by these records. */

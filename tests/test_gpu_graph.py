@@ -1,0 +1,125 @@
+"""Captured runs (wacomm_b200_graph_capture / graph_launch) and the launch autotuner.
+
+A run of intervals recorded as one CUDA graph must give the records, the concentration grid and
+the particle-step count of the same intervals run one call at a time, bit for bit, and a relaunch
+on a new batch of the same size must equal an eager run of that batch. A launch after a change the
+graph cannot see (particle count, config) is refused. The autotuner leaves records and
+concentration as they were and only changes the launch configuration.
+"""
+import numpy as np
+import pytest
+
+from wacommplusplus_b200 import synthetic as syn
+from wacommplusplus_b200._native import WacommError
+from wacommplusplus_b200.engine import Engine
+from wacommplusplus_b200.types import default_config
+
+pytestmark = pytest.mark.gpu
+
+INTERVALS = 4
+
+
+@pytest.fixture(scope="module")
+def setting():
+    win = syn.config1_window(n_frames=INTERVALS + 2)
+    env = syn.environment(win.times[0], INTERVALS + 1, wind_n=80)
+    cfg = default_config(random=True, randomSeed=17, driftModel=1)
+    return win, env, cfg
+
+
+def batch(n, seed, win):
+    p = syn.uniform_particles(n, win.eta, win.xi, seed=seed)
+    rng = np.random.default_rng(seed)
+    p["driftObjectType"] = rng.integers(0, 23, n)
+    p["driftSide"] = rng.choice([-1, 1], n)
+    p["time"] = win.times[0] + rng.uniform(0, 2 * 3600.0, n)  # staggered releases
+    return p
+
+
+def engine(win, env, cfg, particles):
+    e = Engine(0, arithmetic="fp32", storage="fp32")
+    e.set_config(cfg)
+    e.load_window(win)
+    e.set_geo_grid(win.lon, win.lat, win.sWValues)
+    e.regrid_environment("wind", "curvilinear", *env["wind"])
+    e.regrid_environment("stokes", "geographic", *env["stokes"])
+    e.concentration_reset(win.T)
+    e.set_particles(particles)
+    return e
+
+
+def eager(e):
+    steps = 0.0
+    for t in range(INTERVALS):
+        e.move_interval(t)
+        steps += e.stats()["particle_steps"]
+    return steps
+
+
+def same(a, b):
+    pa, pb = a.get_particles(), b.get_particles()
+    for f in pa.dtype.names:
+        assert pa[f].tobytes() == pb[f].tobytes(), f
+    assert np.array_equal(a.concentration(), b.concentration())
+
+
+def test_graph_equals_eager_and_relaunches_on_a_new_batch(cuda_device, setting):
+    win, env, cfg = setting
+    first, second = batch(30000, 1, win), batch(30000, 2, win)
+    ref = engine(win, env, cfg, first)
+    ref_steps = eager(ref)
+    g = engine(win, env, cfg, first)
+    g.graph_capture(0, INTERVALS)
+    g.graph_launch()
+    g.synchronize()
+    assert g.stats()["particle_steps"] == ref_steps > 0
+    same(g, ref)
+    # a new batch of the same size through the same graph
+    ref.set_particles(second)
+    ref.concentration_reset(win.T)
+    eager(ref)
+    g.set_particles(second)
+    g.concentration_reset(win.T)
+    g.graph_launch()
+    g.synchronize()
+    same(g, ref)
+    ref.close()
+    g.close()
+
+
+def test_graph_launch_refused_after_changes(cuda_device, setting):
+    win, env, cfg = setting
+    g = engine(win, env, cfg, batch(5000, 3, win))
+    g.graph_capture(0, INTERVALS)
+    g.set_particles(batch(4000, 4, win))
+    with pytest.raises(WacommError):
+        g.graph_launch()
+    g.set_particles(batch(5000, 4, win))
+    g.graph_launch()
+    g.synchronize()
+    g.set_config(default_config(random=True, randomSeed=18, driftModel=1))
+    with pytest.raises(WacommError):
+        g.graph_launch()
+    g.graph_release()
+    with pytest.raises(WacommError):
+        g.graph_launch()
+    g.set_options(surrogate=1)
+    g.set_surrogate()
+    with pytest.raises(WacommError):
+        g.graph_capture(0, 2)
+    g.close()
+
+
+def test_autotune_changes_only_the_launch_shape(cuda_device, setting):
+    win, env, cfg = setting
+    e = engine(win, env, cfg, batch(40000, 5, win))
+    e.move_interval(0)
+    before, conc = e.get_particles(), e.concentration()
+    shape, ms = e.autotune(1)
+    assert shape in (0, 1, 2, 3) and ms > 0
+    assert e.options().launch_shape == shape
+    after = e.get_particles()
+    for f in before.dtype.names:
+        assert before[f].tobytes() == after[f].tobytes(), f
+    assert np.array_equal(conc, e.concentration())
+    e.close()

@@ -68,6 +68,10 @@ SIGNATURES = {
     "wacomm_b200_geo_positions": (_i, [_vp, _dp, _dp, _dp, _sz]),
     "wacomm_b200_regrid_environment": (_i, [_vp, _i, _i, _i, _i, _dp, _dp, _i, _dp, _fp, _fp]),
     "wacomm_b200_clear_environment": (_i, [_vp, _i]),
+    "wacomm_b200_graph_capture": (_i, [_vp, _i, _i]),
+    "wacomm_b200_graph_launch": (_i, [_vp]),
+    "wacomm_b200_graph_release": (_i, [_vp]),
+    "wacomm_b200_autotune": (_i, [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_float)]),
     "wacomm_b200_get_environment": (_i, [_vp, _i, _i, _fp, _fp]),
     "wacomm_b200_concentration_reset": (_i, [_vp, _i]),
     "wacomm_b200_concentration_count": (_i, [_vp, _i]),

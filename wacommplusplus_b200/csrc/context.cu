@@ -117,6 +117,12 @@ struct wacomm_b200_context {
     double *dGeoLon = nullptr, *dGeoLat = nullptr, *dSWValues = nullptr;  // kji2deplatlon grid
     bool hasGeo = false;
     double *dGeoOut = nullptr;  // [3][n] depth, lat, lon
+    // A captured run of intervals (wacomm_b200_graph_capture) and the buffer layout it was
+    // captured against.
+    cudaGraphExec_t graphExec = nullptr;
+    std::vector<uint64_t> graphLayout;
+    int graphLaunches = 0;
+    bool capturing = false;
     // Wind (0) and Stokes (1) fields regridded to the rho nodes and the forcing times, [T][eta][xi]
     // each; a frame's own uploaded fields take precedence over these.
     EnvField env[2];
@@ -337,13 +343,8 @@ void release_environment(wacomm_b200_context *ctx) {
     }
 }
 
-int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
-    const FrameDevice a = frame_of(ctx, t0), b = frame_of(ctx, t1);
-    bool env = a.windU || a.windV || a.stokesU || b.windU || b.windV || b.stokesU;
-    bool cells = ctx->opt.arithmetic == WACOMM_B200_ARITH_FP32;
-    if (ctx->pairT0 == t0 && ctx->pairT1 == t1 && ctx->pairStorage == ctx->opt.storage &&
-        ctx->pairEnv == env && (!cells || ctx->pairCells))
-        return WACOMM_B200_OK;
+// Device buffers of the packed forcing pair (node records, environment pair, cell-column records).
+int reserve_pair_buffers(wacomm_b200_context *ctx, bool env, bool cells) {
     size_t plane = (size_t)ctx->eta * ctx->xi;
     size_t need = plane * ctx->sW * node_record_bytes(ctx->opt.storage);
     if (need > ctx->nodesBytes) {
@@ -354,10 +355,6 @@ int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
         ctx->nodesBytes = need;
     }
     if (env && !ctx->dEnv) CUDA_TRY(ctx, cudaMalloc(&ctx->dEnv, plane * sizeof(EnvPair)));
-    CUDA_TRY(ctx, pack_pair(ctx->opt.storage, ctx->eta, ctx->xi, ctx->sW, a, b,
-                            ctx->dH, ctx->dNodes, ctx->dSurf, env ? ctx->dEnv : nullptr,
-                            ctx->stream));
-    launches += 2;
     if (cells) {
         size_t cneed = plane * ctx->sW * cell_record_bytes(ctx->opt.storage);
         if (cneed > ctx->cellsBytes) {
@@ -375,6 +372,24 @@ int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
             CUDA_TRY(ctx, cudaMalloc(&ctx->dCellSurface, sneed));
             ctx->cellSurfaceBytes = sneed;
         }
+    }
+    return WACOMM_B200_OK;
+}
+
+int ensure_pair(wacomm_b200_context *ctx, int t0, int t1, int &launches) {
+    const FrameDevice a = frame_of(ctx, t0), b = frame_of(ctx, t1);
+    bool env = a.windU || a.windV || a.stokesU || b.windU || b.windV || b.stokesU;
+    bool cells = ctx->opt.arithmetic == WACOMM_B200_ARITH_FP32;
+    if (ctx->pairT0 == t0 && ctx->pairT1 == t1 && ctx->pairStorage == ctx->opt.storage &&
+        ctx->pairEnv == env && (!cells || ctx->pairCells))
+        return WACOMM_B200_OK;
+    int rc = reserve_pair_buffers(ctx, env, cells);
+    if (rc) return rc;
+    CUDA_TRY(ctx, pack_pair(ctx->opt.storage, ctx->eta, ctx->xi, ctx->sW, a, b,
+                            ctx->dH, ctx->dNodes, ctx->dSurf, env ? ctx->dEnv : nullptr,
+                            ctx->stream));
+    launches += 2;
+    if (cells) {
         CUDA_TRY(ctx, pack_cells(ctx->opt.storage, ctx->eta, ctx->xi, ctx->sW, a, b, ctx->dH,
                                  ctx->dCells, ctx->dCellSurface, ctx->stream));
         launches += 2;
@@ -412,8 +427,8 @@ PackedArgs packed_args(wacomm_b200_context *ctx) {
     return A;
 }
 
-int sort_work(wacomm_b200_context *ctx, const ParticleSoA &S, size_t count, uint32_t *keys,
-              uint32_t *order, int &launches) {
+// Histogram, offsets and scan scratch of the cell sort of `count` records.
+int reserve_sort(wacomm_b200_context *ctx, size_t count) {
     size_t bins = (size_t)ctx->eta * ctx->xi + 1;
     if (ctx->binsCap < bins + 2 || !ctx->dHist || !ctx->dOffsets) {
         cudaFree(ctx->dHist);
@@ -424,8 +439,14 @@ int sort_work(wacomm_b200_context *ctx, const ParticleSoA &S, size_t count, uint
         CUDA_TRY(ctx, cudaMalloc(&ctx->dOffsets, (bins + 2) * sizeof(uint32_t)));
         ctx->binsCap = bins + 2;
     }
+    return reserve_scan(ctx, std::max(bins, count));
+}
+
+int sort_work(wacomm_b200_context *ctx, const ParticleSoA &S, size_t count, uint32_t *keys,
+              uint32_t *order, int &launches) {
+    size_t bins = (size_t)ctx->eta * ctx->xi + 1;
     int rc;
-    if ((rc = reserve_scan(ctx, std::max(bins, count)))) return rc;
+    if ((rc = reserve_sort(ctx, count))) return rc;
     CUDA_TRY(ctx, sort_by_cell(S.j, S.i, (int)count, ctx->eta, ctx->xi, keys, ctx->dHist,
                                ctx->dOffsets, ctx->dScanTemp, order, ctx->stream));
     size_t blocks = (bins + 8191) / 8192;
@@ -462,7 +483,7 @@ int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t of
             if (rc) return rc;
             L.order = order;
         }
-        if (!ctx->moveTimed) {
+        if (!ctx->moveTimed && !ctx->capturing) {
             CUDA_TRY(ctx, cudaEventRecord(ctx->evMove0, ctx->stream));
             ctx->moveTimed = true;
         }
@@ -479,7 +500,7 @@ int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t of
         if (e != cudaSuccess)
             return fail(ctx, WACOMM_B200_ERR_CUDA, "move launch: %s", cudaGetErrorString(e));
         launches++;
-        CUDA_TRY(ctx, cudaEventRecord(ctx->evMove1, ctx->stream));
+        if (!ctx->capturing) CUDA_TRY(ctx, cudaEventRecord(ctx->evMove1, ctx->stream));
     }
     return WACOMM_B200_OK;
 }
@@ -506,6 +527,20 @@ int prepare_interval(wacomm_b200_context *ctx, int time_index, IntervalParams &P
     if ((rc = ensure_metric(ctx))) return rc;
     if ((rc = ensure_pair(ctx, P.t0, P.t1, launches))) return rc;
     return WACOMM_B200_OK;
+}
+
+int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launches);
+
+// The work of one interval on the compute stream (pair packing, sort, move, fused count).
+int enqueue_interval(wacomm_b200_context *ctx, int time_index, int &launches) {
+    IntervalParams P;
+    int rc = prepare_interval(ctx, time_index, P, launches);
+    if (rc) return rc;
+    ctx->surrTimed = false;
+    if (P.skip || !ctx->n) return WACOMM_B200_OK;
+    if (ctx->opt.surrogate) return run_surrogate(ctx, P, launches);
+    if ((rc = reserve_work(ctx, ctx->n))) return rc;
+    return run_interval(ctx, P, 0, ctx->n, ctx->dKeys, ctx->dOrder, launches);
 }
 
 // Surrogate interval: per-cell layer 1 for the forcing pair, cell sort, the tensor-core step, then
@@ -747,6 +782,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dSWValues);
     cudaFree(ctx->dGeoOut);
     release_environment(ctx);
+    if (ctx->graphExec) cudaGraphExecDestroy(ctx->graphExec);
     cudaFree(ctx->dSteps);
     cudaFree(ctx->dErr);
     cudaFree(ctx->dCfg);
@@ -1029,22 +1065,12 @@ int wacomm_b200_particle_count(const wacomm_b200_context *ctx, size_t *out) {
 int wacomm_b200_move_interval(wacomm_b200_context *ctx, int time_index) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     cudaSetDevice(ctx->device);
-    IntervalParams P;
     int launches = 0;
     ctx->moveTimed = false;
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->dSteps, 0, sizeof(unsigned long long), ctx->stream));
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    int rc = prepare_interval(ctx, time_index, P, launches);
+    int rc = enqueue_interval(ctx, time_index, launches);
     if (rc) return rc;
-    ctx->surrTimed = false;
-    if (!P.skip && ctx->n) {
-        if (ctx->opt.surrogate) {
-            if ((rc = run_surrogate(ctx, P, launches))) return rc;
-        } else {
-            if ((rc = reserve_work(ctx, ctx->n))) return rc;
-            if ((rc = run_interval(ctx, P, 0, ctx->n, ctx->dKeys, ctx->dOrder, launches))) return rc;
-        }
-    }
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     ctx->lastLaunches = launches;
     return WACOMM_B200_OK;
@@ -1676,6 +1702,243 @@ int wacomm_b200_get_environment(wacomm_b200_context *ctx, int field, int t, floa
     CUDA_TRY(ctx, cudaMemcpyAsync(v, ctx->env[field].v + t * plane, plane * sizeof(float),
                                   cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return WACOMM_B200_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Everything a captured run reads by address or by value: buffer addresses and sizes, the particle
+// count, the forcing times, the run configuration and options. A graph is launched only while this
+// is unchanged.
+std::vector<uint64_t> layout_of(const wacomm_b200_context *ctx) {
+    std::vector<uint64_t> f;
+    auto add = [&](const void *p) { f.push_back((uint64_t)(uintptr_t)p); };
+    auto bytes = [&](const void *p, size_t n) {
+        const unsigned char *b = (const unsigned char *)p;
+        for (size_t o = 0; o < n; o += 8) {
+            uint64_t w = 0;
+            std::memcpy(&w, b + o, std::min<size_t>(8, n - o));
+            f.push_back(w);
+        }
+    };
+    const ParticleSoA &S = ctx->S.s;
+    f.push_back(ctx->n);
+    for (const void *p : {(const void *)S.id, (const void *)S.k, (const void *)S.j,
+                          (const void *)S.i, (const void *)S.health, (const void *)S.age,
+                          (const void *)S.time, (const void *)S.type, (const void *)S.side,
+                          (const void *)S.elapsed})
+        add(p);
+    for (const void *p : {(const void *)ctx->dKeys, (const void *)ctx->dOrder,
+                          (const void *)ctx->dHist, (const void *)ctx->dOffsets,
+                          (const void *)ctx->dScanTemp, (const void *)ctx->dNodes,
+                          (const void *)ctx->dCells, (const void *)ctx->dCellSurface,
+                          (const void *)ctx->dSurf, (const void *)ctx->dEnv,
+                          (const void *)ctx->dConc, (const void *)ctx->dMetric,
+                          (const void *)ctx->dInvMetric, (const void *)ctx->dLon,
+                          (const void *)ctx->dLat, (const void *)ctx->dH, (const void *)ctx->dDepth,
+                          (const void *)ctx->dDepthF, (const void *)ctx->dMask,
+                          (const void *)ctx->dCfg, (const void *)ctx->dSteps,
+                          (const void *)ctx->dErr})
+        add(p);
+    f.push_back((uint64_t)ctx->concTimes);
+    for (const FrameSlot &s : ctx->slots)
+        for (const void *p : {(const void *)s.zeta, (const void *)s.u, (const void *)s.v,
+                              (const void *)s.w, (const void *)s.akt, (const void *)s.windU,
+                              (const void *)s.windV, (const void *)s.stokesU,
+                              (const void *)s.stokesV})
+            add(p);
+    for (const EnvField &e : ctx->env) {
+        add(e.u);
+        add(e.v);
+    }
+    bytes(ctx->times.data(), ctx->times.size() * sizeof(double));
+    bytes(&ctx->cfg, sizeof ctx->cfg);
+    bytes(&ctx->opt, sizeof ctx->opt);
+    return f;
+}
+
+void release_graph(wacomm_b200_context *ctx) {
+    if (ctx->graphExec) cudaGraphExecDestroy(ctx->graphExec);
+    ctx->graphExec = nullptr;
+    ctx->graphLayout.clear();
+    ctx->graphLaunches = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, int n_intervals) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    const int T = (int)ctx->times.size(), dir = ctx->cfg.trackingDirection;
+    const int last = first_time_index + dir * (n_intervals - 1);
+    if (n_intervals < 1 || first_time_index < 0 || first_time_index >= T || last < 0 || last >= T)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "intervals %d..%d out of [0, %d)",
+                    first_time_index, last, T);
+    if (ctx->opt.surrogate)
+        return fail(ctx, WACOMM_B200_ERR_STATE,
+                    "the surrogate hands its fallback list back to the host: not capturable");
+    cudaSetDevice(ctx->device);
+    release_graph(ctx);
+    // Uploads in flight finish first (their ready events lie outside the capture), and every
+    // buffer the intervals use is sized now: nothing may be allocated while capturing.
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (FrameSlot &s : ctx->slots) s.pending = false;
+    const bool cells = ctx->opt.arithmetic == WACOMM_B200_ARITH_FP32;
+    for (int n = 0, t = first_time_index; n < n_intervals; n++, t += dir) {
+        IntervalParams P;
+        make_interval(ctx->cfg, ctx->times.data(), T, t, ctx->sW, ctx->opt.semantics, P);
+        if (P.skip) continue;
+        if (!ctx->slots[P.t0].loaded || !ctx->slots[P.t1].loaded)
+            return fail(ctx, WACOMM_B200_ERR_STATE, "forcing records %d and %d must be uploaded",
+                        P.t0, P.t1);
+        const FrameDevice a = frame_of(ctx, P.t0), b = frame_of(ctx, P.t1);
+        bool env = a.windU || a.windV || a.stokesU || b.windU || b.windV || b.stokesU;
+        if ((rc = reserve_pair_buffers(ctx, env, cells))) return rc;
+    }
+    if ((rc = ensure_metric(ctx))) return rc;
+    if (ctx->n) {
+        if ((rc = reserve_work(ctx, ctx->n))) return rc;
+        if (ctx->opt.sort_by_cell && (rc = reserve_sort(ctx, ctx->n))) return rc;
+    }
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->pairT0 = ctx->pairT1 = -1;  // the graph packs its own pairs
+    CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    ctx->capturing = true;
+    int launches = 0;
+    cudaError_t e = cudaMemsetAsync(ctx->dSteps, 0, sizeof(unsigned long long), ctx->stream);
+    rc = e == cudaSuccess ? WACOMM_B200_OK
+                          : fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e));
+    for (int n = 0, t = first_time_index; n < n_intervals && !rc; n++, t += dir)
+        rc = enqueue_interval(ctx, t, launches);
+    ctx->capturing = false;
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(ctx->stream, &graph);
+    ctx->pairT0 = ctx->pairT1 = -1;  // nothing captured has run yet
+    if (!rc && e != cudaSuccess)
+        rc = fail(ctx, WACOMM_B200_ERR_CUDA, "capture: %s", cudaGetErrorString(e));
+    if (!rc) {
+        e = cudaGraphInstantiate(&ctx->graphExec, graph, 0);
+        if (e != cudaSuccess) {
+            ctx->graphExec = nullptr;
+            rc = fail(ctx, WACOMM_B200_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+        }
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (rc) return rc;
+    ctx->graphLayout = layout_of(ctx);
+    ctx->graphLaunches = launches;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_graph_launch(wacomm_b200_context *ctx) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!ctx->graphExec) return fail(ctx, WACOMM_B200_ERR_STATE, "no captured graph");
+    if (layout_of(ctx) != ctx->graphLayout)
+        return fail(ctx, WACOMM_B200_ERR_STATE,
+                    "particles, buffers, times, config or options changed since the capture");
+    cudaSetDevice(ctx->device);
+    for (FrameSlot &s : ctx->slots)
+        if (s.pending) {
+            CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, s.ready, 0));
+            s.pending = false;
+        }
+    ctx->moveTimed = false;
+    CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    CUDA_TRY(ctx, cudaGraphLaunch(ctx->graphExec, ctx->stream));
+    CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->pairT0 = ctx->pairT1 = -1;
+    ctx->lastLaunches = ctx->graphLaunches;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_graph_release(wacomm_b200_context *ctx) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    release_graph(ctx);
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_autotune(wacomm_b200_context *ctx, int time_index, int *best, float *best_ms) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (ctx->opt.surrogate)
+        return fail(ctx, WACOMM_B200_ERR_STATE, "autotune times the plain step: surrogate is on");
+    if (!ctx->n) return fail(ctx, WACOMM_B200_ERR_STATE, "no resident particles to time");
+    int rc = check_ready(ctx);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    const bool fp32 = ctx->opt.arithmetic == WACOMM_B200_ARITH_FP32;
+    const std::vector<int> candidates = fp32 ? std::vector<int>{0, 1, 2, 3}
+                                             : std::vector<int>{64, 128, 192, 256};
+    // snapshot: records (AoS), concentration, then one timed interval per candidate from it
+    const size_t n = ctx->n;
+    if ((rc = grow(ctx, ctx->dAos, ctx->aosCap, n))) return rc;
+    CUDA_TRY(ctx, soa_to_aos(ctx->S.s, (int)n, ctx->dAos, ctx->stream));
+    const size_t concBytes = ctx->dConc ? (size_t)ctx->concTimes * ctx->sRho * ctx->eta * ctx->xi *
+                                              sizeof(uint32_t)
+                                        : 0;
+    uint32_t *concCopy = nullptr;
+    if (concBytes) {
+        CUDA_TRY(ctx, cudaMalloc(&concCopy, concBytes));
+        cudaError_t e = cudaMemcpyAsync(concCopy, ctx->dConc, concBytes, cudaMemcpyDeviceToDevice,
+                                        ctx->stream);
+        if (e != cudaSuccess) {
+            cudaFree(concCopy);
+            return fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e));
+        }
+    }
+    const wacomm_b200_options saved = ctx->opt;
+    auto restore = [&]() -> cudaError_t {
+        cudaError_t e = aos_to_soa(ctx->dAos, (int)n, ctx->S.s, ctx->stream);
+        if (e == cudaSuccess && concBytes)
+            e = cudaMemcpyAsync(ctx->dConc, concCopy, concBytes, cudaMemcpyDeviceToDevice,
+                                ctx->stream);
+        return e;
+    };
+    int chosen = fp32 ? saved.launch_shape : saved.block_size;
+    float chosenMs = INFINITY;
+    for (int pass = 0; pass < 2 && !rc; pass++)  // the first pass warms every variant up
+        for (int c : candidates) {
+            if (fp32) ctx->opt.launch_shape = c;
+            else ctx->opt.block_size = c;
+            cudaError_t e = restore();
+            if (e != cudaSuccess) {
+                rc = fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e));
+                break;
+            }
+            if ((rc = wacomm_b200_move_interval(ctx, time_index))) break;
+            float ms = 0;
+            e = cudaEventSynchronize(ctx->ev1);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+            if (e != cudaSuccess) {
+                rc = fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e));
+                break;
+            }
+            if (pass == 1 && ms < chosenMs) {
+                chosenMs = ms;
+                chosen = c;
+            }
+        }
+    ctx->opt = saved;
+    if (!rc) {
+        if (fp32) ctx->opt.launch_shape = chosen;
+        else ctx->opt.block_size = chosen;
+    }
+    cudaError_t e = restore();
+    cudaError_t s = cudaStreamSynchronize(ctx->stream);
+    cudaFree(concCopy);
+    if (rc) return rc;
+    if (e != cudaSuccess || s != cudaSuccess)
+        return fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e != cudaSuccess ? e : s));
+    if (best) *best = chosen;
+    if (best_ms) *best_ms = chosenMs;
     return WACOMM_B200_OK;
 }
 

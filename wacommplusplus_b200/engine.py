@@ -183,6 +183,24 @@ class Engine:
     def move_interval(self, time_index):
         self._check(self._lib.wacomm_b200_move_interval(self._ctx, time_index))
 
+    def graph_capture(self, first_time_index, n_intervals):
+        """Records n_intervals intervals from first_time_index on as one CUDA graph."""
+        self._check(self._lib.wacomm_b200_graph_capture(self._ctx, first_time_index, n_intervals))
+
+    def graph_launch(self):
+        self._check(self._lib.wacomm_b200_graph_launch(self._ctx))
+
+    def graph_release(self):
+        self._check(self._lib.wacomm_b200_graph_release(self._ctx))
+
+    def autotune(self, time_index):
+        """Times each launch configuration on interval time_index and keeps the fastest;
+        returns (chosen launch_shape or block_size, its device ms)."""
+        best, ms = ctypes.c_int(), ctypes.c_float()
+        self._check(self._lib.wacomm_b200_autotune(self._ctx, time_index, ctypes.byref(best),
+                                                   ctypes.byref(ms)))
+        return best.value, ms.value
+
     def move_interval_host(self, time_index, particles):
         """Moves a host record array in place through the pipelined host-buffer entry."""
         assert particles.dtype == PARTICLE_DTYPE and particles.flags.c_contiguous
