@@ -315,3 +315,38 @@ def environment(t0, hours, wind_n=340, seed=11):
     st = t0 + 10800.0 * np.arange(hours // 3 + 1 + (hours % 3 > 0))
     su, sv = vector_series(slon.shape, len(st), 0.1, seed + 1, 3.0, period_records=8.0)
     return {"wind": (wlon, wlat, wt, wu, wv), "stokes": (slon, slat, st, su, sv)}
+
+
+def batched_scenarios(win, n_scenarios=256, seed=5, smallest=1000, largest=256000,
+                      release_hours=24.0, first_id=0):
+    """Independent drift scenarios batched into one particle set: scenario s has a size drawn
+    log-uniform in [smallest, largest] (about 11.8 M in all for 256), its own point source (an
+    interior cell of the grid, 0-1 m deep), its own release window (start uniform in the first
+    ``release_hours`` hours, 1-6 h long, uniform rate) and its own drift object of the leeway
+    catalogue (types 1-22; side left or right per particle). Returns (records, table) with the
+    table giving per scenario: first record, size, object type, release start and end (s)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(smallest), np.log(largest), n_scenarios)).astype(np.int64)
+    total = int(sizes.sum())
+    out = np.zeros(total, dtype=PARTICLE_DTYPE)
+    table = np.zeros(n_scenarios, dtype=[("first", "<i8"), ("size", "<i8"), ("type", "<u2"),
+                                         ("start", "<f8"), ("end", "<f8")])
+    sw1 = 0.1
+    at = 0
+    for s, n in enumerate(sizes):
+        j0, i0 = rng.uniform(8, win.eta - 9), rng.uniform(8, win.xi - 9)
+        start = win.times[0] + rng.uniform(0, release_hours * 3600.0)
+        length = rng.uniform(1.0, 6.0) * 3600.0
+        kind = int(rng.integers(1, 23))
+        rec = out[at:at + n]
+        rec["id"] = np.arange(first_id + at, first_id + at + n, dtype=np.uint64)
+        rec["j"] = j0 + 0.25 * rng.standard_normal(n)
+        rec["i"] = i0 + 0.25 * rng.standard_normal(n)
+        rec["k"] = -rng.uniform(0.0, 1.0, n) / (win.h[0, 0] * sw1)
+        rec["health"] = 1.0
+        rec["time"] = start + (np.arange(n) + 0.5) * (length / n)
+        rec["driftObjectType"] = kind
+        rec["driftSide"] = rng.choice(np.array([-1, 1], np.int8), n)
+        table[s] = (at, n, kind, start, start + length)
+        at += n
+    return out, table
