@@ -17,6 +17,8 @@
  *                                                               Sources.cpp:233-249 (wacomm_b200_emit)
  *   - OceanModelAdapter::kji2deplatlon                          OceanModelAdapter.cpp:271-327
  *                                                               (wacomm_b200_geo_positions)
+ *   - the record normalization of ROMSAdapter::process          OceanModelAdapters/ROMSAdapter.cpp:228-462
+ *                                                               (wacomm_b200_upload_roms_frame)
  *   - EnvironmentalRegridder::bilinearGeographic /              EnvironmentalRegridder.cpp:239-334,
  *     bilinearCurvilinearGeographic of wind and Stokes fields   WacommPlusPlus.cpp:162-173
  *                                                               (wacomm_b200_regrid_environment)
@@ -184,6 +186,33 @@ int wacomm_b200_upload_frame_async(wacomm_b200_context *ctx, int t, const float 
                                    const float *akt, const float *wind_u10,
                                    const float *wind_v10, const float *stokes_u,
                                    const float *stokes_v);
+
+/* ROMS records as the model writes them, normalized on the device into forcing records: the
+ * per-record part of ROMSAdapter::process (OceanModelAdapters/ROMSAdapter.cpp:228-306) with
+ * uv2rho (:309-368) and wakt2wakt (:431-462). set_roms_grid takes the u-face mask [eta][xi-1], the
+ * v-face mask [eta-1][xi] and the grid angle [eta][xi] in radians (NULL when u/v are already
+ * east/north), on the grid of set_grid, whose mask is the rho mask (required); masks must hold 0
+ * or 1 and the angle must be finite on wet nodes (the reference's checks, :139-160).
+ * upload_roms_frame stages record t from u on u faces [s_rho][eta][xi-1], v on v faces
+ * [s_rho][eta-1][xi], w and AKt [s_w][eta][xi] and zeta [eta][xi] (the adapter's own array
+ * orders): zeta is zeroed on land and at fill values >= 1e36, u/v are averaged from the wet faces
+ * to the rho nodes and rotated to east/north in double, w/AKt are zeroed on land. A non-finite u/v
+ * on a wet face or a rotated velocity outside the float range is an error, as in the reference
+ * (the record is then not loaded). Wind and Stokes as in upload_frame. Synchronous. The grid-only
+ * part of process (h and zeta zeroed on land, lon/lat to radians, depth intervals) belongs to the
+ * set_grid arguments. */
+/* Copies the ocean fields of loaded record t back to host arrays in the upload_frame layout (any
+ * pointer may be NULL): the processed input the reference saves with SaveInput
+ * (WacommPlusPlus.cpp:204-216). */
+int wacomm_b200_get_frame(wacomm_b200_context *ctx, int t, float *zeta, float *u, float *v,
+                          float *w, float *akt);
+int wacomm_b200_set_roms_grid(wacomm_b200_context *ctx, const double *mask_u,
+                              const double *mask_v, const double *angle);
+int wacomm_b200_upload_roms_frame(wacomm_b200_context *ctx, int t, const float *zeta,
+                                  const float *u_faces, const float *v_faces, const float *w,
+                                  const float *akt, const float *wind_u10,
+                                  const float *wind_v10, const float *stokes_u,
+                                  const float *stokes_v);
 
 /* Particle records in and out (reference particle_data layout, host memory). set replaces the
  * resident set, append adds after it, get copies the resident records (in their order) into

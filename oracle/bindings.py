@@ -344,3 +344,25 @@ def align_times(src_times, src, dst_times):
     out = np.zeros((dt.size,) + src.shape[1:], dtype=np.float32)
     rc = fn(st.size, _dptr(st), plane, _fptr(src), dt.size, _dptr(dt), _fptr(out))
     return rc, out
+
+
+def roms_normalize(mask_rho, mask_u, mask_v, angle, zeta, u, v, w, akt):
+    """wo_roms_normalize on one ROMS record; returns (code, zeta, u, v, w, akt) on the rho grid.
+    angle None: u/v already east/north."""
+    lib = oracle_lib()
+    fn = lib.wo_roms_normalize
+    if fn.argtypes is None:
+        fn.restype = ctypes.c_int
+        fn.argtypes = [ctypes.c_int] * 3 + [_c_double_p] * 4 + [_c_float_p] * 10
+    f64 = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+    f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+    mask_rho, mask_u, mask_v, angle = f64(mask_rho), f64(mask_u), f64(mask_v), f64(angle)
+    zeta, u, v, w, akt = f32(zeta), f32(u), f32(v), f32(w), f32(akt)
+    eta, xi = mask_rho.shape
+    s_rho = u.shape[0]
+    outs = [np.zeros((eta, xi), np.float32), np.zeros((s_rho, eta, xi), np.float32),
+            np.zeros((s_rho, eta, xi), np.float32), np.zeros((s_rho + 1, eta, xi), np.float32),
+            np.zeros((s_rho + 1, eta, xi), np.float32)]
+    rc = fn(eta, xi, s_rho, _dptr(mask_rho), _dptr(mask_u), _dptr(mask_v), _dptr(angle),
+            _fptr(zeta), _fptr(u), _fptr(v), _fptr(w), _fptr(akt), *[_fptr(o) for o in outs])
+    return (rc, *outs)

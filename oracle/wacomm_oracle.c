@@ -1339,3 +1339,91 @@ int wo_align_times(int nSrc, const double *srcTimes, long plane, const float *sr
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------------------------------
+ * ROMS record normalization (OceanModelAdapters/ROMSAdapter.cpp)
+ * ------------------------------------------------------------------------------------------ */
+
+int wo_roms_normalize(int eta, int xi, int sRho, const double *maskRho, const double *maskU,
+                      const double *maskV, const double *angle, const float *zeta, const float *u,
+                      const float *v, const float *w, const float *akt, float *zetaOut,
+                      float *uOut, float *vOut, float *wOut, float *aktOut) {
+    const int xiU = xi - 1, etaV = eta - 1, sW = sRho + 1;
+    const size_t plane = (size_t)eta * xi, planeU = (size_t)eta * xiU, planeV = (size_t)etaV * xi;
+    /* grid checks (ROMSAdapter.cpp:139-147,148-160) */
+    for (size_t n = 0; n < plane; n++) {
+        if (maskRho[n] != 0.0 && maskRho[n] != 1.0) return WO_ROMS_MASK;
+        if (angle && maskRho[n] > 0.0 && !isfinite(angle[n])) return WO_ROMS_ANGLE;
+    }
+    for (size_t n = 0; n < planeU; n++) {
+        if (maskU[n] != 0.0 && maskU[n] != 1.0) return WO_ROMS_MASK;
+        if (maskU[n] > 0.0)
+            for (int k = 0; k < sRho; k++)
+                if (!isfinite(u[k * planeU + n])) return WO_ROMS_FACE;
+    }
+    for (size_t n = 0; n < planeV; n++) {
+        if (maskV[n] != 0.0 && maskV[n] != 1.0) return WO_ROMS_MASK;
+        if (maskV[n] > 0.0)
+            for (int k = 0; k < sRho; k++)
+                if (!isfinite(v[k * planeV + n])) return WO_ROMS_FACE;
+    }
+    /* zeta (:254-265) */
+    for (size_t n = 0; n < plane; n++)
+        zetaOut[n] = (maskRho[n] == 0 || zeta[n] >= 1e+36f) ? 0.0f : zeta[n];
+    /* uv2rho (:309-368) */
+    for (int k = 0; k < sRho; k++)
+        for (int j = 0; j < eta; j++)
+            for (int i = 0; i < xi; i++) {
+                float usum = 0.0f, vsum = 0.0f;
+                int ucount = 0, vcount = 0;
+                size_t o = k * plane + (size_t)j * xi + i;
+                if (maskRho[(size_t)j * xi + i] > 0.0) {
+                    if (i < xiU && maskU[(size_t)j * xiU + i] > 0.0) {
+                        usum += u[k * planeU + (size_t)j * xiU + i];
+                        ucount++;
+                    }
+                    if (i > 0 && i - 1 < xiU && maskU[(size_t)j * xiU + i - 1] > 0.0) {
+                        usum += u[k * planeU + (size_t)j * xiU + i - 1];
+                        ucount++;
+                    }
+                    if (j < etaV && maskV[(size_t)j * xi + i] > 0.0) {
+                        vsum += v[k * planeV + (size_t)j * xi + i];
+                        vcount++;
+                    }
+                    if (j > 0 && j - 1 < etaV && maskV[(size_t)(j - 1) * xi + i] > 0.0) {
+                        vsum += v[k * planeV + (size_t)(j - 1) * xi + i];
+                        vcount++;
+                    }
+                    uOut[o] = ucount > 0 ? usum / ucount : 0.0f;
+                    vOut[o] = vcount > 0 ? vsum / vcount : 0.0f;
+                } else {
+                    uOut[o] = 0.0f;
+                    vOut[o] = 0.0f;
+                }
+            }
+    /* rotation to east/north (:273-302) */
+    int invalid = 0;
+    for (int k = 0; k < sRho; k++)
+        for (size_t n = 0; n < plane; n++) {
+            if (maskRho[n] <= 0.0) continue;
+            double c = angle ? cos(angle[n]) : 1.0, s = angle ? sin(angle[n]) : 0.0;
+            double gridU = uOut[k * plane + n], gridV = vOut[k * plane + n];
+            double east = angle ? gridU * c - gridV * s : gridU;
+            double north = angle ? gridU * s + gridV * c : gridV;
+            if (!isfinite(east) || !isfinite(north) || fabs(east) > FLT_MAX || fabs(north) > FLT_MAX) {
+                invalid = 1;
+            } else {
+                uOut[k * plane + n] = (float)east;
+                vOut[k * plane + n] = (float)north;
+            }
+        }
+    if (invalid) return WO_ROMS_VELOCITY;
+    /* wakt2wakt (:431-462) */
+    for (int k = 0; k < sW; k++)
+        for (size_t n = 0; n < plane; n++) {
+            int wet = maskRho[n] > 0.0;
+            wOut[k * plane + n] = wet ? w[k * plane + n] : 0.0f;
+            aktOut[k * plane + n] = wet ? akt[k * plane + n] : 0.0f;
+        }
+    return 0;
+}

@@ -8,7 +8,10 @@
  * reference's own known-answer tests (pinned RNG values, leeway catalogue, analytic
  * interval, integrator order ratios, concentration count preservation), and record-for-
  * record against the reference Particle::move compiled from its own sources
- * (oracle/_ref, built by oracle/Makefile when the reference tree is present).
+ * (oracle/_ref, built by oracle/Makefile when the reference tree is present). The regridders are
+ * pinned the same two ways (EnvironmentalRegridderTest.cpp and EnvironmentalRegridder.cpp built
+ * into oracle/_ref); the ROMS normalization only against the known answers of
+ * ROMSAdapterTest.cpp, since the adapter reads NetCDF and is not built here.
  */
 #ifndef WACOMM_ORACLE_H
 #define WACOMM_ORACLE_H
@@ -173,6 +176,23 @@ int wo_regrid_curvilinear(int eta, int xi, const double *lon, const double *lat,
  * plane values per record; out[nDst][plane]. The reference requires equal times instead. */
 int wo_align_times(int nSrc, const double *srcTimes, long plane, const float *src, int nDst,
                    const double *dstTimes, float *out);
+
+/* The per-record normalization of ROMSAdapter::process (OceanModelAdapters/ROMSAdapter.cpp:
+ * 228-306, uv2rho :309-368, wakt2wakt :431-462): zeta zeroed on land and at fill values (>= 1e36),
+ * u/v averaged from the wet faces to the rho nodes, rotated by the grid angle to east/north
+ * (angle NULL: already earth-relative), w/AKt zeroed on land. mask_rho [eta][xi], mask_u
+ * [eta][xi-1], mask_v [eta-1][xi] (0 or 1); u [sRho][eta][xi-1], v [sRho][eta-1][xi], w/akt
+ * [sRho+1][eta][xi], zeta [eta][xi]; outputs on the rho grid. Returns 0, WO_ROMS_MASK (a mask
+ * value other than 0/1), WO_ROMS_ANGLE (a non-finite angle at a wet node), WO_ROMS_FACE (a
+ * non-finite u/v at a wet face) or WO_ROMS_VELOCITY (a rotated velocity outside the float range). */
+#define WO_ROMS_MASK (-1)
+#define WO_ROMS_ANGLE (-2)
+#define WO_ROMS_FACE (-3)
+#define WO_ROMS_VELOCITY (-4)
+int wo_roms_normalize(int eta, int xi, int sRho, const double *maskRho, const double *maskU,
+                      const double *maskV, const double *angle, const float *zeta, const float *u,
+                      const float *v, const float *w, const float *akt, float *zetaOut,
+                      float *uOut, float *vOut, float *wOut, float *aktOut);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,9 @@ SIGNATURES = {
     "wacomm_b200_geo_positions": (_i, [_vp, _dp, _dp, _dp, _sz]),
     "wacomm_b200_regrid_environment": (_i, [_vp, _i, _i, _i, _i, _dp, _dp, _i, _dp, _fp, _fp]),
     "wacomm_b200_clear_environment": (_i, [_vp, _i]),
+    "wacomm_b200_get_frame": (_i, [_vp, _i] + [_fp] * 5),
+    "wacomm_b200_set_roms_grid": (_i, [_vp, _dp, _dp, _dp]),
+    "wacomm_b200_upload_roms_frame": (_i, [_vp, _i] + [_fp] * 9),
     "wacomm_b200_graph_capture": (_i, [_vp, _i, _i]),
     "wacomm_b200_graph_launch": (_i, [_vp]),
     "wacomm_b200_graph_release": (_i, [_vp]),

@@ -123,6 +123,13 @@ struct wacomm_b200_context {
     std::vector<uint64_t> graphLayout;
     int graphLaunches = 0;
     bool capturing = false;
+    // ROMS grid (wacomm_b200_set_roms_grid): rho/u/v masks as bytes in one allocation, the
+    // angle's (cos, sin) per rho node (null: earth-relative), and staging for raw records.
+    uint8_t *dRomsMask = nullptr;
+    double2 *dRomsRot = nullptr;
+    bool hasRoms = false;
+    float *dRomsRaw = nullptr;
+    size_t romsRawCap = 0;
     // Wind (0) and Stokes (1) fields regridded to the rho nodes and the forcing times, [T][eta][xi]
     // each; a frame's own uploaded fields take precedence over these.
     EnvField env[2];
@@ -333,6 +340,17 @@ FrameDevice frame_of(const wacomm_b200_context *ctx, int t) {
         f.stokesV = ctx->env[1].v + at;
     }
     return f;
+}
+
+void release_roms(wacomm_b200_context *ctx) {
+    cudaFree(ctx->dRomsMask);
+    cudaFree(ctx->dRomsRot);
+    cudaFree(ctx->dRomsRaw);
+    ctx->dRomsMask = nullptr;
+    ctx->dRomsRot = nullptr;
+    ctx->dRomsRaw = nullptr;
+    ctx->romsRawCap = 0;
+    ctx->hasRoms = false;
 }
 
 void release_environment(wacomm_b200_context *ctx) {
@@ -782,6 +800,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dSWValues);
     cudaFree(ctx->dGeoOut);
     release_environment(ctx);
+    release_roms(ctx);
     if (ctx->graphExec) cudaGraphExecDestroy(ctx->graphExec);
     cudaFree(ctx->dSteps);
     cudaFree(ctx->dErr);
@@ -872,6 +891,7 @@ int wacomm_b200_set_grid(wacomm_b200_context *ctx, int eta, int xi, int s_rho, i
     ctx->dGeoLon = ctx->dGeoLat = ctx->dSWValues = nullptr;
     ctx->hasGeo = false;
     release_environment(ctx);
+    release_roms(ctx);
     CUDA_TRY(ctx, cudaMalloc(&ctx->dLon, plane * sizeof(double)));
     CUDA_TRY(ctx, cudaMalloc(&ctx->dLat, plane * sizeof(double)));
     CUDA_TRY(ctx, cudaMalloc(&ctx->dH, plane * sizeof(double)));
@@ -936,9 +956,11 @@ namespace {
 // the compute stream is drained first and the copies are waited for. Asynchronous: the copy
 // stream waits for the work enqueued so far on the compute stream (which may still read the
 // slot), and the slot's ready event is recorded for the next interval to wait on.
+// With copyOcean false the ocean fields' device arrays are only allocated (their values come from
+// a kernel afterwards).
 int stage_frame(wacomm_b200_context *ctx, int t, const float *zeta, const float *u, const float *v,
                 const float *w, const float *akt, const float *wind_u10, const float *wind_v10,
-                const float *stokes_u, const float *stokes_v, bool async) {
+                const float *stokes_u, const float *stokes_v, bool async, bool copyOcean = true) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     if (!ctx->hasGrid) return fail(ctx, WACOMM_B200_ERR_STATE, "set_grid has not been called");
     if (t < 0 || t >= (int)ctx->times.size())
@@ -973,12 +995,17 @@ int stage_frame(wacomm_b200_context *ctx, int t, const float *zeta, const float 
         // The pair cache may reference this slot: finish kernels that read it first.
         CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     }
+    auto ocean = [&](float *&dst, const float *src, size_t count) -> int {
+        if (copyOcean) return put(dst, src, count);
+        if (!dst) CUDA_TRY(ctx, cudaMalloc(&dst, count * sizeof(float)));
+        return WACOMM_B200_OK;
+    };
     int rc;
-    if ((rc = put(s.zeta, zeta, plane))) return rc;
-    if ((rc = put(s.u, u, plane * ctx->sRho))) return rc;
-    if ((rc = put(s.v, v, plane * ctx->sRho))) return rc;
-    if ((rc = put(s.w, w, plane * ctx->sW))) return rc;
-    if ((rc = put(s.akt, akt, plane * ctx->sW))) return rc;
+    if ((rc = ocean(s.zeta, zeta, plane))) return rc;
+    if ((rc = ocean(s.u, u, plane * ctx->sRho))) return rc;
+    if ((rc = ocean(s.v, v, plane * ctx->sRho))) return rc;
+    if ((rc = ocean(s.w, w, plane * ctx->sW))) return rc;
+    if ((rc = ocean(s.akt, akt, plane * ctx->sW))) return rc;
     if ((rc = put(s.windU, wind_u10, plane))) return rc;
     if ((rc = put(s.windV, wind_v10, plane))) return rc;
     if ((rc = put(s.stokesU, stokes_u, plane))) return rc;
@@ -1939,6 +1966,141 @@ int wacomm_b200_autotune(wacomm_b200_context *ctx, int time_index, int *best, fl
         return fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e != cudaSuccess ? e : s));
     if (best) *best = chosen;
     if (best_ms) *best_ms = chosenMs;
+    return WACOMM_B200_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int wacomm_b200_set_roms_grid(wacomm_b200_context *ctx, const double *mask_u,
+                              const double *mask_v, const double *angle) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!ctx->hasGrid || !ctx->hasMask)
+        return fail(ctx, WACOMM_B200_ERR_STATE, "set_grid with the rho mask comes first");
+    if (!mask_u || !mask_v) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null mask");
+    cudaSetDevice(ctx->device);
+    const int eta = ctx->eta, xi = ctx->xi;
+    const size_t plane = (size_t)eta * xi, planeU = (size_t)eta * (xi - 1),
+                 planeV = (size_t)(eta - 1) * xi;
+    std::vector<double> maskRho(plane);
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpy(maskRho.data(), ctx->dMask, plane * sizeof(double),
+                             cudaMemcpyDeviceToHost));
+    // ROMSAdapter.cpp:139-160: masks of 0 and 1 only, a finite angle at every wet node
+    std::vector<uint8_t> bytes(plane + planeU + planeV);
+    auto take = [&](const double *m, size_t count, uint8_t *out) {
+        for (size_t n = 0; n < count; n++) {
+            if (m[n] != 0.0 && m[n] != 1.0) return false;
+            out[n] = m[n] > 0.0;
+        }
+        return true;
+    };
+    if (!take(maskRho.data(), plane, bytes.data()) || !take(mask_u, planeU, bytes.data() + plane) ||
+        !take(mask_v, planeV, bytes.data() + plane + planeU))
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "ROMS masks must hold 0 or 1 only");
+    std::vector<double2> rot;
+    if (angle) {
+        rot.resize(plane);
+        for (size_t n = 0; n < plane; n++) {
+            if (maskRho[n] > 0.0 && !std::isfinite(angle[n]))
+                return fail(ctx, WACOMM_B200_ERR_ARGUMENT,
+                            "ROMS angle is non-finite at wet rho node %zu", n);
+            // ROMSAdapter.cpp:276-280, with the host libm the reference uses
+            rot[n] = maskRho[n] > 0.0 ? make_double2(std::cos(angle[n]), std::sin(angle[n]))
+                                      : make_double2(1.0, 0.0);
+        }
+    }
+    release_roms(ctx);
+    CUDA_TRY(ctx, cudaMalloc(&ctx->dRomsMask, bytes.size()));
+    CUDA_TRY(ctx, cudaMemcpy(ctx->dRomsMask, bytes.data(), bytes.size(), cudaMemcpyHostToDevice));
+    if (angle) {
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dRomsRot, plane * sizeof(double2)));
+        CUDA_TRY(ctx, cudaMemcpy(ctx->dRomsRot, rot.data(), plane * sizeof(double2),
+                                 cudaMemcpyHostToDevice));
+    }
+    ctx->hasRoms = true;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_upload_roms_frame(wacomm_b200_context *ctx, int t, const float *zeta,
+                                  const float *u_faces, const float *v_faces, const float *w,
+                                  const float *akt, const float *wind_u10,
+                                  const float *wind_v10, const float *stokes_u,
+                                  const float *stokes_v) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!ctx->hasRoms) return fail(ctx, WACOMM_B200_ERR_STATE, "set_roms_grid has not been called");
+    if (t < 0 || t >= (int)ctx->times.size())
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "frame %d out of [0, %zu)", t, ctx->times.size());
+    if (!zeta || !u_faces || !v_faces || !w || !akt)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null field");
+    // wind and Stokes as upload_frame takes them; the ocean fields follow
+    int rc = stage_frame(ctx, t, zeta, zeta, zeta, zeta, zeta, wind_u10, wind_v10, stokes_u,
+                         stokes_v, false, false);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    const int eta = ctx->eta, xi = ctx->xi, sRho = ctx->sRho, sW = ctx->sW;
+    const size_t plane = (size_t)eta * xi, planeU = (size_t)eta * (xi - 1),
+                 planeV = (size_t)(eta - 1) * xi;
+    const size_t nU = sRho * planeU, nV = sRho * planeV, nW = sW * plane;
+    const size_t raw = plane + nU + nV + 2 * nW;
+    if ((rc = grow(ctx, ctx->dRomsRaw, ctx->romsRawCap, raw))) return rc;
+    float *r = ctx->dRomsRaw;
+    FrameSlot &s = ctx->slots[t];
+    CUDA_TRY(ctx, cudaMemcpyAsync(r, zeta, plane * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(r + plane, u_faces, nU * sizeof(float), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(r + plane + nU, v_faces, nV * sizeof(float),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(r + plane + nU + nV, w, nW * sizeof(float),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(r + plane + nU + nV + nW, akt, nW * sizeof(float),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemsetAsync(ctx->dErr, 0, sizeof(int), ctx->stream));
+    RomsGrid G{ctx->dRomsMask, ctx->dRomsMask + plane, ctx->dRomsMask + plane + planeU,
+               ctx->dRomsRot, eta, xi, sRho};
+    RomsRecord R{r, r + plane, r + plane + nU, r + plane + nU + nV, r + plane + nU + nV + nW,
+                 s.zeta, s.u, s.v, s.w, s.akt};
+    CUDA_TRY(ctx, roms_record(G, R, ctx->dErr, ctx->stream));
+    int err = 0;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&err, ctx->dErr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (err) {
+        s.loaded = false;
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "%s",
+                    (err & ROMS_ERR_FACE) ? "ROMS u or v is non-finite at a wet face"
+                                          : "ROMS normalized velocity is outside finite float range");
+    }
+    return WACOMM_B200_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int wacomm_b200_get_frame(wacomm_b200_context *ctx, int t, float *zeta, float *u, float *v,
+                          float *w, float *akt) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (t < 0 || t >= (int)ctx->times.size())
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "frame %d out of [0, %zu)", t, ctx->times.size());
+    const FrameSlot &s = ctx->slots[t];
+    if (!s.loaded) return fail(ctx, WACOMM_B200_ERR_STATE, "record %d is not loaded", t);
+    cudaSetDevice(ctx->device);
+    const size_t plane = (size_t)ctx->eta * ctx->xi;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
+    auto get = [&](float *dst, const float *src, size_t count) -> int {
+        if (dst)
+            CUDA_TRY(ctx, cudaMemcpyAsync(dst, src, count * sizeof(float), cudaMemcpyDeviceToHost,
+                                          ctx->stream));
+        return WACOMM_B200_OK;
+    };
+    int rc;
+    if ((rc = get(zeta, s.zeta, plane))) return rc;
+    if ((rc = get(u, s.u, plane * ctx->sRho))) return rc;
+    if ((rc = get(v, s.v, plane * ctx->sRho))) return rc;
+    if ((rc = get(w, s.w, plane * ctx->sW))) return rc;
+    if ((rc = get(akt, s.akt, plane * ctx->sW))) return rc;
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return WACOMM_B200_OK;
 }
 

@@ -168,6 +168,28 @@ cudaError_t regrid_apply(bool curvilinear, const RegridPlan *plan, long long nTa
                          const RegridTime *times, int nTimes, float *outU, float *outV,
                          cudaStream_t stream);
 
+// roms.cu ----------------------------------------------------------------------------------
+
+constexpr int ROMS_ERR_FACE = 1, ROMS_ERR_VELOCITY = 2;
+
+// Grid part of the ROMS normalization: masks of rho nodes [eta][xi], u faces [eta][xi-1] and v
+// faces [eta-1][xi] as 0/1 bytes; (cos, sin) of the grid angle per rho node, or null when the
+// velocities are already east/north.
+struct RomsGrid {
+    const uint8_t *maskRho, *maskU, *maskV;
+    const double2 *rotation;
+    int eta, xi, sRho;
+};
+
+// One raw ROMS record (u [sRho][eta][xi-1], v [sRho][eta-1][xi], w/akt [sRho+1][eta][xi], zeta
+// [eta][xi]) and the forcing record it becomes (u, v on the rho nodes).
+struct RomsRecord {
+    const float *zeta, *u, *v, *w, *akt;
+    float *zetaOut, *uOut, *vOut, *wOut, *aktOut;
+};
+
+cudaError_t roms_record(const RomsGrid &G, const RomsRecord &R, int *err, cudaStream_t stream);
+
 // surrogate.cu -----------------------------------------------------------------------------
 
 // One surrogate interval: grid, interval, run parameters, the dry-node table, the per-cell layer-1

@@ -183,6 +183,35 @@ class Engine:
     def move_interval(self, time_index):
         self._check(self._lib.wacomm_b200_move_interval(self._ctx, time_index))
 
+    def get_frame(self, t):
+        """dict of the ocean fields of loaded record t (zeta, u, v, w, akt) as float32."""
+        s_rho, eta, xi = self._grid_shape
+        out = {"zeta": np.empty((eta, xi), np.float32),
+               "u": np.empty((s_rho, eta, xi), np.float32),
+               "v": np.empty((s_rho, eta, xi), np.float32),
+               "w": np.empty((s_rho + 1, eta, xi), np.float32),
+               "akt": np.empty((s_rho + 1, eta, xi), np.float32)}
+        self._check(self._lib.wacomm_b200_get_frame(
+            self._ctx, t, *[out[k].ctypes.data_as(_fp) for k in ("zeta", "u", "v", "w", "akt")]))
+        return out
+
+    def set_roms_grid(self, mask_u, mask_v, angle=None):
+        """u-face mask [eta, xi-1], v-face mask [eta-1, xi] and the grid angle [eta, xi] in
+        radians (None: velocities already east/north) for upload_roms_frame."""
+        self._roms = [_d(mask_u), _d(mask_v), None if angle is None else _d(angle)]
+        self._check(self._lib.wacomm_b200_set_roms_grid(
+            self._ctx, self._roms[0][1], self._roms[1][1],
+            None if angle is None else self._roms[2][1]))
+
+    def upload_roms_frame(self, t, zeta, u_faces, v_faces, w, akt, wind_u10=None, wind_v10=None,
+                          stokes_u=None, stokes_v=None):
+        """Forcing record t from a raw ROMS record (u/v on their faces), normalized on the
+        device."""
+        args = [_f(a) for a in (zeta, u_faces, v_faces, w, akt, wind_u10, wind_v10, stokes_u,
+                                stokes_v)]
+        self._check(self._lib.wacomm_b200_upload_roms_frame(
+            self._ctx, t, *[None if a is None else a[1] for a in args]))
+
     def graph_capture(self, first_time_index, n_intervals):
         """Records n_intervals intervals from first_time_index on as one CUDA graph."""
         self._check(self._lib.wacomm_b200_graph_capture(self._ctx, first_time_index, n_intervals))
