@@ -296,7 +296,7 @@ def run_batched(args):
 
     hours = 48
     win = syn.config1_window(n_frames=hours + 1)
-    records, table = syn.batched_scenarios(win)
+    records, table = syn.batched_scenarios(win, n_scenarios=args.scenarios)
     n = len(records)
     env = syn.environment(win.times[0], hours)
     cfg = default_config(random=True, randomSeed=23, driftModel=1)
@@ -373,7 +373,7 @@ def run_batched(args):
         "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": mean_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "batched: 256 drift scenarios (log-uniform 1k-256k, "
+        "config": {"workload": f"batched: {args.scenarios} drift scenarios (log-uniform 1k-256k, "
                                f"{n} particles, own source, release window and leeway object), "
                                "analytic 128x128x10 ocean, 48 h at dt=30 s, wind 340x340 3-km "
                                "curvilinear hourly and Stokes 0.05-degree 3-hourly regridded on "
@@ -497,6 +497,8 @@ def main():
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-cpu", action="store_true")
     parser.add_argument("--no-surrogate", action="store_true")
+    parser.add_argument("--scenarios", type=int, default=256,
+                        help="batched workload: number of scenarios")
     parser.add_argument("--workload", default="precision",
                         choices=["precision", "realistic", "batched"])
     args = parser.parse_args()

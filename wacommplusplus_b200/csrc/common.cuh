@@ -145,31 +145,36 @@ __device__ __forceinline__ void philox_normals3(uint64_t key, long long interval
 // ------------------------------------------------------------------ drift objects
 // Leeway regression coefficients per DriftObjectType id, in LeewayCoefficients order
 // (DriftModel.hpp:46-56; values DriftModel.hpp:176-202).
-__constant__ static double c_leeway_catalogue[23][9] = {
-    {0, 0, 0, 0, 0, 0, 0, 0, 0},
-    {.0096, 0, .12, .0054, 0, .094, -.0054, 0, .094},
-    {.0339, 0, .024, .0149, 0, .024, -.0149, 0, .024},
-    {.0121, 0, .12, .0092, 0, .094, -.0092, 0, .094},
-    {.0247, 0, .12, .0276, 0, .094, -.0276, 0, .094},
-    {.0125, .0396, .0281, .0019, .0114, .0436, -.0019, -.0114, .0436},
-    {.0048, 0, .083, .0015, 0, .067, -.0015, 0, .067},
-    {.0171, .0112, .0393, .0136, -.033, .0171, -.0013, -.0265, .0162},
-    {.01117, .102, .0304, .0004, .039, .0405, -.0004, -.039, .0405},
-    {.0352, -.025, .061, .0062, -.03, .035, -.0045, -.002, .036},
-    {.0088, 0, .025, .0018, 0, .024, -.0018, 0, .024},
-    {.0116, .1112, .0412, .0041, 0, .0439, -.0041, 0, .0439},
-    {.0193, 0, .083, .0051, 0, .067, -.0051, 0, .067},
-    {.0315, 0, .022, .0129, 0, .022, -.0129, 0, .022},
-    {.0165, 0, .031, .0039, 0, .029, -.0039, 0, .029},
-    {.0654, 0, .03, .0219, 0, .028, -.0219, 0, .028},
-    {.0187, 0, .083, .0209, 0, .067, -.0209, 0, .067},
-    {.045, 0, .194, .0495, 0, .1842, -.0282, 0, .2495},
-    {.0197, 0, .083, .0036, 0, .067, -.0036, 0, .067},
-    {.0075, .0266, .0283, .0048, .0288, .0392, -.0045, -.0146, .0459},
-    {.0107, .0447, .0655, .0041, .0115, .0413, -.0041, -.0115, .0413},
-    {.0156, .083, .0153, .00078, .027, .0152, -.00078, -.027, .0152},
-    {.0275, 0, .12, .005, 0, .094, -.005, 0, .094},
-};
+#define WB_LEEWAY_CATALOGUE { \
+    {0, 0, 0, 0, 0, 0, 0, 0, 0}, \
+    {.0096, 0, .12, .0054, 0, .094, -.0054, 0, .094}, \
+    {.0339, 0, .024, .0149, 0, .024, -.0149, 0, .024}, \
+    {.0121, 0, .12, .0092, 0, .094, -.0092, 0, .094}, \
+    {.0247, 0, .12, .0276, 0, .094, -.0276, 0, .094}, \
+    {.0125, .0396, .0281, .0019, .0114, .0436, -.0019, -.0114, .0436}, \
+    {.0048, 0, .083, .0015, 0, .067, -.0015, 0, .067}, \
+    {.0171, .0112, .0393, .0136, -.033, .0171, -.0013, -.0265, .0162}, \
+    {.01117, .102, .0304, .0004, .039, .0405, -.0004, -.039, .0405}, \
+    {.0352, -.025, .061, .0062, -.03, .035, -.0045, -.002, .036}, \
+    {.0088, 0, .025, .0018, 0, .024, -.0018, 0, .024}, \
+    {.0116, .1112, .0412, .0041, 0, .0439, -.0041, 0, .0439}, \
+    {.0193, 0, .083, .0051, 0, .067, -.0051, 0, .067}, \
+    {.0315, 0, .022, .0129, 0, .022, -.0129, 0, .022}, \
+    {.0165, 0, .031, .0039, 0, .029, -.0039, 0, .029}, \
+    {.0654, 0, .03, .0219, 0, .028, -.0219, 0, .028}, \
+    {.0187, 0, .083, .0209, 0, .067, -.0209, 0, .067}, \
+    {.045, 0, .194, .0495, 0, .1842, -.0282, 0, .2495}, \
+    {.0197, 0, .083, .0036, 0, .067, -.0036, 0, .067}, \
+    {.0075, .0266, .0283, .0048, .0288, .0392, -.0045, -.0146, .0459}, \
+    {.0107, .0447, .0655, .0041, .0115, .0413, -.0041, -.0115, .0413}, \
+    {.0156, .083, .0153, .00078, .027, .0152, -.00078, -.027, .0152}, \
+    {.0275, 0, .12, .005, 0, .094, -.005, 0, .094}, \
+}
+
+__constant__ static double c_leeway_catalogue[23][9] = WB_LEEWAY_CATALOGUE;
+// The same rows in FP32 for the FP32 step, read through L1 (lanes of a warp may hold
+// different objects; constant-bank reads of different addresses would serialize).
+__device__ static const float c_leeway_catalogue_f32[23][9] = WB_LEEWAY_CATALOGUE;
 
 struct Leeway {
     double u, v;

@@ -107,14 +107,18 @@ __device__ __forceinline__ void current_cell(const CellView<STORE> &C, int kI, f
 }
 
 
-// Leeway and Stokes velocity of a drifting object (the drift branch of advective_velocity).
+// Leeway and Stokes velocity of a drifting object (the drift branch of advective_velocity) in FP32:
+// wind and Stokes interpolated from the environment pair, the leeway regression of the object's
+// catalogue row (computeLeeway, DriftModel.hpp:204-219) on the interpolated 10-m wind. The
+// position-dependent parts (calibration regions, wind-error fields) run in FP64 and only when the
+// run configures them.
 template <class View>
 __device__ __forceinline__ void drift_velocity(const wacomm_b200_config &cfg, const IntervalParams &P,
                                             const View &V, uint64_t id, int type, int side,
-                                            int jI, double jF, int iI, double iF, double sa,
+                                            int jI, float jF, int iI, float iF, float a,
                                             double elapsed, double physicalTime, double stepDt,
                                             float &du, float &dv) {
-    double windU = cfg.windU10, windV = cfg.windV10;
+    float windU = (float)cfg.windU10, windV = (float)cfg.windV10;
     EnvPair e1{}, e2{}, e3{}, e4{};
     if (V.hasWindU || V.hasWindV || V.hasStokes) {
         e1 = V.environment(jI, iI);
@@ -122,49 +126,62 @@ __device__ __forceinline__ void drift_velocity(const wacomm_b200_config &cfg, co
         e3 = V.environment(jI + 1, iI + 1);
         e4 = V.environment(jI, iI + 1);
     }
-    float fi = (float)iF, fj = (float)jF, a = (float)sa;
-    float w1 = (1.f - fi) * (1.f - fj), w2 = (1.f - fi) * fj, w3 = fi * fj, w4 = fi * (1.f - fj);
+    const float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
     if (V.hasWindU)
         windU = at_f32(e1.wu0 * w1 + e2.wu0 * w2 + e3.wu0 * w3 + e4.wu0 * w4,
                        e1.wu1 * w1 + e2.wu1 * w2 + e3.wu1 * w3 + e4.wu1 * w4, a);
     if (V.hasWindV)
         windV = at_f32(e1.wv0 * w1 + e2.wv0 * w2 + e3.wv0 * w3 + e4.wv0 * w4,
                        e1.wv1 * w1 + e2.wv1 * w2 + e3.wv1 * w3 + e4.wv1 * w4, a);
-    double longitude = V.lon(jI, iI) * (1.0 - iF) * (1.0 - jF) + V.lon(jI + 1, iI) * (1.0 - iF) * jF +
-                       V.lon(jI + 1, iI + 1) * iF * jF + V.lon(jI, iI + 1) * iF * (1.0 - jF);
-    double latitude = V.lat(jI, iI) * (1.0 - iF) * (1.0 - jF) + V.lat(jI + 1, iI) * (1.0 - iF) * jF +
-                      V.lat(jI + 1, iI + 1) * iF * jF + V.lat(jI, iI + 1) * iF * (1.0 - jF);
-    double stdDev = cfg.windErrorStdDev, corr = cfg.windErrorComponentCorrelation;
-    double spatial = cfg.windErrorSpatialScale, temporal = cfg.windErrorTemporalScale;
-    int region = calibration_region(cfg, longitude, latitude);
-    if (region >= 0) {
-        const wacomm_b200_calibration_region &g = cfg.observationalCalibrationRegions[region];
-        stdDev = g.windErrorStdDev;
-        corr = g.windErrorComponentCorrelation;
-        spatial = g.windErrorSpatialScale;
-        temporal = g.windErrorTemporalScale;
+    if (cfg.observationalCalibrationRegionCount > 0 || cfg.windErrorStdDev > 0) {
+        const double jd = jF, id_ = iF;
+        double longitude = V.lon(jI, iI) * (1.0 - id_) * (1.0 - jd) + V.lon(jI + 1, iI) * (1.0 - id_) * jd +
+                           V.lon(jI + 1, iI + 1) * id_ * jd + V.lon(jI, iI + 1) * id_ * (1.0 - jd);
+        double latitude = V.lat(jI, iI) * (1.0 - id_) * (1.0 - jd) + V.lat(jI + 1, iI) * (1.0 - id_) * jd +
+                          V.lat(jI + 1, iI + 1) * id_ * jd + V.lat(jI, iI + 1) * id_ * (1.0 - jd);
+        double stdDev = cfg.windErrorStdDev, corr = cfg.windErrorComponentCorrelation;
+        double spatial = cfg.windErrorSpatialScale, temporal = cfg.windErrorTemporalScale;
+        int region = calibration_region(cfg, longitude, latitude);
+        if (region >= 0) {
+            const wacomm_b200_calibration_region &g = cfg.observationalCalibrationRegions[region];
+            stdDev = g.windErrorStdDev;
+            corr = g.windErrorComponentCorrelation;
+            spatial = g.windErrorSpatialScale;
+            temporal = g.windErrorTemporalScale;
+        }
+        if (stdDev > 0) {
+            uint64_t substep = (uint64_t)floor(elapsed / cfg.dti);
+            double when = physicalTime + .5 * P.direction * stepDt;
+            double first = forcing_error_normal(cfg.randomSeed, id, P.intervalKey, substep,
+                                                WIND_U_COMPONENT, longitude, latitude, when,
+                                                spatial, temporal);
+            double second = forcing_error_normal(cfg.randomSeed, id, P.intervalKey, substep,
+                                                 WIND_V_COMPONENT, longitude, latitude, when,
+                                                 spatial, temporal);
+            windU = (float)(windU + stdDev * first);
+            windV = (float)(windV + stdDev * correlated_normal(first, second, corr));
+        }
     }
-    if (stdDev > 0) {
-        uint64_t substep = (uint64_t)floor(elapsed / cfg.dti);
-        double when = physicalTime + .5 * P.direction * stepDt;
-        double first = forcing_error_normal(cfg.randomSeed, id, P.intervalKey, substep,
-                                            WIND_U_COMPONENT, longitude, latitude, when, spatial,
-                                            temporal);
-        double second = forcing_error_normal(cfg.randomSeed, id, P.intervalKey, substep,
-                                             WIND_V_COMPONENT, longitude, latitude, when, spatial,
-                                             temporal);
-        windU += stdDev * first;
-        windV += stdDev * correlated_normal(first, second, corr);
-    }
-    double dn = 0, cn = 0;
+    float dn = 0.f, cn = 0.f;
     if (cfg.leewayCoefficientEnsemble) {
         uint64_t ens = key_prefix(cfg.randomSeed, id, ENSEMBLE_INTERVAL, 0);
-        dn = prefix_normal(ens, 0);
-        cn = correlated_normal(dn, prefix_normal(ens, 1), cfg.leewayResidualCorrelation);
+        double n0 = prefix_normal(ens, 0);
+        dn = (float)n0;
+        cn = (float)correlated_normal(n0, prefix_normal(ens, 1), cfg.leewayResidualCorrelation);
     }
-    Leeway lw = compute_leeway(type, windU, windV, side, dn, cn);
-    du = (float)lw.u;
-    dv = (float)lw.v;
+    du = dv = 0.f;
+    const float speed = sqrtf(windU * windU + windV * windV);
+    if (speed >= 1.0e-12f && side != 0 && type >= 0 && type <= 22) {
+        const float *c = c_leeway_catalogue_f32[type];
+        const bool right = side == 1;
+        const float rs = 1.0f / speed;
+        const float ux = windU * rs, uy = windV * rs;
+        const float downwind = __ldg(c + 0) * speed + __ldg(c + 1) + __ldg(c + 2) * dn;
+        const float crosswind = right ? __ldg(c + 3) * speed + __ldg(c + 4) + __ldg(c + 5) * cn
+                                      : __ldg(c + 6) * speed + __ldg(c + 7) - __ldg(c + 8) * cn;
+        du = downwind * ux - crosswind * uy;
+        dv = downwind * uy + crosswind * ux;
+    }
     if (V.hasStokes) {
         du += at_f32(e1.su0 * w1 + e2.su0 * w2 + e3.su0 * w3 + e4.su0 * w4,
                      e1.su1 * w1 + e2.su1 * w2 + e3.su1 * w3 + e4.su1 * w4, a);
@@ -256,8 +273,8 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         current_cell(C, kM, kF, jI, jF, iI, iF, sa, alpha, diffuse, uu, vv, ww, aa);
         if (drift) {
             float du, dv;
-            drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, (double)jF, iI, (double)iF, sa,
-                           elapsed, physicalTime, stepDt, du, dv);
+            drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, jF, iI, iF, sa, elapsed,
+                           physicalTime, stepDt, du, dv);
             uu += du;
             vv += dv;
         }
@@ -312,8 +329,8 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 current_cell(C, kMI, kMF, jMI, jMF, iMI, iMF, alpha, alpha, false, um, vm, wm, unused);
                 if (drift) {
                     float du, dv;
-                    drift_velocity(cfg, P, V, p.id, p.type, p.side, jMI, (double)jMF, iMI,
-                                   (double)iMF, (double)alpha, elapsed, physicalTime, stepDt, du, dv);
+                    drift_velocity(cfg, P, V, p.id, p.type, p.side, jMI, jMF, iMI, iMF, alpha,
+                                   elapsed, physicalTime, stepDt, du, dv);
                     um += du;
                     vm += dv;
                 }
@@ -327,8 +344,8 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 current_cell(C, kM, kF, jI, jF, iI, iF, alpha, alpha, false, ue, ve, we, unused);
                 if (drift) {
                     float du, dv;
-                    drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, (double)jF, iI,
-                                   (double)iF, (double)alpha, elapsed, physicalTime, stepDt, du, dv);
+                    drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, jF, iI, iF, alpha, elapsed,
+                                   physicalTime, stepDt, du, dv);
                     ue += du;
                     ve += dv;
                 }
