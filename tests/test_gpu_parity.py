@@ -210,6 +210,28 @@ def test_host_buffer_entry_matches_resident_path(cuda_device):
         assert records_equal(host, resident)
 
 
+@pytest.mark.parametrize("n", [2_200_000, 4_500_001, 9_000_000])
+def test_host_buffer_slabs_match_resident_path(cuda_device, n):
+    """Every slab layout of the host-buffer entry (two slabs; small end slabs around one or two
+    middle slabs) gives the resident path's records and concentration."""
+    win = syn.config1_window(n_frames=3)
+    p0 = syn.uniform_particles(n, win.eta, win.xi, seed=8)
+    cfg = default_config(random=True, randomSeed=4)
+    with Engine(cuda_device, arithmetic="fp32", rng="philox") as e:
+        e.load_window(win)
+        e.set_config(cfg)
+        e.concentration_reset(win.T)
+        e.set_particles(p0)
+        e.move_interval(0)
+        resident, conc = e.get_particles(), e.concentration()
+        e.concentration_reset(win.T)
+        host = p0.copy()
+        e.move_interval_host(0, host)
+        assert e.stats()["particle_steps"] == 120 * n
+        assert records_equal(host, resident)
+        assert np.array_equal(e.concentration(), conc)
+
+
 def test_remove_dead_keeps_order(cuda_device):
     win = syn.config1_window(n_frames=2)
     p = syn.uniform_particles(1000, win.eta, win.xi, seed=3)

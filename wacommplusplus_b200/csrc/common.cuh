@@ -18,6 +18,13 @@ constexpr int STORE_F32 = WACOMM_B200_STORAGE_FP32;
 constexpr int STORE_F16 = WACOMM_B200_STORAGE_FP16;
 constexpr int STORE_BF16 = WACOMM_B200_STORAGE_BF16;
 
+// Compiled forms of the FP32 step (move_particle_fast's VARIANT): the branches a run can reach.
+constexpr int VAR_LEAN = 0;     // deterministic passive tracking: no random walk, drift or jibing
+constexpr int VAR_DIFFUSE = 1;  // random walk; no drifting objects, no jibing
+constexpr int VAR_DRIFT = 2;    // leeway drift without wind-error fields, calibration regions or
+                                // coefficient ensemble, with or without the random walk; no jibing
+constexpr int VAR_FULL = 3;     // every branch
+
 constexpr int CLOSURE_CONSTRAINT = 1;  // Config.hpp:201-203
 constexpr int CLOSURE_KILL = 2;
 constexpr int CLOSURE_REFLECTION = 3;

@@ -1119,10 +1119,22 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
     if ((rc = reserve_work(ctx, n))) return rc;
     if ((rc = grow(ctx, ctx->dAos, ctx->aosCap, n))) return rc;
     ctx->n = n;
-    // Slabs: the upload of slab s+1 and the download of slab s-1 overlap the move of slab s.
-    const size_t minSlab = (size_t)1 << 20;
-    int slabs = n >= 4 * minSlab ? 4 : (n >= 2 * minSlab ? 2 : 1);
-    size_t per = (n + slabs - 1) / slabs;
+    // Slabs: the upload of slab s+1 and the download of slab s-1 overlap the move of slab s. Only
+    // the first upload and the last download are exposed, so the two end slabs are small (1/16 of
+    // the records) and the rest is split into slabs of about 4 M records, whose move outlasts
+    // the copies of their neighbours.
+    std::vector<size_t> bounds{0};
+    if (n >= ((size_t)4 << 20)) {
+        const size_t edge = n / 16, rest = n - 2 * edge;
+        const size_t pieces = (rest + ((size_t)4 << 20) - 1) / ((size_t)4 << 20);
+        bounds.push_back(edge);
+        for (size_t q = 1; q <= pieces; q++) bounds.push_back(edge + rest * q / pieces);
+        bounds.push_back(n);
+    } else {
+        const size_t pieces = n >= ((size_t)2 << 20) ? 2 : 1;
+        for (size_t q = 1; q <= pieces; q++) bounds.push_back(n * q / pieces);
+    }
+    const int slabs = (int)bounds.size() - 1;
     std::vector<cudaEvent_t> up(slabs), done(slabs);
     for (int s = 0; s < slabs; s++) {
         cudaEventCreateWithFlags(&up[s], cudaEventDisableTiming);
@@ -1130,7 +1142,7 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
     }
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     for (int s = 0; s < slabs; s++) {
-        size_t off = s * per, cnt = std::min(per, n - std::min(n, off));
+        size_t off = bounds[s], cnt = bounds[s + 1] - bounds[s];
         if (cnt == 0) continue;
         CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dAos + off, particles + off,
                                       cnt * sizeof(wacomm_b200_particle), cudaMemcpyHostToDevice,
@@ -1138,7 +1150,7 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
         CUDA_TRY(ctx, cudaEventRecord(up[s], ctx->h2d));
     }
     for (int s = 0; s < slabs; s++) {
-        size_t off = s * per, cnt = std::min(per, n - std::min(n, off));
+        size_t off = bounds[s], cnt = bounds[s + 1] - bounds[s];
         if (cnt == 0) continue;
         CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, up[s], 0));
         ParticleSoA S = offset_soa(ctx->S.s, off);

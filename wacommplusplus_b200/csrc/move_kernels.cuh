@@ -108,7 +108,7 @@ struct LaunchShape<3> {
 };
 
 // FP32 step over the cell-column pair (step_fast.cuh); same state handling as move_soa_kernel.
-template <int SEM, int STORE, int SHAPE, bool LEAN>
+template <int SEM, int STORE, int SHAPE, int VARIANT>
 __global__ void __launch_bounds__(LaunchShape<SHAPE>::threads, LaunchShape<SHAPE>::minBlocks)
     move_fast_kernel(const wacomm_b200_config cfg,
                                                         const IntervalParams P,
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(LaunchShape<SHAPE>::threads, LaunchShape<SHAPE
         p.type = S.type[slot];
         p.side = S.side[slot];
         double elapsed = P.firstChunk ? P.elapsed0 : S.elapsed[slot];
-        steps = move_particle_fast<SEM, STORE, LEAN>(cfg, P, F, p, elapsed, L.err);
+        steps = move_particle_fast<SEM, STORE, VARIANT>(cfg, P, F, p, elapsed, L.err);
         S.k[slot] = p.k;
         S.j[slot] = p.j;
         S.i[slot] = p.i;
@@ -145,14 +145,14 @@ __global__ void __launch_bounds__(LaunchShape<SHAPE>::threads, LaunchShape<SHAPE
     if (L.conc && P.lastChunk) warp_count(L.conc, cell);
 }
 
-template <int SEM, int STORE, int SHAPE, bool LEAN>
+template <int SEM, int STORE, int SHAPE, int VARIANT>
 cudaError_t launch_move_fast(const wacomm_b200_config &cfg, const IntervalParams &P,
                              const FastView<STORE> &F, const ParticleSoA &S, const MoveLaunch &L,
                              cudaStream_t stream) {
     if (L.count <= 0) return cudaSuccess;
     constexpr int threads = LaunchShape<SHAPE>::threads;
     int blocks = (L.count + threads - 1) / threads;
-    move_fast_kernel<SEM, STORE, SHAPE, LEAN><<<blocks, threads, 0, stream>>>(cfg, P, F, S, L);
+    move_fast_kernel<SEM, STORE, SHAPE, VARIANT><<<blocks, threads, 0, stream>>>(cfg, P, F, S, L);
     return cudaGetLastError();
 }
 

@@ -110,9 +110,9 @@ __device__ __forceinline__ void current_cell(const CellView<STORE> &C, int kI, f
 // Leeway and Stokes velocity of a drifting object (the drift branch of advective_velocity) in FP32:
 // wind and Stokes interpolated from the environment pair, the leeway regression of the object's
 // catalogue row (computeLeeway, DriftModel.hpp:204-219) on the interpolated 10-m wind. The
-// position-dependent parts (calibration regions, wind-error fields) run in FP64 and only when the
-// run configures them.
-template <class View>
+// position-dependent parts (calibration regions, wind-error fields) and the coefficient ensemble
+// exist only in the FULL form, run in FP64 there and only when the run configures them.
+template <bool FULL, class View>
 __device__ __forceinline__ void drift_velocity(const wacomm_b200_config &cfg, const IntervalParams &P,
                                             const View &V, uint64_t id, int type, int side,
                                             int jI, float jF, int iI, float iF, float a,
@@ -133,7 +133,7 @@ __device__ __forceinline__ void drift_velocity(const wacomm_b200_config &cfg, co
     if (V.hasWindV)
         windV = at_f32(e1.wv0 * w1 + e2.wv0 * w2 + e3.wv0 * w3 + e4.wv0 * w4,
                        e1.wv1 * w1 + e2.wv1 * w2 + e3.wv1 * w3 + e4.wv1 * w4, a);
-    if (cfg.observationalCalibrationRegionCount > 0 || cfg.windErrorStdDev > 0) {
+    if (FULL && (cfg.observationalCalibrationRegionCount > 0 || cfg.windErrorStdDev > 0)) {
         const double jd = jF, id_ = iF;
         double longitude = V.lon(jI, iI) * (1.0 - id_) * (1.0 - jd) + V.lon(jI + 1, iI) * (1.0 - id_) * jd +
                            V.lon(jI + 1, iI + 1) * id_ * jd + V.lon(jI, iI + 1) * id_ * (1.0 - jd);
@@ -163,7 +163,7 @@ __device__ __forceinline__ void drift_velocity(const wacomm_b200_config &cfg, co
         }
     }
     float dn = 0.f, cn = 0.f;
-    if (cfg.leewayCoefficientEnsemble) {
+    if (FULL && cfg.leewayCoefficientEnsemble) {
         uint64_t ens = key_prefix(cfg.randomSeed, id, ENSEMBLE_INTERVAL, 0);
         double n0 = prefix_normal(ens, 0);
         dn = (float)n0;
@@ -194,9 +194,9 @@ __device__ __forceinline__ float signf_of(float a, float b) {
     return fabsf(a) * (float)((b > 0.f) - (b < 0.f));
 }
 
-// LEAN: the run parameters exclude diffusion, drifting objects and jibing (deterministic passive
-// tracking), so those branches are compiled out.
-template <int SEM, int STORE, bool LEAN>
+// VARIANT (VAR_*): the branches the run parameters can reach are compiled in, the rest out --
+// fewer registers and a smaller instruction footprint for the common runs.
+template <int SEM, int STORE, int VARIANT>
 __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalParams &P,
                                   const FastView<STORE> &F, ParticleState &p, double &elapsed,
                                   int *err) {
@@ -209,9 +209,11 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
     const float dirf = (float)direction;
     const float sv = (float)cfg.sv, shore = (float)cfg.shoreLimit;
     const bool midpoint = cfg.integrator == INTEGRATOR_MIDPOINT;
-    const bool diffuse = !LEAN && cfg.random && (direction > 0 || cfg.backwardDiffusion);
-    const bool drift = !LEAN && cfg.driftModel == 1 && p.type != 0;
-    const bool jibe = !LEAN && cfg.leewayJibeProbabilityHourly > 0 && p.type != 0;
+    constexpr bool canDiffuse = VARIANT != VAR_LEAN, canDrift = VARIANT >= VAR_DRIFT;
+    constexpr bool full = VARIANT == VAR_FULL;
+    const bool diffuse = canDiffuse && cfg.random && (direction > 0 || cfg.backwardDiffusion);
+    const bool drift = canDrift && cfg.driftModel == 1 && p.type != 0;
+    const bool jibe = full && cfg.leewayJibeProbabilityHourly > 0 && p.type != 0;
     if (drift && SEM == SEM_HOST && (p.type < 0 || p.type > 22)) atomicOr(err, ERR_DRIFT_OBJECT);
     bool lazy = false;
     int steps = 0;
@@ -273,7 +275,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         current_cell(C, kM, kF, jI, jF, iI, iF, sa, alpha, diffuse, uu, vv, ww, aa);
         if (drift) {
             float du, dv;
-            drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, jF, iI, iF, sa, elapsed,
+            drift_velocity<full>(cfg, P, V, p.id, p.type, p.side, jI, jF, iI, iF, sa, elapsed,
                            physicalTime, stepDt, du, dv);
             uu += du;
             vv += dv;
@@ -329,7 +331,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 current_cell(C, kMI, kMF, jMI, jMF, iMI, iMF, alpha, alpha, false, um, vm, wm, unused);
                 if (drift) {
                     float du, dv;
-                    drift_velocity(cfg, P, V, p.id, p.type, p.side, jMI, jMF, iMI, iMF, alpha,
+                    drift_velocity<full>(cfg, P, V, p.id, p.type, p.side, jMI, jMF, iMI, iMF, alpha,
                                    elapsed, physicalTime, stepDt, du, dv);
                     um += du;
                     vm += dv;
@@ -344,7 +346,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 current_cell(C, kM, kF, jI, jF, iI, iF, alpha, alpha, false, ue, ve, we, unused);
                 if (drift) {
                     float du, dv;
-                    drift_velocity(cfg, P, V, p.id, p.type, p.side, jI, jF, iI, iF, alpha, elapsed,
+                    drift_velocity<full>(cfg, P, V, p.id, p.type, p.side, jI, jF, iI, iF, alpha, elapsed,
                                    physicalTime, stepDt, du, dv);
                     ue += du;
                     ve += dv;
