@@ -115,7 +115,7 @@ typedef struct wacomm_b200_source {
 #define WACOMM_B200_STORAGE_BF16 2     /* forcing pair stored as bfloat16 (requires ARITH_FP32) */
 
 #define WACOMM_B200_RNG_REFERENCE 0    /* ordered-splitmix64-v2 draws, draw-for-draw with the reference */
-#define WACOMM_B200_RNG_PHILOX 1       /* Philox4x32-10 keyed on (particle id, interval, substep) */
+#define WACOMM_B200_RNG_PHILOX 1       /* Philox4x32-10 keyed on (particle id, interval, step time) */
 
 typedef struct wacomm_b200_options {
     int semantics;            /* WACOMM_B200_SEMANTICS_* */

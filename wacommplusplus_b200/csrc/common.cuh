@@ -131,19 +131,22 @@ __device__ __forceinline__ Philox4 philox4x32_10(Philox4 ctr, uint32_t k0, uint3
     return ctr;
 }
 
-// Three standard normals for (particle key, substep) in single precision.
-__device__ __forceinline__ void philox_normals3(uint64_t key, long long interval, uint64_t substep,
+// Three standard normals in single precision for (particle key, interval, step), the step named by
+// any 64-bit value unique within the interval (the bits of its elapsed time).
+__device__ __forceinline__ void philox_normals3(uint64_t key, long long interval, uint64_t step,
                                                 float &n0, float &n1, float &n2) {
-    Philox4 ctr{(uint32_t)substep, (uint32_t)(substep >> 32), (uint32_t)interval,
+    Philox4 ctr{(uint32_t)step, (uint32_t)(step >> 32), (uint32_t)interval,
                 (uint32_t)((uint64_t)interval >> 32)};
     Philox4 r = philox4x32_10(ctr, (uint32_t)key, (uint32_t)(key >> 32));
     const float scale = 2.3283064365386963e-10f;  // 2^-32; uniforms in (0,1]
     float u0 = ((float)r.x + 1.0f) * scale, u1 = (float)r.y * scale;
     float u2 = ((float)r.z + 1.0f) * scale, u3 = (float)r.w * scale;
     float rad0 = sqrtf(-2.0f * __logf(u0)), rad1 = sqrtf(-2.0f * __logf(u2));
+    // angles (2u - 1) pi in [-pi, pi), where the hardware sine and cosine are accurate to ~5e-7
+    const float pi = 3.14159265358979f;
     float s0, c0, s1, c1;
-    sincospif(2.0f * u1, &s0, &c0);
-    sincospif(2.0f * u3, &s1, &c1);
+    __sincosf(fmaf(2.0f, u1, -1.0f) * pi, &s0, &c0);
+    __sincosf(fmaf(2.0f, u3, -1.0f) * pi, &s1, &c1);
     n0 = rad0 * c0;
     n1 = rad0 * s0;
     n2 = rad1 * c1;

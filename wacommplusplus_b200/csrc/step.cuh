@@ -26,6 +26,7 @@ struct IntervalParams {
     double chunkEnd;          // substeps that start before this elapsed run in this launch
     int firstChunk, lastChunk;
     double kLower;            // -sW + 2
+    double invKLower;         // 1 / kLower (FP32 step: depth factor of the random walk)
     // Survival test without a per-step exp: health = exp(-age/tau0) is below survprob for
     // age >= ageKillHi, above it for age <= ageKillLo, and evaluated exactly in between;
     // exp(-age/tau0) > 0 is certain for age < ageUnder.
@@ -73,6 +74,7 @@ __host__ __device__ inline void make_interval(const wacomm_b200_config &cfg, con
         }
     }
     P.kLower = -sW + 2;
+    P.invKLower = 1.0 / P.kLower;
     P.chunkEnd = INFINITY;
     P.firstChunk = 1;
     P.lastChunk = 1;
@@ -466,7 +468,8 @@ __device__ int move_particle(const wacomm_b200_config &cfg, const IntervalParams
             double n0, n1, n2;
             if (P.rng == WACOMM_B200_RNG_PHILOX) {
                 float f0, f1, f2;
-                philox_normals3(keys.philoxKey, P.intervalKey, substep, f0, f1, f2);
+                philox_normals3(keys.philoxKey, P.intervalKey,
+                                (uint64_t)__double_as_longlong(elapsed), f0, f1, f2);
                 n0 = f0;
                 n1 = f1;
                 n2 = f2;

@@ -280,18 +280,19 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
             uu += du;
             vv += dv;
         }
-        uint64_t substep = 0, stepKey = 0;
-        if (diffuse || jibe) {
-            substep = (uint64_t)floor(elapsed / cfg.dti);
-            stepKey = fold(prefix, substep);
-        }
+        // the substep index keys the reference draws and the jibe draw; Philox streams are keyed
+        // on the step's elapsed time instead (unique per step, no division)
+        uint64_t stepKey = 0;
+        const bool philox = P.rng == WACOMM_B200_RNG_PHILOX;
+        if ((diffuse && !philox) || jibe) stepKey = fold(prefix, (uint64_t)floor(elapsed / cfg.dti));
         float rx = 0.f, ry = 0.f, rz = 0.f;
         if (diffuse) {
-            float sigmaDepth = (float)(cfg.sigma * (1 - p.k / kLower));
+            float sigmaDepth = (float)(cfg.sigma * (1 - p.k * P.invKLower));
             float scale = sqrtf(dt / (float)cfg.dti);
             float n0, n1, n2;
-            if (P.rng == WACOMM_B200_RNG_PHILOX) {
-                philox_normals3(philoxKey, P.intervalKey, substep, n0, n1, n2);
+            if (philox) {
+                philox_normals3(philoxKey, P.intervalKey, (uint64_t)__double_as_longlong(elapsed),
+                                n0, n1, n2);
             } else {
                 n0 = (float)prefix_normal(stepKey, 0);
                 n1 = (float)prefix_normal(stepKey, 1);
