@@ -82,7 +82,7 @@ struct alignas(16) CellCorners {
     float wU[2][4], wL[2][4];  // w levels kI and kI-1
     float zeta[2][4];
     float h[4];
-    double xdist, ydist, depth;  // cell metric, depthIntervals(kI)
+    double invXdist, invYdist, depth;  // reciprocal cell metric, depthIntervals(kI)
     float gate, pad;
 };
 static_assert(sizeof(CellCorners) == 208, "corner record layout");
@@ -282,8 +282,8 @@ __global__ void __launch_bounds__(128, 1) surrogate_cell_kernel(const CellArgs a
                 c.h[q] = (float)a.h[corner[q]];
             }
             const double2 m = a.metric[c00];
-            c.xdist = m.x;
-            c.ydist = m.y;
+            c.invXdist = 1.0 / m.x;
+            c.invYdist = 1.0 / m.y;
             c.depth = a.depthIntervals[kI + a.sW - 2];
             c.gate = fminf(sqrtf(gsum / 256.f) / GATE_SIGMA, 1.f);
             c.pad = 0.f;
@@ -311,6 +311,7 @@ __global__ void __launch_bounds__(128, 1) surrogate_cell_kernel(const CellArgs a
 struct StepArgs {
     int eta, xi, sW, sRho;
     double start, length, dti, tau0, survprob, sv;
+    double invLength, invDti, invTau0;  // reciprocals: the row epilogue multiplies
     int upper, lower, horizontal;
     int fallbackAll;  // run parameters outside the surrogate: every active particle falls back
     int drift;        // driftModel == 1: drifting objects fall back
@@ -336,16 +337,20 @@ struct RowTag {
     int cl;
 };
 
-// Bilinear value from the four corners (j,i), (j+1,i), (j+1,i+1), (j,i+1) held in x, y, z, w.
-__device__ __forceinline__ double bil4(const float4 c, double jF, double iF) {
-    return (double)c.x * (1 - iF) * (1 - jF) + (double)c.y * (1 - iF) * jF + (double)c.z * iF * jF +
-           (double)c.w * iF * (1 - jF);
+// Bilinear value from the four corners (j,i), (j+1,i), (j+1,i+1), (j,i+1) held in x, y, z, w, as
+// nested linear blends: equal corners give their value exactly.
+__device__ __forceinline__ float bil4(const float4 c, float jF, float iF) {
+    const float lo = fmaf(c.w - c.x, iF, c.x), hi = fmaf(c.z - c.y, iF, c.y);
+    return fmaf(hi - lo, jF, lo);
 }
 
-// End of nSub equal substeps of disp/nSub along one axis of [0, maximum): a particle leaving the
+__device__ __forceinline__ float blend(float a, float b, float t) { return fmaf(b - a, t, a); }
+
+// End of nSub equal substeps d = disp/nSub along one axis of [0, maximum): a particle leaving the
 // domain at substep m under repeated reflectDomain alternates its overshoot e and d - e.
-__device__ double pinned_axis(double x0, double disp, double nSub, double maximum, double &m) {
-    const double d = disp / nSub, end = x0 + disp, big = nSub + 1;
+__device__ double pinned_axis(double x0, double disp, double d, double nSub, double maximum,
+                              double &m) {
+    const double end = x0 + disp, big = nSub + 1;
     const bool up = end >= maximum, down = end < 0;
     if (!up && !down) {
         m = big;
@@ -655,36 +660,38 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                 const double ptime = S.time[slot], page = S.age[slot], phealth = S.health[slot];
                 if (status == ROW_RUN) {
                     // the corner record: u[0],u[1],v[0],v[1],wU[0],wU[1],wL[0],wL[1],zeta[0],zeta[1],h
-                    // as float4s, then {xdist, ydist}, then {depth, gate}
+                    // as float4s, then {1/xdist, 1/ydist}, then {depth, gate}
                     const float4 *cf = reinterpret_cast<const float4 *>(a.corners + tag.cl);
                     const float4 cu0 = __ldg(cf + 0), cu1 = __ldg(cf + 1), cv0 = __ldg(cf + 2),
                                  cv1 = __ldg(cf + 3), cwU0 = __ldg(cf + 4), cwU1 = __ldg(cf + 5),
                                  cwL0 = __ldg(cf + 6), cwL1 = __ldg(cf + 7), cz0 = __ldg(cf + 8),
                                  cz1 = __ldg(cf + 9), ch = __ldg(cf + 10);
-                    const double2 met = __ldg(reinterpret_cast<const double2 *>(cf + 11));
+                    const double2 inv = __ldg(reinterpret_cast<const double2 *>(cf + 11));
                     const double depth = __ldg(reinterpret_cast<const double *>(cf + 12));
                     const float gate = __ldg(reinterpret_cast<const float *>(cf + 12) + 2);
                     const double y0 = (double)((o0 + red[r * 3 + 0] + b4s[0]) * gate);
                     const double y1 = (double)((o1 + red[r * 3 + 1] + b4s[1]) * gate);
                     const double y2 = (double)((o2 + red[r * 3 + 2] + b4s[2]) * gate);
                     const double fj = floor(pj), fi = floor(pi), ck = ceil(pk);
-                    const double jF = pj - fj, iF = pi - fi, kF = ck - pk;
-                    const double da0 = ptime > T0 ? (ptime - T0) / a.length : 0.0;
+                    const float jF = (float)(pj - fj), iF = (float)(pi - fi), kF = (float)(ck - pk);
+                    const double da0 = ptime > T0 ? (ptime - T0) * a.invLength : 0.0;
                     const double amid = 0.5 * (da0 + 1.0), trem = (1.0 - da0) * a.length;
-                    const double nSub = fmax(1.0, ceil(trem / a.dti - 1e-9));
-                    const double ub = (1 - amid) * bil4(cu0, jF, iF) + amid * bil4(cu1, jF, iF);
-                    const double vb = (1 - amid) * bil4(cv0, jF, iF) + amid * bil4(cv1, jF, iF);
-                    const double wb = (1 - amid) * ((1 - kF) * bil4(cwU0, jF, iF) + kF * bil4(cwL0, jF, iF)) +
-                                      amid * ((1 - kF) * bil4(cwU1, jF, iF) + kF * bil4(cwL1, jF, iF));
-                    const double hc = bil4(ch, jF, iF) + (1 - amid) * bil4(cz0, jF, iF) +
-                                      amid * bil4(cz1, jF, iF);
-                    const double zdist = hc * depth;
-                    const double dI = (ub * trem + OUT_H * y0) / met.x;
-                    const double dJ = (vb * trem + OUT_H * y1) / met.y;
-                    const double dK = ((wb + a.sv) * trem + OUT_V * y2) / zdist;
+                    const double nSub = fmax(1.0, ceil(trem * a.invDti - 1e-9));
+                    const float am = (float)amid;
+                    const float ub = blend(bil4(cu0, jF, iF), bil4(cu1, jF, iF), am);
+                    const float vb = blend(bil4(cv0, jF, iF), bil4(cv1, jF, iF), am);
+                    const float wb = blend(blend(bil4(cwU0, jF, iF), bil4(cwL0, jF, iF), kF),
+                                           blend(bil4(cwU1, jF, iF), bil4(cwL1, jF, iF), kF), am);
+                    const float hc = bil4(ch, jF, iF) + blend(bil4(cz0, jF, iF), bil4(cz1, jF, iF), am);
+                    const float zdist = hc * (float)depth;
+                    const double dI = ((double)ub * trem + OUT_H * y0) * inv.x;
+                    const double dJ = ((double)vb * trem + OUT_H * y1) * inv.y;
+                    const double dK = (double)(((wb + (float)a.sv) * (float)trem + OUT_V * (float)y2) *
+                                               __frcp_rn(zdist));
+                    const double invSub = 1.0 / nSub;
                     double mj, mi;
-                    double jn = pinned_axis(pj, dJ, nSub, (double)(a.eta - 1), mj);
-                    double in = pinned_axis(pi, dI, nSub, (double)(a.xi - 1), mi);
+                    double jn = pinned_axis(pj, dJ, dJ * invSub, nSub, (double)(a.eta - 1), mj);
+                    double in = pinned_axis(pi, dI, dI * invSub, nSub, (double)(a.xi - 1), mi);
                     const double m = fmin(mj, mi);
                     const bool crossed = m <= nSub;
                     bool dead = false;
@@ -718,7 +725,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                         status = ROW_FALLBACK;
                     } else {
                         const double age = page + trem;
-                        const double health = exp(-age / a.tau0);
+                        const double health = exp(-age * a.invTau0);
                         dead = dead || health < a.survprob;
                         S.j[slot] = jn;
                         S.i[slot] = in;
@@ -917,6 +924,9 @@ cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const M
     a.length = s.length;
     a.dti = s.cfg.dti;
     a.tau0 = s.cfg.tau0;
+    a.invLength = s.length == 0 ? 0.0 : 1.0 / s.length;
+    a.invDti = 1.0 / s.cfg.dti;
+    a.invTau0 = 1.0 / s.cfg.tau0;
     a.survprob = s.cfg.survprob;
     a.sv = s.cfg.sv;
     a.upper = s.cfg.upperClosure;
