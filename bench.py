@@ -349,6 +349,7 @@ def run_batched(args):
     peak, peak_kind = measured_peaks("hbm_gbs", 6650.0)
     mean_ms = statistics.mean(device_ms)
     achieved = per_step * B_ALG / (mean_ms / 1000.0) / 1e9
+    traffic = profile_traffic("move_kernel_batched.md")
     cpu = None
     if not args.no_cpu:
         # the reference CPU step (leeway objects, wind and Stokes on the ocean grid) on a sample
@@ -382,9 +383,11 @@ def run_batched(args):
                    "launch_shape": shape, "autotune_ms": tune_ms, "regrid_s": t_regrid,
                    "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": None if traffic is None else traffic * per_step,
                      "note": f"B_alg 118 B per particle-step over the whole graph (sorts and "
-                             f"packing included), {peak_kind} peak"},
+                             f"packing included), {peak_kind} peak; traffic per run from the "
+                             f"ncu summary's bytes per particle-step"},
         "cpu_baseline": cpu,
         "e2e": {"value": steps_total / e2e_s, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": n * PARTICLE_DTYPE.itemsize,
