@@ -123,3 +123,43 @@ def test_autotune_changes_only_the_launch_shape(cuda_device, setting):
         assert before[f].tobytes() == after[f].tobytes(), f
     assert np.array_equal(conc, e.concentration())
     e.close()
+
+
+def test_graph_of_chunked_launches_and_full_drift_form(cuda_device, setting):
+    """Intervals split into launches of 40 substeps, with the wind-error field and the leeway
+    coefficient ensemble on (the full form of the FP32 step): captured equals eager."""
+    win, env, _ = setting
+    cfg = default_config(random=True, randomSeed=5, driftModel=1, windErrorStdDev=1.0,
+                         windErrorComponentCorrelation=0.3, leewayCoefficientEnsemble=True,
+                         leewayResidualCorrelation=-0.35)
+    parts = batch(20000, 6, win)
+    ref = engine(win, env, cfg, parts)
+    ref.set_options(substeps_per_launch=40)
+    ref_steps = eager(ref)
+    g = engine(win, env, cfg, parts)
+    g.set_options(substeps_per_launch=40)
+    g.graph_capture(0, INTERVALS)
+    g.graph_launch()
+    g.synchronize()
+    assert g.stats()["particle_steps"] == ref_steps > 0
+    same(g, ref)
+    ref.close()
+    g.close()
+
+
+def test_autotune_block_size_under_reference_arithmetic(cuda_device, setting):
+    win, env, cfg = setting
+    e = Engine(0, arithmetic="reference")
+    e.set_config(cfg)
+    e.load_window(win)
+    e.concentration_reset(win.T)
+    e.set_particles(batch(20000, 7, win))
+    before, conc = e.get_particles(), e.concentration()
+    size, ms = e.autotune(1)
+    assert size in (64, 128, 192, 256) and ms > 0
+    assert e.options().block_size == size
+    after = e.get_particles()
+    for f in before.dtype.names:
+        assert before[f].tobytes() == after[f].tobytes(), f
+    assert np.array_equal(conc, e.concentration())
+    e.close()

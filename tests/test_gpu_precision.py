@@ -133,3 +133,37 @@ def test_fp32_step_on_reference_fixture_cases(cuda_device, case_name):
           f"max {err.max():.3g} m flips {flips}")
     assert flips <= max(2, len(got) // 100)
     assert err.mean() <= 0.1 and np.percentile(err, 99) <= 1.0
+
+
+@pytest.mark.parametrize("random", [False, True])
+def test_plain_drift_form_against_fp64_oracle(cuda_device, random):
+    """The plain-drift form of the FP32 step (leeway regression in FP32, wind and Stokes from
+    the environment pair, with and without the random walk under the reference draws) against
+    the FP64 oracle: every catalogue object on both sides, six hours over the analytic grid with
+    wind and Stokes fields on the rho nodes."""
+    win = syn.config1_window(n_frames=7)
+    env = syn.environment(win.times[0], 6, wind_n=60)
+    with Engine(cuda_device, arithmetic="fp32") as e:
+        e.load_window(win)
+        e.set_geo_grid(win.lon, win.lat, win.sWValues)
+        e.regrid_environment("wind", "curvilinear", *env["wind"])
+        e.regrid_environment("stokes", "geographic", *env["stokes"])
+        wind = [e.environment("wind", t) for t in range(win.T)]
+        stokes = [e.environment("stokes", t) for t in range(win.T)]
+    win.windU10 = np.ascontiguousarray([w[0] for w in wind])
+    win.windV10 = np.ascontiguousarray([w[1] for w in wind])
+    win.stokesU = np.ascontiguousarray([s[0] for s in stokes])
+    win.stokesV = np.ascontiguousarray([s[1] for s in stokes])
+    p = syn.uniform_particles(8192, win.eta, win.xi, seed=12)
+    p["driftObjectType"] = 1 + np.arange(len(p)) % 22
+    p["driftSide"] = np.where(np.arange(len(p)) % 3 == 0, 1, -1)
+    cfg = default_config(random=random, driftModel=1, horizontalClosure=1, randomSeed=77)
+    want = _oracle(win, cfg, p, range(6))
+    with Engine(cuda_device, arithmetic="fp32") as e:
+        got = _run(e, win, cfg, p, range(6))
+    both = (got["health"] > 0) & (want["health"] > 0)
+    err = great_circle_m(win.lon, win.lat, got[both], want[both])
+    print(f"plain drift random={random}: mean {err.mean():.3g} m p99 "
+          f"{np.percentile(err, 99):.3g} m max {err.max():.3g} m")
+    assert np.array_equal(got["health"] > 0, want["health"] > 0)
+    assert err.mean() <= 0.05 and np.percentile(err, 99) <= 0.5
