@@ -53,29 +53,26 @@ __device__ __forceinline__ float blend(const QuadPair &q, const Weights8 &w) {
     return x + y;
 }
 
-// Bilinear h, zeta@t0 and zeta@t1 at a fractional position of a cell (FP32); the water column
-// height at time weight a is h + at_f32(z0, z1, a).
+// Bilinear h + zeta@t0 and zeta@t1 - zeta@t0 at a fractional position of a cell (FP32); the water
+// column height at time weight a is s + a d.
 struct SurfaceSums {
-    float h, z0, z1;
-    __device__ __forceinline__ float height(float a) const { return h + at_f32(z0, z1, a); }
+    float s, d;
+    __device__ __forceinline__ float height(float a) const { return fmaf(a, d, s); }
 };
 
 template <int STORE>
 __device__ __forceinline__ SurfaceSums surface_sums(const CellView<STORE> &C, int jI, int iI,
                                                     float jF, float iF) {
-    CellSurface s = C.surf(jI, iI);
+    CellSurface c = C.surf(jI, iI);
     float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
-    float h = s.h.x * w1, z0 = s.z0.x * w1, z1 = s.z1.x * w1;
-    h = fmaf(s.h.y, w2, h);
-    z0 = fmaf(s.z0.y, w2, z0);
-    z1 = fmaf(s.z1.y, w2, z1);
-    h = fmaf(s.h.z, w3, h);
-    z0 = fmaf(s.z0.z, w3, z0);
-    z1 = fmaf(s.z1.z, w3, z1);
-    h = fmaf(s.h.w, w4, h);
-    z0 = fmaf(s.z0.w, w4, z0);
-    z1 = fmaf(s.z1.w, w4, z1);
-    return SurfaceSums{h, z0, z1};
+    float s = c.s0.x * w1, d = c.dz.x * w1;
+    s = fmaf(c.s0.y, w2, s);
+    d = fmaf(c.dz.y, w2, d);
+    s = fmaf(c.s0.z, w3, s);
+    d = fmaf(c.dz.z, w3, d);
+    s = fmaf(c.s0.w, w4, s);
+    d = fmaf(c.dz.w, w4, d);
+    return SurfaceSums{s, d};
 }
 
 // Water column height h + zeta at a fractional position of a cell (FP32).
@@ -226,7 +223,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
     const uint64_t philoxKey = p.id ^ mix64(cfg.randomSeed);
     const double stop = P.chunkEnd < length ? P.chunkEnd : length;
     // surface sums at the previous step's destination, valid while the particle still sits there
-    SurfaceSums carried{0.f, 0.f, 0.f};
+    SurfaceSums carried{0.f, 0.f};
     bool haveCarried = false;
 
     while (elapsed < stop) {

@@ -210,11 +210,12 @@ __global__ void pack_cell_surface_kernel(int eta, int xi, FrameDevice f0, FrameD
         CellSurface s;
         if (j + 1 < eta && i + 1 < xi) {
             size_t c1 = cell, c2 = cell + xi, c3 = cell + xi + 1, c4 = cell + 1;
-            s.h = make_float4((float)h[c1], (float)h[c2], (float)h[c3], (float)h[c4]);
-            s.z0 = make_float4(f0.zeta[c1], f0.zeta[c2], f0.zeta[c3], f0.zeta[c4]);
-            s.z1 = make_float4(f1.zeta[c1], f1.zeta[c2], f1.zeta[c3], f1.zeta[c4]);
+            s.s0 = make_float4((float)h[c1] + f0.zeta[c1], (float)h[c2] + f0.zeta[c2],
+                               (float)h[c3] + f0.zeta[c3], (float)h[c4] + f0.zeta[c4]);
+            s.dz = make_float4(f1.zeta[c1] - f0.zeta[c1], f1.zeta[c2] - f0.zeta[c2],
+                               f1.zeta[c3] - f0.zeta[c3], f1.zeta[c4] - f0.zeta[c4]);
         } else {
-            s.h = s.z0 = s.z1 = make_float4(0, 0, 0, 0);
+            s.s0 = s.dz = make_float4(0, 0, 0, 0);
         }
         out[cell] = s;
     }

@@ -252,8 +252,8 @@ __device__ __forceinline__ void load_first<STORE_BF16>(const CellQuad<STORE_BF16
     a.t1 = quad_bf(x.z, x.w);
 }
 
-struct CellSurface {  // FP32: h, zeta@t0, zeta@t1 at the 4 corners
-    float4 h, z0, z1;
+struct CellSurface {  // FP32 at the 4 corners: h + zeta@t0, and zeta@t1 - zeta@t0
+    float4 s0, dz;
 };
 
 template <int STORE>
@@ -284,7 +284,7 @@ struct CellView {
     }
     __device__ __forceinline__ CellSurface surf(int j, int i) const {
         const float4 *q = reinterpret_cast<const float4 *>(surface + ((size_t)j * xi + i));
-        return CellSurface{__ldg(q), __ldg(q + 1), __ldg(q + 2)};
+        return CellSurface{__ldg(q), __ldg(q + 1)};
     }
 };
 
