@@ -82,12 +82,29 @@ __device__ __forceinline__ float column_height(const CellView<STORE> &C, int jI,
     return surface_sums(C, jI, iI, jF, iF).height(a);
 }
 
-// Current (u, v, w) and, when wanted, AKT at a fractional position: one stencil read.
-template <int STORE>
+// The velocity stencil of one cell and level at one time: u, v and the two w levels per corner.
+struct StencilAt {
+    Quad u, v, wUp, wLo;
+};
+
+__device__ __forceinline__ Quad at_time(const QuadPair &q, float a) {
+    return Quad{fmaf(a, q.t1.c1 - q.t0.c1, q.t0.c1), fmaf(a, q.t1.c2 - q.t0.c2, q.t0.c2),
+                fmaf(a, q.t1.c3 - q.t0.c3, q.t0.c3), fmaf(a, q.t1.c4 - q.t0.c4, q.t0.c4)};
+}
+
+__device__ __forceinline__ float bilinear4(const Quad &q, float w1, float w2, float w3, float w4) {
+    return fmaf(q.c4, w4, fmaf(q.c3, w3, fmaf(q.c2, w2, q.c1 * w1)));
+}
+
+// Current (u, v, w) and, when wanted, AKT at a fractional position: one stencil read. With `keep`
+// the stencil's corners blended to time weight aKeep are returned as well, for a second
+// evaluation in the same cell and level without a second read.
+template <int STORE, bool KEEP = false>
 __device__ __forceinline__ void current_cell(const CellView<STORE> &C, int kI, float kF, int jI,
                                              float jF, int iI, float iF, float a, float aAkt,
                                              bool wantAkt, float &uu, float &vv, float &ww,
-                                             float &aa) {
+                                             float &aa, float aKeep = 0.f,
+                                             StencilAt *keep = nullptr) {
     QuadPair u, v, wUp, aUp, wLo, aLo;
     if (wantAkt) C.stencil(kI, jI, iI, u, v, wUp, aUp, wLo, aLo);
     else C.stencil_w(kI, jI, iI, u, v, wUp, wLo);
@@ -101,6 +118,23 @@ __device__ __forceinline__ void current_cell(const CellView<STORE> &C, int kI, f
         float au = blend(aUp, wa), al = blend(aLo, wa);
         aa = fmaf(al - au, kF, au);
     }
+    if (KEEP) {
+        keep->u = at_time(u, aKeep);
+        keep->v = at_time(v, aKeep);
+        keep->wUp = at_time(wUp, aKeep);
+        keep->wLo = at_time(wLo, aKeep);
+    }
+}
+
+// Current (u, v, w) from a kept stencil at a fractional position of its cell and level.
+__device__ __forceinline__ void current_kept(const StencilAt &k, float kF, float jF, float iF,
+                                             float &uu, float &vv, float &ww) {
+    const float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF,
+                w4 = iF * (1.f - jF);
+    uu = bilinear4(k.u, w1, w2, w3, w4);
+    vv = bilinear4(k.v, w1, w2, w3, w4);
+    const float up = bilinear4(k.wUp, w1, w2, w3, w4), lo = bilinear4(k.wLo, w1, w2, w3, w4);
+    ww = fmaf(lo - up, kF, up);
 }
 
 
@@ -269,7 +303,14 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         const int kM = mem_level(kI, sW);
         const float sa = midpoint ? alphaStart : alpha;
         float uu, vv, ww, aa = 0.f;
-        current_cell(C, kM, kF, jI, jF, iI, iF, sa, alpha, diffuse, uu, vv, ww, aa);
+        // the start stencil at the mid-stage time (midpoint rule; the lean form has the registers)
+        constexpr bool keepStencil = VARIANT == VAR_LEAN;
+        StencilAt kept;
+        if (keepStencil && midpoint)
+            current_cell<STORE, true>(C, kM, kF, jI, jF, iI, iF, sa, alpha, diffuse, uu, vv, ww, aa,
+                                      alpha, &kept);
+        else
+            current_cell(C, kM, kF, jI, jF, iI, iF, sa, alpha, diffuse, uu, vv, ww, aa);
         if (drift) {
             float du, dv;
             drift_velocity<full>(cfg, P, V, p.id, p.type, p.side, jI, jF, iI, iF, sa, elapsed,
@@ -326,7 +367,11 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 int kMI = mem_level(to_index<SEM>(kmc), sW);
                 float kMF = (float)(kmc - kMid);
                 float um, vm, wm, unused;
-                current_cell(C, kMI, kMF, jMI, jMF, iMI, iMF, alpha, alpha, false, um, vm, wm, unused);
+                if (keepStencil && kMI == kM && jMI == jI && iMI == iI)
+                    current_kept(kept, kMF, jMF, iMF, um, vm, wm);
+                else
+                    current_cell(C, kMI, kMF, jMI, jMF, iMI, iMF, alpha, alpha, false, um, vm, wm,
+                                 unused);
                 if (drift) {
                     float du, dv;
                     drift_velocity<full>(cfg, P, V, p.id, p.type, p.side, jMI, jMF, iMI, iMF, alpha,
@@ -341,7 +386,8 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 detZ = dirf * (sv + wm) * dt * zdist * __frcp_rn(zdistMid);
             } else {
                 float ue, ve, we, unused;
-                current_cell(C, kM, kF, jI, jF, iI, iF, alpha, alpha, false, ue, ve, we, unused);
+                if (keepStencil) current_kept(kept, kF, jF, iF, ue, ve, we);
+                else current_cell(C, kM, kF, jI, jF, iI, iF, alpha, alpha, false, ue, ve, we, unused);
                 if (drift) {
                     float du, dv;
                     drift_velocity<full>(cfg, P, V, p.id, p.type, p.side, jI, jF, iI, iF, alpha, elapsed,
