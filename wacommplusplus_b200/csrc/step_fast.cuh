@@ -60,10 +60,7 @@ struct SurfaceSums {
     __device__ __forceinline__ float height(float a) const { return fmaf(a, d, s); }
 };
 
-template <int STORE>
-__device__ __forceinline__ SurfaceSums surface_sums(const CellView<STORE> &C, int jI, int iI,
-                                                    float jF, float iF) {
-    CellSurface c = C.surf(jI, iI);
+__device__ __forceinline__ SurfaceSums surface_from(const CellSurface &c, float jF, float iF) {
     float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
     float s = c.s0.x * w1, d = c.dz.x * w1;
     s = fmaf(c.s0.y, w2, s);
@@ -73,6 +70,12 @@ __device__ __forceinline__ SurfaceSums surface_sums(const CellView<STORE> &C, in
     s = fmaf(c.s0.w, w4, s);
     d = fmaf(c.dz.w, w4, d);
     return SurfaceSums{s, d};
+}
+
+template <int STORE>
+__device__ __forceinline__ SurfaceSums surface_sums(const CellView<STORE> &C, int jI, int iI,
+                                                    float jF, float iF) {
+    return surface_from(C.surf(jI, iI), jF, iF);
 }
 
 // Water column height h + zeta at a fractional position of a cell (FP32).
@@ -257,6 +260,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
     const uint64_t philoxKey = p.id ^ mix64(cfg.randomSeed);
     const double stop = P.chunkEnd < length ? P.chunkEnd : length;
     // surface sums at the previous step's destination, valid while the particle still sits there
+    constexpr bool keepStencil = VARIANT == VAR_LEAN;
     SurfaceSums carried{0.f, 0.f};
     bool haveCarried = false;
 
@@ -304,7 +308,6 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         const float sa = midpoint ? alphaStart : alpha;
         float uu, vv, ww, aa = 0.f;
         // the start stencil at the mid-stage time (midpoint rule; the lean form has the registers)
-        constexpr bool keepStencil = VARIANT == VAR_LEAN;
         StencilAt kept;
         if (keepStencil && midpoint)
             current_cell<STORE, true>(C, kM, kF, jI, jF, iI, iF, sa, alpha, diffuse, uu, vv, ww, aa,
@@ -341,7 +344,8 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
             rz = sigmaDepth * n2 * aa * (float)cfg.crid * scale;
         }
         const float2 inv = __ldg(F.X.invMetric + (size_t)jI * xi + iI);
-        const float zdist = hc * __ldg(F.X.depthIntervals + (kM + sW - 2));
+        const float depthHere = __ldg(F.X.depthIntervals + (kM + sW - 2));
+        const float zdist = hc * depthHere;
         const float rzdist = __frcp_rn(zdist);
         // index increments (i, j) and the vertical leap in metres
         float dI, dJ, zleap;
@@ -379,8 +383,10 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                     um += du;
                     vm += dv;
                 }
-                const float2 im = __ldg(F.X.invMetric + (size_t)jMI * xi + iMI);
-                float zdistMid = hcMid * __ldg(F.X.depthIntervals + (kMI + sW - 2));
+                const bool sameCell = jMI == jI && iMI == iI;
+                const float2 im = sameCell ? inv : __ldg(F.X.invMetric + (size_t)jMI * xi + iMI);
+                float zdistMid =
+                    hcMid * (kMI == kM ? depthHere : __ldg(F.X.depthIntervals + (kMI + sW - 2)));
                 dI = dirf * um * dt * im.x;
                 dJ = dirf * vm * dt * im.y;
                 detZ = dirf * (sv + wm) * dt * zdist * __frcp_rn(zdistMid);
@@ -417,7 +423,8 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         double fjd = floor(jdet), fid = floor(idet);
         int jdetI = to_index<SEM>(fjd), idetI = to_index<SEM>(fid);
         if (valid_cell(jdetI, idetI, eta, xi)) {
-            const SurfaceSums there = surface_sums(C, jdetI, idetI, (float)(jdet - fjd), (float)(idet - fid));
+            const SurfaceSums there =
+                surface_sums(C, jdetI, idetI, (float)(jdet - fjd), (float)(idet - fid));
             float hcdet = there.height(alpha);
             // the next step starts here unless a closure moves the particle
             carried = there;
