@@ -238,8 +238,8 @@ int wacomm_b200_move_interval(wacomm_b200_context *ctx, int time_index);
  * of the capture: new record values (upload_frame into existing slots, set_particles with the
  * same count, a new batch of scenarios) are picked up by the next launch, while any change of
  * those is refused at launch with WACOMM_B200_ERR_STATE (capture again). Not with the surrogate
- * option (its fallback list returns to the host). last_interval_stats after a launch reports
- * the whole run (device ms, particle-steps). No reference counterpart. */
+ * option (its per-interval timing and statistics are kept per call). last_interval_stats after a
+ * launch reports the whole run (device ms, particle-steps). No reference counterpart. */
 int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, int n_intervals);
 int wacomm_b200_graph_launch(wacomm_b200_context *ctx);
 int wacomm_b200_graph_release(wacomm_b200_context *ctx);
@@ -340,6 +340,11 @@ int wacomm_b200_concentration_get_float(wacomm_b200_context *ctx, float *out, si
 int wacomm_b200_concentration_device(wacomm_b200_context *ctx, void **device_ptr, size_t *cells);
 
 int wacomm_b200_synchronize(wacomm_b200_context *ctx);
+
+/* Particle-steps of every interval (and captured run) since the context was created or the last
+ * reset, counted by the kernels and summed on the device, so a caller can enqueue many intervals
+ * without waiting between them and read the count once. Waits for the context's stream. */
+int wacomm_b200_particle_steps_total(wacomm_b200_context *ctx, int reset, double *total);
 
 /* Statistics of the last move_interval: device milliseconds of all its kernels (CUDA events on
  * the context stream around pack, sort and move), of the move kernel launches alone, how many

@@ -73,6 +73,9 @@ def test_graph_equals_eager_and_relaunches_on_a_new_batch(cuda_device, setting):
     g.graph_launch()
     g.synchronize()
     assert g.stats()["particle_steps"] == ref_steps > 0
+    # the device-side running totals agree with the per-interval counts
+    assert g.steps_total() == ref_steps and ref.steps_total(reset=True) == ref_steps
+    assert ref.steps_total() == 0
     same(g, ref)
     # a new batch of the same size through the same graph
     ref.set_particles(second)

@@ -71,6 +71,7 @@ SIGNATURES = {
     "wacomm_b200_get_frame": (_i, [_vp, _i] + [_fp] * 5),
     "wacomm_b200_set_roms_grid": (_i, [_vp, _dp, _dp, _dp]),
     "wacomm_b200_upload_roms_frame": (_i, [_vp, _i] + [_fp] * 9),
+    "wacomm_b200_particle_steps_total": (_i, [_vp, _i, _dp]),
     "wacomm_b200_graph_capture": (_i, [_vp, _i, _i]),
     "wacomm_b200_graph_launch": (_i, [_vp]),
     "wacomm_b200_graph_release": (_i, [_vp]),

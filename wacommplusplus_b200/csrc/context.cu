@@ -111,7 +111,6 @@ struct wacomm_b200_context {
     unsigned long long *dSurrCounts = nullptr;  // [0]: fallback count (low 32 bits), [1]: run count
     cudaEvent_t evCell0 = nullptr, evCell1 = nullptr, evStep0 = nullptr, evStep1 = nullptr;
     bool surrTimed = false;
-    size_t lastRun = 0, lastFallback = 0;
     int smCount = 148;
 
     double *dGeoLon = nullptr, *dGeoLat = nullptr, *dSWValues = nullptr;  // kji2deplatlon grid
@@ -135,7 +134,7 @@ struct wacomm_b200_context {
     EnvField env[2];
     size_t geoOutCap = 0;
 
-    unsigned long long *dSteps = nullptr;
+    unsigned long long *dSteps = nullptr;  // [0]: the last interval or run, [1]: running total
     int *dErr = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evMove0 = nullptr, evMove1 = nullptr;
     cudaEvent_t evComputeMark = nullptr;  // orders asynchronous frame copies after enqueued kernels
@@ -649,8 +648,6 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
                                   ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     const size_t nFallback = (size_t)(counts[0] & 0xffffffffull);
-    ctx->lastFallback = nFallback;
-    ctx->lastRun = (size_t)counts[1];
     ctx->surrTimed = true;
     if (nFallback) {
         IntervalParams Q = P;
@@ -734,7 +731,8 @@ int wacomm_b200_context_create(int device, wacomm_b200_context **out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->evComputeMark, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->evMove0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->evMove1);
-    if (e == cudaSuccess) e = cudaMalloc(&ctx->dSteps, sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->dSteps, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(ctx->dSteps, 0, 2 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&ctx->dErr, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&ctx->dCount, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(ctx->dErr, 0, sizeof(int));
@@ -1099,6 +1097,7 @@ int wacomm_b200_move_interval(wacomm_b200_context *ctx, int time_index) {
     int rc = enqueue_interval(ctx, time_index, launches);
     if (rc) return rc;
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    CUDA_TRY(ctx, accumulate_steps(ctx->dSteps, ctx->dSteps + 1, ctx->stream));
     ctx->lastLaunches = launches;
     return WACOMM_B200_OK;
 }
@@ -1169,6 +1168,7 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
                                       ctx->d2h));
     }
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    CUDA_TRY(ctx, accumulate_steps(ctx->dSteps, ctx->dSteps + 1, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->d2h));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     for (int s = 0; s < slabs; s++) {
@@ -1376,14 +1376,18 @@ int wacomm_b200_set_surrogate(wacomm_b200_context *ctx, const float *parameters,
 int wacomm_b200_last_surrogate_stats(const wacomm_b200_context *ctx, size_t *run, size_t *fallback,
                                      float *cell_ms, float *step_ms) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
-    if (run) *run = ctx->surrTimed ? ctx->lastRun : 0;
-    if (fallback) *fallback = ctx->surrTimed ? ctx->lastFallback : 0;
+    unsigned long long counts[2] = {0, 0};
     float c = 0.f, s = 0.f;
     if (ctx->surrTimed) {
         cudaSetDevice(ctx->device);
+        wacomm_b200_context *m = const_cast<wacomm_b200_context *>(ctx);
+        CUDA_TRY(m, cudaEventSynchronize(ctx->evStep1));
+        CUDA_TRY(m, cudaMemcpy(counts, ctx->dSurrCounts, sizeof(counts), cudaMemcpyDeviceToHost));
         if (cudaEventElapsedTime(&c, ctx->evCell0, ctx->evCell1) != cudaSuccess) c = 0.f;
         if (cudaEventElapsedTime(&s, ctx->evStep0, ctx->evStep1) != cudaSuccess) s = 0.f;
     }
+    if (run) *run = (size_t)counts[1];
+    if (fallback) *fallback = (size_t)(counts[0] & 0xffffffffull);
     if (cell_ms) *cell_ms = c;
     if (step_ms) *step_ms = s;
     return WACOMM_B200_OK;
@@ -1820,7 +1824,7 @@ int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, in
                     first_time_index, last, T);
     if (ctx->opt.surrogate)
         return fail(ctx, WACOMM_B200_ERR_STATE,
-                    "the surrogate hands its fallback list back to the host: not capturable");
+                    "runs with the surrogate option are not captured");
     cudaSetDevice(ctx->device);
     release_graph(ctx);
     // Uploads in flight finish first (their ready events lie outside the capture), and every
@@ -1892,6 +1896,7 @@ int wacomm_b200_graph_launch(wacomm_b200_context *ctx) {
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     CUDA_TRY(ctx, cudaGraphLaunch(ctx->graphExec, ctx->stream));
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    CUDA_TRY(ctx, accumulate_steps(ctx->dSteps, ctx->dSteps + 1, ctx->stream));
     ctx->pairT0 = ctx->pairT1 = -1;
     ctx->lastLaunches = ctx->graphLaunches;
     return WACOMM_B200_OK;
@@ -2113,6 +2118,22 @@ int wacomm_b200_get_frame(wacomm_b200_context *ctx, int t, float *zeta, float *u
     if ((rc = get(w, s.w, plane * ctx->sW))) return rc;
     if ((rc = get(akt, s.akt, plane * ctx->sW))) return rc;
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return WACOMM_B200_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int wacomm_b200_particle_steps_total(wacomm_b200_context *ctx, int reset, double *total) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    unsigned long long steps = 0;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&steps, ctx->dSteps + 1, sizeof(steps), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    if (reset) CUDA_TRY(ctx, cudaMemsetAsync(ctx->dSteps + 1, 0, sizeof(steps), ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (total) *total = (double)steps;
     return WACOMM_B200_OK;
 }
 

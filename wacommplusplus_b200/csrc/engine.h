@@ -89,6 +89,10 @@ cudaError_t compact_alive(const ParticleSoA &S, int n, const ParticleSoA &tmp, u
                           uint32_t *positions, uint32_t *temp, uint32_t *kept,
                           cudaStream_t stream);
 
+// *total += *steps on the stream (the running particle-step count of a context).
+cudaError_t accumulate_steps(const unsigned long long *steps, unsigned long long *total,
+                             cudaStream_t stream);
+
 cudaError_t count_concentration(const ParticleSoA &S, int n, int concTime, int sRho, int eta,
                                 int xi, uint32_t *conc, cudaStream_t stream);
 

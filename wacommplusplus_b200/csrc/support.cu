@@ -546,6 +546,17 @@ __global__ void count_kernel(ParticleSoA S, int n, int concTime, int sRho, int e
     }
 }
 
+__global__ void accumulate_steps_kernel(const unsigned long long *steps,
+                                        unsigned long long *total) {
+    *total += *steps;
+}
+
+cudaError_t accumulate_steps(const unsigned long long *steps, unsigned long long *total,
+                             cudaStream_t stream) {
+    accumulate_steps_kernel<<<1, 1, 0, stream>>>(steps, total);
+    return cudaGetLastError();
+}
+
 cudaError_t count_concentration(const ParticleSoA &S, int n, int concTime, int sRho, int eta,
                                 int xi, uint32_t *conc, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;

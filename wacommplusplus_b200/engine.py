@@ -308,6 +308,13 @@ class Engine:
         self._check(self._lib.wacomm_b200_synchronize(self._ctx))
         self._in_flight = {}
 
+    def steps_total(self, reset=False):
+        """Particle-steps of every interval since creation or the last reset (device-summed)."""
+        total = ctypes.c_double()
+        self._check(self._lib.wacomm_b200_particle_steps_total(self._ctx, int(bool(reset)),
+                                                               ctypes.byref(total)))
+        return total.value
+
     def stats(self):
         """dict of the last interval: device ms of all kernels, ms of the move launches, kernel
         launches and particle-steps."""
