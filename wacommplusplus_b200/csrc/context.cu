@@ -76,6 +76,10 @@ struct wacomm_b200_context {
     size_t n = 0;
     SoABuffers S, T;
     uint32_t *dKeys = nullptr, *dOrder = nullptr, *dFlags = nullptr, *dPositions = nullptr;
+    // the last full sort's order, the sequence the next sort walks; valid while it is a
+    // permutation of [0, seqN) and seqN is the resident count
+    uint32_t *dSeq = nullptr;
+    size_t seqN = 0;
     size_t workCap = 0;
     uint32_t *dHist = nullptr, *dOffsets = nullptr;
     size_t binsCap = 0;
@@ -121,6 +125,7 @@ struct wacomm_b200_context {
     cudaGraphExec_t graphExec = nullptr;
     std::vector<uint64_t> graphLayout;
     int graphLaunches = 0;
+    size_t graphSeqN = 0;  // the sort sequence a launch of the graph leaves behind
     bool capturing = false;
     // ROMS grid (wacomm_b200_set_roms_grid): rho/u/v masks as bytes in one allocation, the
     // angle's (cos, sin) per rho node (null: earth-relative), and staging for raw records.
@@ -249,12 +254,14 @@ int reserve_particles(wacomm_b200_context *ctx, size_t need, size_t keep) {
 int reserve_work(wacomm_b200_context *ctx, size_t n) {
     if (n <= ctx->workCap && ctx->dKeys) return WACOMM_B200_OK;
     size_t cap = std::max(n, ctx->workCap + ctx->workCap / 2);
-    size_t c1 = 0, c2 = 0, c3 = 0, c4 = 0;
+    size_t c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0;
     int rc;
+    ctx->seqN = 0;
     if ((rc = grow(ctx, ctx->dKeys, c1, cap))) return rc;
     if ((rc = grow(ctx, ctx->dOrder, c2, cap))) return rc;
     if ((rc = grow(ctx, ctx->dFlags, c3, cap))) return rc;
     if ((rc = grow(ctx, ctx->dPositions, c4, cap))) return rc;
+    if ((rc = grow(ctx, ctx->dSeq, c5, cap))) return rc;
     ctx->workCap = cap;
     return WACOMM_B200_OK;
 }
@@ -459,15 +466,25 @@ int reserve_sort(wacomm_b200_context *ctx, size_t count) {
     return reserve_scan(ctx, std::max(bins, count));
 }
 
+// Orders `count` records by cell into order[]. A sort of the whole resident set walks the records
+// in the previous full sort's order (when that is still a permutation of the slots) and keeps its
+// own result for the next one; a sort of a slab walks its slots in order.
 int sort_work(wacomm_b200_context *ctx, const ParticleSoA &S, size_t count, uint32_t *keys,
               uint32_t *order, int &launches) {
     size_t bins = (size_t)ctx->eta * ctx->xi + 1;
     int rc;
     if ((rc = reserve_sort(ctx, count))) return rc;
-    CUDA_TRY(ctx, sort_by_cell(S.j, S.i, (int)count, ctx->eta, ctx->xi, keys, ctx->dHist,
+    const bool whole = order == ctx->dOrder && count == ctx->n && ctx->dSeq;
+    const uint32_t *seq = whole && ctx->seqN == count ? ctx->dSeq : nullptr;
+    CUDA_TRY(ctx, sort_by_cell(S.j, S.i, (int)count, ctx->eta, ctx->xi, seq, keys, ctx->dHist,
                                ctx->dOffsets, ctx->dScanTemp, order, ctx->stream));
     size_t blocks = (bins + 8191) / 8192;
     launches += 3 + (blocks > 1 ? 2 : 0);
+    if (whole) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dSeq, order, count * sizeof(uint32_t),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+        ctx->seqN = count;
+    }
     return WACOMM_B200_OK;
 }
 
@@ -773,6 +790,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     free_soa(ctx->T);
     cudaFree(ctx->dKeys);
     cudaFree(ctx->dOrder);
+    cudaFree(ctx->dSeq);
     cudaFree(ctx->dFlags);
     cudaFree(ctx->dPositions);
     cudaFree(ctx->dHist);
@@ -1774,6 +1792,7 @@ std::vector<uint64_t> layout_of(const wacomm_b200_context *ctx) {
                           (const void *)S.elapsed})
         add(p);
     for (const void *p : {(const void *)ctx->dKeys, (const void *)ctx->dOrder,
+                          (const void *)ctx->dSeq,
                           (const void *)ctx->dHist, (const void *)ctx->dOffsets,
                           (const void *)ctx->dScanTemp, (const void *)ctx->dNodes,
                           (const void *)ctx->dCells, (const void *)ctx->dCellSurface,
@@ -1853,6 +1872,7 @@ int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, in
     ctx->pairT0 = ctx->pairT1 = -1;  // the graph packs its own pairs
     CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     ctx->capturing = true;
+    const size_t seqBefore = ctx->seqN;  // the captured sorts' sequence is written only at launch
     int launches = 0;
     cudaError_t e = cudaMemsetAsync(ctx->dSteps, 0, sizeof(unsigned long long), ctx->stream);
     rc = e == cudaSuccess ? WACOMM_B200_OK
@@ -1860,6 +1880,8 @@ int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, in
     for (int n = 0, t = first_time_index; n < n_intervals && !rc; n++, t += dir)
         rc = enqueue_interval(ctx, t, launches);
     ctx->capturing = false;
+    ctx->graphSeqN = ctx->seqN;
+    ctx->seqN = seqBefore;
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(ctx->stream, &graph);
     ctx->pairT0 = ctx->pairT1 = -1;  // nothing captured has run yet
@@ -1895,6 +1917,7 @@ int wacomm_b200_graph_launch(wacomm_b200_context *ctx) {
     ctx->moveTimed = false;
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     CUDA_TRY(ctx, cudaGraphLaunch(ctx->graphExec, ctx->stream));
+    ctx->seqN = ctx->graphSeqN;
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     CUDA_TRY(ctx, accumulate_steps(ctx->dSteps, ctx->dSteps + 1, ctx->stream));
     ctx->pairT0 = ctx->pairT1 = -1;

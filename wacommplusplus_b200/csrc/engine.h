@@ -73,10 +73,11 @@ cudaError_t exclusive_scan(const uint32_t *in, uint32_t *out, size_t n, uint32_t
                            uint32_t *temp, cudaStream_t stream);
 
 // Counting sort of particles by forcing cell: order[] receives particle slots grouped by cell.
+// The records are visited in the sequence seq[n] (a permutation of the slots; null: slot order).
 // keys/hist/offsets/temp are scratch: keys[n], hist[eta*xi+1], offsets[eta*xi+2].
-cudaError_t sort_by_cell(const double *j, const double *i, int n, int eta, int xi, uint32_t *keys,
-                         uint32_t *hist, uint32_t *offsets, uint32_t *temp, uint32_t *order,
-                         cudaStream_t stream);
+cudaError_t sort_by_cell(const double *j, const double *i, int n, int eta, int xi,
+                         const uint32_t *seq, uint32_t *keys, uint32_t *hist, uint32_t *offsets,
+                         uint32_t *temp, uint32_t *order, cudaStream_t stream);
 
 cudaError_t aos_to_soa(const wacomm_b200_particle *aos, int n, const ParticleSoA &S,
                        cudaStream_t stream);

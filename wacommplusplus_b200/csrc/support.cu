@@ -400,21 +400,26 @@ __device__ __forceinline__ uint32_t cell_key(double j, double i, int eta, int xi
     return (uint32_t)((int)fj * xi + (int)fi);
 }
 
+// Both passes walk the records in the sequence `seq` (a permutation of the slots, or the identity
+// when null); keys are kept in sequence order. Walking in the previous interval's cell order puts
+// the records of one cell next to each other, so a warp's atomics collapse to one per cell even
+// where walls gather hundreds of thousands of records into a few cells.
 __global__ void key_histogram_kernel(const double *j, const double *i, int n, int eta, int xi,
-                                     uint32_t *keys, uint32_t *hist) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+                                     const uint32_t *seq, uint32_t *keys, uint32_t *hist) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t p = seq ? seq[t] : (uint32_t)t;
         uint32_t key = cell_key(j[p], i[p], eta, xi);
-        keys[p] = key;
+        keys[t] = key;
         unsigned active = __activemask();
         unsigned peers = __match_any_sync(active, key);
         if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(hist + key, (uint32_t)__popc(peers));
     }
 }
 
-__global__ void key_scatter_kernel(const uint32_t *keys, int n, uint32_t *cursor,
-                                   uint32_t *order) {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-        uint32_t key = keys[p];
+__global__ void key_scatter_kernel(const uint32_t *keys, int n, const uint32_t *seq,
+                                   uint32_t *cursor, uint32_t *order) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        uint32_t key = keys[t];
         unsigned active = __activemask();
         unsigned peers = __match_any_sync(active, key);
         int lane = threadIdx.x & 31;
@@ -423,20 +428,20 @@ __global__ void key_scatter_kernel(const uint32_t *keys, int n, uint32_t *cursor
         if (lane == leader) base = atomicAdd(cursor + key, (uint32_t)__popc(peers));
         base = __shfl_sync(peers, base, leader);
         uint32_t rank = __popc(peers & ((1u << lane) - 1u));
-        order[base + rank] = (uint32_t)p;
+        order[base + rank] = seq ? seq[t] : (uint32_t)t;
     }
 }
 
-cudaError_t sort_by_cell(const double *j, const double *i, int n, int eta, int xi, uint32_t *keys,
-                         uint32_t *hist, uint32_t *offsets, uint32_t *temp, uint32_t *order,
-                         cudaStream_t stream) {
+cudaError_t sort_by_cell(const double *j, const double *i, int n, int eta, int xi,
+                         const uint32_t *seq, uint32_t *keys, uint32_t *hist, uint32_t *offsets,
+                         uint32_t *temp, uint32_t *order, cudaStream_t stream) {
     size_t bins = (size_t)eta * xi + 1;
     cudaMemsetAsync(hist, 0, bins * sizeof(uint32_t), stream);
     int blocks = grid_for((size_t)n, 256);
-    key_histogram_kernel<<<blocks, 256, 0, stream>>>(j, i, n, eta, xi, keys, hist);
+    key_histogram_kernel<<<blocks, 256, 0, stream>>>(j, i, n, eta, xi, seq, keys, hist);
     cudaError_t e = exclusive_scan(hist, offsets, bins, offsets + bins, temp, stream);
     if (e != cudaSuccess) return e;
-    key_scatter_kernel<<<blocks, 256, 0, stream>>>(keys, n, offsets, order);
+    key_scatter_kernel<<<blocks, 256, 0, stream>>>(keys, n, seq, offsets, order);
     return cudaGetLastError();
 }
 
