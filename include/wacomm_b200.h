@@ -376,7 +376,11 @@ int wacomm_b200_stream(const wacomm_b200_context *ctx, void **out);
  * pointer owned by the caller, particles (AoS particle_data) are updated in place,
  * the call is asynchronous on `stream` (a cudaStream_t, NULL = legacy default stream) and returns
  * the CUDA error code of the launch (0 = cudaSuccess). mask, num_thread and num_gpu are ignored
- * like the reference does; wind/stokes may be NULL. Device semantics, reference arithmetic. */
+ * like the reference does; wind/stokes may be NULL. Device semantics, reference arithmetic.
+ * The records are moved in horizontal-cell order (key, histogram, scan, scatter; the order
+ * changes no result) with working memory taken from the device's memory pool on `stream`
+ * (cudaMallocAsync, about 8 B per record + 8 B per cell, released with cudaFreeAsync); when the
+ * pool has none, the records are moved in caller order. */
 int wacomm_b200_cuda_move_particle(const wacomm_b200_config *config_device,
                                    wacomm_b200_particle *particles_device, int time_index,
                                    int ocean_time, int s_w, int s_rho, int eta, int xi,
@@ -393,7 +397,7 @@ int wacomm_b200_cuda_move_particle(const wacomm_b200_config *config_device,
  * memory: cudaFree synchronizes the whole device (and cudaMalloc may), stalling every other
  * stream a multi-stream or multi-GPU driver keeps in flight, and some host frameworks own all
  * device memory through their own pool. Same arguments, meaning and results as
- * wacomm_b200_cuda_move_particle; it also orders the work by horizontal cell, and its working
+ * wacomm_b200_cuda_move_particle, whose horizontal-cell ordering it shares, but its working
  * memory (keys, histogram, scan, order) is a fixed array of about 25 MB compiled into the library
  * and held on every GPU that loads it. Limits: particle_count <= 2,097,152 and eta*xi <=
  * 1,048,576; larger calls return -WACOMM_B200_ERR_CAPACITY and do nothing. Otherwise returns 0 or

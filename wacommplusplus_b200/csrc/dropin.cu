@@ -1,20 +1,55 @@
 // Drop-in replacement of the reference GPU launcher (kernel.cu:370-382): same arguments, same
 // in-place update of the caller's particle_data records, device rules and reference arithmetic.
-// Compiled with -fmad=false.
+// The work is ordered by horizontal cell first (key per record, histogram, exclusive scan,
+// scatter into a work order), so that the threads of a warp gather the same forcing cells; each
+// record still moves independently, so the order changes no result. The ordering scratch is
+// stream-ordered (cudaMallocAsync/cudaFreeAsync on the caller's stream, served from the device's
+// memory pool without a device-wide synchronization); if it cannot be had, the records are moved
+// in caller order. Compiled with -fmad=false.
 #include "engine.h"
 #include "move_kernels.cuh"
 #include "wacomm_b200_kernel.h"
 
 namespace wb {
 
-// One thread per record. Like the reference kernel, each thread derives the interval from the
-// device copies of config and times (kernel.cu:158-171); the particle is read from and written
-// back to the caller's AoS array.
+// Cell key of each record (last bin for records outside the interpolation cells) and the
+// warp-aggregated histogram of the keys.
+__global__ void dropin_key_kernel(const wacomm_b200_particle *particles, int n, int eta, int xi,
+                                  uint32_t *keys, uint32_t *hist) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        double fj = floor(particles[p].j), fi = floor(particles[p].i);
+        uint32_t key = (fj >= 0.0 && fi >= 0.0 && fj < (double)(eta - 1) && fi < (double)(xi - 1))
+                           ? (uint32_t)((int)fj * xi + (int)fi)
+                           : (uint32_t)((size_t)eta * xi);
+        keys[p] = key;
+        unsigned peers = __match_any_sync(__activemask(), key);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(hist + key, (uint32_t)__popc(peers));
+    }
+}
+
+// Work order: record slots grouped by key, from the exclusive offsets of the histogram.
+__global__ void dropin_scatter_kernel(const uint32_t *keys, int n, uint32_t *cursor,
+                                      uint32_t *order) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        uint32_t key = keys[p];
+        unsigned peers = __match_any_sync(__activemask(), key);
+        int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(cursor + key, (uint32_t)__popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        order[base + __popc(peers & ((1u << lane) - 1u))] = (uint32_t)p;
+    }
+}
+
+// One thread per record, taken in the work order (null: caller order). Like the reference
+// kernel, each thread derives the interval from the device copies of config and times
+// (kernel.cu:158-171); the particle is read from and written back to the caller's AoS array.
 __global__ void __launch_bounds__(256) dropin_move_kernel(
     const wacomm_b200_config *__restrict__ config, wacomm_b200_particle *particles,
-    int timeIndex, int oceanTime, const double *__restrict__ times, RawView V, int count) {
-    int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= count) return;
+    const uint32_t *__restrict__ order, int timeIndex, int oceanTime,
+    const double *__restrict__ times, RawView V, int count) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
     const wacomm_b200_config &cfg = *config;
     IntervalParams P;
     make_interval(cfg, times, oceanTime, timeIndex, V.g.sW, SEM_DEVICE, P);
@@ -22,6 +57,7 @@ __global__ void __launch_bounds__(256) dropin_move_kernel(
     RawView view = V;
     view.t0 = P.t0;
     view.t1 = P.t1;
+    uint32_t idx = order ? order[t] : (uint32_t)t;
     wacomm_b200_particle rec = particles[idx];
     ParticleState p;
     p.id = rec.id;
@@ -70,11 +106,44 @@ int dropin_move(const wacomm_b200_config *config, wacomm_b200_particle *particle
     V.hasWindU = windU != nullptr;
     V.hasWindV = windV != nullptr;
     V.hasStokes = stokesU != nullptr && stokesV != nullptr;
+    uint32_t *order = nullptr, *scratch = nullptr;
+    if (eta >= 2 && xi >= 2) {
+        // keys[count] | order[count] | histogram[bins] | offsets[bins + 1] | scan partials
+        size_t bins = (size_t)eta * xi + 1;
+        size_t words = 2 * (size_t)count + 2 * bins + 1 + scan_temp_words(bins);
+        if (cudaMallocAsync((void **)&scratch, words * sizeof(uint32_t), stream) == cudaSuccess) {
+            uint32_t *keys = scratch, *hist = scratch + 2 * (size_t)count;
+            uint32_t *offsets = hist + bins, *partials = offsets + bins + 1;
+            int blocks = (count + 255) / 256;
+            if (blocks > 148 * 16) blocks = 148 * 16;
+            cudaError_t e = cudaMemsetAsync(hist, 0, bins * sizeof(uint32_t), stream);
+            if (e == cudaSuccess) {
+                dropin_key_kernel<<<blocks, 256, 0, stream>>>(particles, count, eta, xi, keys,
+                                                              hist);
+                e = exclusive_scan(hist, offsets, bins, offsets + bins, partials, stream);
+            }
+            if (e == cudaSuccess) {
+                order = keys + count;
+                dropin_scatter_kernel<<<blocks, 256, 0, stream>>>(keys, count, offsets, order);
+            } else {
+                cudaFreeAsync(scratch, stream);
+                return (int)e;
+            }
+        } else {
+            scratch = nullptr;
+            (void)cudaGetLastError();  // no pool memory: caller order
+        }
+    }
     const int threads = 128;
     int blocks = count / threads + ((count % threads) == 0 ? 0 : 1);
-    dropin_move_kernel<<<blocks, threads, 0, stream>>>(config, particles, timeIndex, oceanTime,
-                                                       times, V, count);
-    return (int)cudaGetLastError();
+    dropin_move_kernel<<<blocks, threads, 0, stream>>>(config, particles, order, timeIndex,
+                                                       oceanTime, times, V, count);
+    cudaError_t e = cudaGetLastError();
+    if (scratch) {
+        cudaError_t f = cudaFreeAsync(scratch, stream);
+        if (e == cudaSuccess) e = f;
+    }
+    return (int)e;
 }
 
 }  // namespace wb
