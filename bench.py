@@ -467,7 +467,8 @@ def surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, d
            "gpu_launches": launches,
            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                         "frac": achieved / peak, "peak_source": peak_kind,
-                        "kernel": "surrogate_step_kernel", "kernel_ms": kernel_ms,
+                        "kernel": "surrogate_step_kernel + surrogate_post_kernel",
+                        "kernel_ms": kernel_ms,
                         "flop_per_particle_interval": SURROGATE_FLOP,
                         "cell_kernel_ms": statistics.mean(cell_ms),
                         "traffic": traffic}}

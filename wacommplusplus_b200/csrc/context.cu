@@ -112,6 +112,8 @@ struct wacomm_b200_context {
     bool dryValid = false;
     uint32_t *dFallback = nullptr;  // fallback list
     size_t fallbackCap = 0;
+    float4 *dSurrRows = nullptr;  // surrogate layer-4 sums and row tags per work item
+    size_t surrRowsCap = 0;
     unsigned long long *dSurrCounts = nullptr;  // [0]: fallback count (low 32 bits), [1]: run count
     cudaEvent_t evCell0 = nullptr, evCell1 = nullptr, evStep0 = nullptr, evStep1 = nullptr;
     bool surrTimed = false;
@@ -620,14 +622,15 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
         ctx->zSemantics = ctx->metricSemantics;
     }
     CUDA_TRY(ctx, cudaEventRecord(ctx->evCell1, ctx->stream));
-    // work order and fallback list
+    // Work in slot order, unsorted: the per-cell data the step kernel gathers (FP16 layer-1 sums
+    // and corner records) stays in L2, while the particle state is read and written coalesced.
     if ((rc = reserve_work(ctx, count))) return rc;
     if ((rc = grow(ctx, ctx->dFallback, ctx->fallbackCap, count))) return rc;
-    if ((rc = sort_work(ctx, ctx->S.s, count, ctx->dKeys, ctx->dOrder, launches))) return rc;
+    if ((rc = grow(ctx, ctx->dSurrRows, ctx->surrRowsCap, count))) return rc;
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->dSurrCounts, 0, 2 * sizeof(unsigned long long), ctx->stream));
     MoveLaunch L;
     L.count = (int)count;
-    L.order = ctx->dOrder;
+    L.order = nullptr;
     const int concTime = P.t0 + P.direction;
     const bool countHere = ctx->opt.fuse_concentration && ctx->dConc && concTime >= 0 &&
                            concTime < ctx->concTimes;
@@ -654,11 +657,12 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     st.fallback = ctx->dFallback;
     st.fallbackCount = reinterpret_cast<uint32_t *>(ctx->dSurrCounts);
     st.runCount = ctx->dSurrCounts + 1;
+    st.rows = ctx->dSurrRows;
     CUDA_TRY(ctx, cudaEventRecord(ctx->evMove0, ctx->stream));
     CUDA_TRY(ctx, cudaEventRecord(ctx->evStep0, ctx->stream));
     ctx->moveTimed = true;
     CUDA_TRY(ctx, surrogate_step(st, ctx->S.s, L, ctx->smCount, ctx->stream));
-    launches++;
+    launches += 2;
     CUDA_TRY(ctx, cudaEventRecord(ctx->evStep1, ctx->stream));
     unsigned long long counts[2] = {0, 0};
     CUDA_TRY(ctx, cudaMemcpyAsync(counts, ctx->dSurrCounts, sizeof(counts), cudaMemcpyDeviceToHost,
@@ -804,6 +808,7 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dCorners);
     cudaFree(ctx->dDry);
     cudaFree(ctx->dFallback);
+    cudaFree(ctx->dSurrRows);
     cudaFree(ctx->dSurrCounts);
     if (ctx->evCell0) cudaEventDestroy(ctx->evCell0);
     if (ctx->evCell1) cudaEventDestroy(ctx->evCell1);

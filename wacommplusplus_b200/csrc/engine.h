@@ -210,6 +210,7 @@ struct SurrogateStep {
     const uint8_t *weights;
     uint32_t *fallback, *fallbackCount;
     unsigned long long *runCount;
+    float4 *rows;  // per work item (count): layer-4 sums and row tag, step kernel -> post kernel
 };
 
 size_t surrogate_packed_bytes();
@@ -223,6 +224,8 @@ cudaError_t surrogate_cells(int eta, int xi, int sW, int sRho, const FrameDevice
                             const FrameDevice &f1, const double *h, const double *depthIntervals,
                             const double2 *metric, const uint8_t *weights, __half *z, void *corners,
                             int *err, int smCount, cudaStream_t stream);
+// The step kernel (layers 1-4 of every work item into s.rows) and the post kernel (displacement,
+// closures, state, concentration, fallback list): two launches.
 cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const MoveLaunch &L,
                            int smCount, cudaStream_t stream);
 // Inclusive 2-D prefix sums [(eta+1)][(xi+1)] of nodes with mask 0 or h <= shore.

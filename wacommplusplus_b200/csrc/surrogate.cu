@@ -6,12 +6,17 @@
 //   particle starts in, so it is evaluated once per cell-level as a GEMM
 //   [cell-levels x 384] x [384 x 256] (BF16 operands, FP32 accumulation in TMEM) and stored as
 //   FP16 pre-activations z, together with the uniformity gate of the stencil;
-// * surrogate_step_kernel: per tile of 128 particles (in cell order), layer 1 is finished on the
-//   CUDA cores from z and the four particle features, layers 2 and 3 run as two
-//   [128 x 256] x [256 x 256] tcgen05 GEMMs with the weights streamed through a 3-stage
-//   shared-memory ring by bulk copies, layer 3's epilogue folds in the 3-output layer 4, and the
-//   displacement is applied with the closures in closed form. Particles the surrogate does not
-//   cover are appended to a fallback list for the plain kernel.
+// * surrogate_step_kernel: per tile of 128 particles (taken in slot order: the particle state is
+//   read coalesced, and the per-cell z rows and corner records it gathers stay in L2), layer 1 is
+//   finished on the CUDA cores from z and the four particle features, layers 2 and 3 run as two
+//   [128 x 256] x [256 x 256] tcgen05 GEMMs with the weights streamed through a 2-stage
+//   shared-memory ring by bulk copies, and layer 3's epilogue folds in the 3-output layer 4. The
+//   three outputs and a row tag go to rows[] per work item;
+// * surrogate_post_kernel: one thread per work item applies the displacement with the closures in
+//   closed form, updates the state and the fused concentration, and appends the particles the
+//   surrogate does not cover to a fallback list for the plain kernel. Run apart from the GEMM
+//   pipeline, its dependent loads overlap across a full SM of warps instead of stalling the row
+//   warps of the step kernel.
 //
 // Warp roles of the step kernel (320 threads): warps 0-7 own the tile's rows (warp w holds rows
 // 32(w%4).. and columns 128(w/4).. of the accumulator, the TMEM lane quarter it may access), warp
@@ -321,6 +326,7 @@ struct StepArgs {
     const uint8_t *weights;
     uint32_t *fallback, *fallbackCount;
     unsigned long long *runCount;
+    float4 *rows;     // per work item: layer-4 sums (with b4, before the gate), row tag
 };
 
 constexpr int STEP_THREADS = 320;
@@ -329,6 +335,9 @@ constexpr uint32_t A_BYTES = HID_KB * KBLOCK_A;  // 64 KB: one tile's activation
 constexpr size_t STEP_SMEM = 2 * (size_t)A_BYTES + WRING * (size_t)KBLOCK_W + 1024;
 
 enum : int { ROW_NONE = 0, ROW_RUN = 1, ROW_FALLBACK = 2, ROW_EMPTY = 3 };
+// Row tag of a work item in rows[]: the cell-level (>= 0) of a row the surrogate moves, or one of
+// these.
+constexpr int ROW_CODE_NONE = -1, ROW_CODE_FALLBACK = -2;
 
 // A tile's row as the prologue classified it.
 struct RowTag {
@@ -647,142 +656,33 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             return ok;
         };
 
-        // displacement, closures and state of a row of tile x (lower column half)
-        auto post = [&](const RowTag &tag, float o0, float o1, float o2, bool ok) {
-            long long concCell = -1;
-            int steps = 0;
-            bool run = false;
-            int status = tag.status;
-            const bool write = ok && !abortFlag;
-            if (status != ROW_EMPTY && write) {
-                const uint32_t slot = tag.slot;
-                const double pj = S.j[slot], pi = S.i[slot], pk = S.k[slot];
-                const double ptime = S.time[slot], page = S.age[slot], phealth = S.health[slot];
-                if (status == ROW_RUN) {
-                    // the corner record: u[0],u[1],v[0],v[1],wU[0],wU[1],wL[0],wL[1],zeta[0],zeta[1],h
-                    // as float4s, then {1/xdist, 1/ydist}, then {depth, gate}
-                    const float4 *cf = reinterpret_cast<const float4 *>(a.corners + tag.cl);
-                    const float4 cu0 = __ldg(cf + 0), cu1 = __ldg(cf + 1), cv0 = __ldg(cf + 2),
-                                 cv1 = __ldg(cf + 3), cwU0 = __ldg(cf + 4), cwU1 = __ldg(cf + 5),
-                                 cwL0 = __ldg(cf + 6), cwL1 = __ldg(cf + 7), cz0 = __ldg(cf + 8),
-                                 cz1 = __ldg(cf + 9), ch = __ldg(cf + 10);
-                    const double2 inv = __ldg(reinterpret_cast<const double2 *>(cf + 11));
-                    const double depth = __ldg(reinterpret_cast<const double *>(cf + 12));
-                    const float gate = __ldg(reinterpret_cast<const float *>(cf + 12) + 2);
-                    const double y0 = (double)((o0 + red[r * 3 + 0] + b4s[0]) * gate);
-                    const double y1 = (double)((o1 + red[r * 3 + 1] + b4s[1]) * gate);
-                    const double y2 = (double)((o2 + red[r * 3 + 2] + b4s[2]) * gate);
-                    const double fj = floor(pj), fi = floor(pi), ck = ceil(pk);
-                    const float jF = (float)(pj - fj), iF = (float)(pi - fi), kF = (float)(ck - pk);
-                    const double da0 = ptime > T0 ? (ptime - T0) * a.invLength : 0.0;
-                    const double amid = 0.5 * (da0 + 1.0), trem = (1.0 - da0) * a.length;
-                    const double nSub = fmax(1.0, ceil(trem * a.invDti - 1e-9));
-                    const float am = (float)amid;
-                    const float ub = blend(bil4(cu0, jF, iF), bil4(cu1, jF, iF), am);
-                    const float vb = blend(bil4(cv0, jF, iF), bil4(cv1, jF, iF), am);
-                    const float wb = blend(blend(bil4(cwU0, jF, iF), bil4(cwL0, jF, iF), kF),
-                                           blend(bil4(cwU1, jF, iF), bil4(cwL1, jF, iF), kF), am);
-                    const float hc = bil4(ch, jF, iF) + blend(bil4(cz0, jF, iF), bil4(cz1, jF, iF), am);
-                    const float zdist = hc * (float)depth;
-                    const double dI = ((double)ub * trem + OUT_H * y0) * inv.x;
-                    const double dJ = ((double)vb * trem + OUT_H * y1) * inv.y;
-                    const double dK = (double)(((wb + (float)a.sv) * (float)trem + OUT_V * (float)y2) *
-                                               __frcp_rn(zdist));
-                    const double invSub = 1.0 / nSub;
-                    double mj, mi;
-                    double jn = pinned_axis(pj, dJ, dJ * invSub, nSub, (double)(a.eta - 1), mj);
-                    double in = pinned_axis(pi, dI, dI * invSub, nSub, (double)(a.xi - 1), mi);
-                    const double m = fmin(mj, mi);
-                    const bool crossed = m <= nSub;
-                    bool dead = false;
-                    if (a.horizontal == 1) {  // constraint: the last in-domain substep
-                        const double keep = crossed ? (m - 1) / nSub : 1.0;
-                        jn = pj + keep * dJ;
-                        in = pi + keep * dI;
-                    } else if (a.horizontal == 2 && crossed) {  // kill
-                        dead = true;
-                        jn = pj;
-                        in = pi;
-                    }
-                    double kn = pk + dK;
-                    if (kn > 0) {
-                        if (a.upper == 1) kn = 0;
-                        else if (a.upper == 2) dead = true;
-                        else if (a.upper == 3) kn = -kn;
-                    }
-                    if (kn < kLower) {
-                        if (a.lower == 1) kn = kLower;
-                        else if (a.lower == 2) dead = true;
-                        else if (a.lower == 3) kn = 2.0 * kLower - kn;
-                    }
-                    int ja = (int)floor(fmin(pj, jn)), jb = (int)floor(fmax(pj, jn)) + 1;
-                    int ia = (int)floor(fmin(pi, in)), ib = (int)floor(fmax(pi, in)) + 1;
-                    ja = ja < 0 ? 0 : (ja > a.eta - 1 ? a.eta - 1 : ja);
-                    jb = jb < 0 ? 0 : (jb > a.eta - 1 ? a.eta - 1 : jb);
-                    ia = ia < 0 ? 0 : (ia > a.xi - 1 ? a.xi - 1 : ia);
-                    ib = ib < 0 ? 0 : (ib > a.xi - 1 ? a.xi - 1 : ib);
-                    if (dry_in_box(a.dry, a.xi, ja, jb, ia, ib) > 0) {
-                        status = ROW_FALLBACK;
-                    } else {
-                        const double age = page + trem;
-                        const double health = exp(-age * a.invTau0);
-                        dead = dead || health < a.survprob;
-                        S.j[slot] = jn;
-                        S.i[slot] = in;
-                        S.k[slot] = kn;
-                        S.age[slot] = age;
-                        S.health[slot] = dead ? -1.0 : health;
-                        ParticleState p;
-                        p.j = jn;
-                        p.i = in;
-                        p.k = kn;
-                        p.health = dead ? -1.0 : health;
-                        if (L.conc) concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
-                        steps = (int)nSub;
-                        run = true;
-                    }
-                } else if (status == ROW_NONE && L.conc) {
-                    ParticleState p;
-                    p.j = pj;
-                    p.i = pi;
-                    p.k = pk;
-                    p.health = phealth;
-                    concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
-                }
-                if (status == ROW_FALLBACK) {
-                    const uint32_t at = atomicAdd(a.fallbackCount, 1u);
-                    a.fallback[at] = slot;
-                }
-            }
-            __syncwarp();
-            if (L.steps) warp_sum_steps(L.steps, steps);
-            if (L.conc) warp_count(L.conc, concCell);
-            const unsigned ran = __ballot_sync(0xffffffffu, run);
-            if (lane == 0 && ran) atomicAdd(a.runCount, (unsigned long long)__popc(ran));
-        };
-
         RowTag cur{0u, ROW_EMPTY, 0}, next{0u, ROW_EMPTY, 0}, after{0u, ROW_EMPTY, 0};
-        bool okCur = true, okNext = true;
         if (nT > 0) cur = prologue(0, fetch(0));
         if (nT > 1) next = prologue(1, fetch(1));
-        if (nT > 0) okCur = epilogue2(0);
+        if (nT > 0) epilogue2(0);
         for (int k = 0; k < nT; k++) {
             // the state gather of tile k+2 overlaps the epilogues below
             const RowState ahead = fetch(k + 2);
-            if (k + 1 < nT) okNext = epilogue2(k + 1);
+            if (k + 1 < nT) epilogue2(k + 1);
             float o0, o1, o2;
-            okCur = epilogue3(k, o0, o1, o2) && okCur;
+            epilogue3(k, o0, o1, o2);
+            if (half == 0 && cur.status != ROW_EMPTY) {
+                // layer-4 sums and the row tag of the work item, for surrogate_post_kernel
+                const int code = cur.status == ROW_RUN
+                                     ? cur.cl
+                                     : (cur.status == ROW_FALLBACK ? ROW_CODE_FALLBACK : ROW_CODE_NONE);
+                a.rows[tileOf(k) * TILE + r] =
+                    make_float4(o0 + red[r * 3 + 0] + b4s[0], o1 + red[r * 3 + 1] + b4s[1],
+                                o2 + red[r * 3 + 2] + b4s[2], __int_as_float(code));
+            }
             if (k + 2 < nT) after = prologue(k + 2, ahead);
-            if (half == 0) post(cur, o0, o1, o2, okCur);
             // uniform stop decision of the row warps
             named_sync(1, 256);
             if (tid == 0) rowStop = abortFlag;
             named_sync(1, 256);
             if (rowStop) break;
             cur = next;
-            okCur = okNext;
             next = after;
-            okNext = true;
         }
     }
     fence_before_sync();
@@ -792,6 +692,128 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
         tmem_dealloc(tmem, 512);
     }
     if (tid == 0 && abortFlag) atomicOr(L.err, ERR_SURROGATE_WAIT);
+}
+
+// Displacement, closures and state update of one work item from its layer-4 sums and row tag
+// (rows[n], written by surrogate_step_kernel): one thread per item, so that the dependent loads
+// of the particle state, the corner record and the dry-node table overlap across many warps.
+__global__ void __launch_bounds__(256) surrogate_post_kernel(const StepArgs a, ParticleSoA S,
+                                                             const MoveLaunch L) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const double T0 = a.start;
+    const double kLower = -a.sW + 2;
+    // a step kernel that gave up on a wait left its rows incomplete: nothing is written
+    const bool write = n < L.count && !(L.err && (*L.err & ERR_SURROGATE_WAIT));
+    long long concCell = -1;
+    int steps = 0;
+    bool run = false;
+    if (write) {
+        const float4 row = a.rows[n];
+        const int code = __float_as_int(row.w);
+        int status = code >= 0 ? ROW_RUN : (code == ROW_CODE_FALLBACK ? ROW_FALLBACK : ROW_NONE);
+        const uint32_t slot = L.order ? L.order[n] : (uint32_t)n;
+        const double pj = S.j[slot], pi = S.i[slot], pk = S.k[slot];
+        const double ptime = S.time[slot], page = S.age[slot], phealth = S.health[slot];
+        if (status == ROW_RUN) {
+            // the corner record: u[0],u[1],v[0],v[1],wU[0],wU[1],wL[0],wL[1],zeta[0],zeta[1],h
+            // as float4s, then {1/xdist, 1/ydist}, then {depth, gate}
+            const float4 *cf = reinterpret_cast<const float4 *>(a.corners + code);
+            const float4 cu0 = __ldg(cf + 0), cu1 = __ldg(cf + 1), cv0 = __ldg(cf + 2),
+                         cv1 = __ldg(cf + 3), cwU0 = __ldg(cf + 4), cwU1 = __ldg(cf + 5),
+                         cwL0 = __ldg(cf + 6), cwL1 = __ldg(cf + 7), cz0 = __ldg(cf + 8),
+                         cz1 = __ldg(cf + 9), ch = __ldg(cf + 10);
+            const double2 inv = __ldg(reinterpret_cast<const double2 *>(cf + 11));
+            const double depth = __ldg(reinterpret_cast<const double *>(cf + 12));
+            const float gate = __ldg(reinterpret_cast<const float *>(cf + 12) + 2);
+            const double y0 = (double)(row.x * gate);
+            const double y1 = (double)(row.y * gate);
+            const double y2 = (double)(row.z * gate);
+            const double fj = floor(pj), fi = floor(pi), ck = ceil(pk);
+            const float jF = (float)(pj - fj), iF = (float)(pi - fi), kF = (float)(ck - pk);
+            const double da0 = ptime > T0 ? (ptime - T0) * a.invLength : 0.0;
+            const double amid = 0.5 * (da0 + 1.0), trem = (1.0 - da0) * a.length;
+            const double nSub = fmax(1.0, ceil(trem * a.invDti - 1e-9));
+            const float am = (float)amid;
+            const float ub = blend(bil4(cu0, jF, iF), bil4(cu1, jF, iF), am);
+            const float vb = blend(bil4(cv0, jF, iF), bil4(cv1, jF, iF), am);
+            const float wb = blend(blend(bil4(cwU0, jF, iF), bil4(cwL0, jF, iF), kF),
+                                   blend(bil4(cwU1, jF, iF), bil4(cwL1, jF, iF), kF), am);
+            const float hc = bil4(ch, jF, iF) + blend(bil4(cz0, jF, iF), bil4(cz1, jF, iF), am);
+            const float zdist = hc * (float)depth;
+            const double dI = ((double)ub * trem + OUT_H * y0) * inv.x;
+            const double dJ = ((double)vb * trem + OUT_H * y1) * inv.y;
+            const double dK = (double)(((wb + (float)a.sv) * (float)trem + OUT_V * (float)y2) *
+                                       __frcp_rn(zdist));
+            const double invSub = 1.0 / nSub;
+            double mj, mi;
+            double jn = pinned_axis(pj, dJ, dJ * invSub, nSub, (double)(a.eta - 1), mj);
+            double in = pinned_axis(pi, dI, dI * invSub, nSub, (double)(a.xi - 1), mi);
+            const double m = fmin(mj, mi);
+            const bool crossed = m <= nSub;
+            bool dead = false;
+            if (a.horizontal == 1) {  // constraint: the last in-domain substep
+                const double keep = crossed ? (m - 1) / nSub : 1.0;
+                jn = pj + keep * dJ;
+                in = pi + keep * dI;
+            } else if (a.horizontal == 2 && crossed) {  // kill
+                dead = true;
+                jn = pj;
+                in = pi;
+            }
+            double kn = pk + dK;
+            if (kn > 0) {
+                if (a.upper == 1) kn = 0;
+                else if (a.upper == 2) dead = true;
+                else if (a.upper == 3) kn = -kn;
+            }
+            if (kn < kLower) {
+                if (a.lower == 1) kn = kLower;
+                else if (a.lower == 2) dead = true;
+                else if (a.lower == 3) kn = 2.0 * kLower - kn;
+            }
+            int ja = (int)floor(fmin(pj, jn)), jb = (int)floor(fmax(pj, jn)) + 1;
+            int ia = (int)floor(fmin(pi, in)), ib = (int)floor(fmax(pi, in)) + 1;
+            ja = ja < 0 ? 0 : (ja > a.eta - 1 ? a.eta - 1 : ja);
+            jb = jb < 0 ? 0 : (jb > a.eta - 1 ? a.eta - 1 : jb);
+            ia = ia < 0 ? 0 : (ia > a.xi - 1 ? a.xi - 1 : ia);
+            ib = ib < 0 ? 0 : (ib > a.xi - 1 ? a.xi - 1 : ib);
+            if (dry_in_box(a.dry, a.xi, ja, jb, ia, ib) > 0) {
+                status = ROW_FALLBACK;
+            } else {
+                const double age = page + trem;
+                const double health = exp(-age * a.invTau0);
+                dead = dead || health < a.survprob;
+                S.j[slot] = jn;
+                S.i[slot] = in;
+                S.k[slot] = kn;
+                S.age[slot] = age;
+                S.health[slot] = dead ? -1.0 : health;
+                ParticleState p;
+                p.j = jn;
+                p.i = in;
+                p.k = kn;
+                p.health = dead ? -1.0 : health;
+                if (L.conc) concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
+                steps = (int)nSub;
+                run = true;
+            }
+        } else if (status == ROW_NONE && L.conc) {
+            ParticleState p;
+            p.j = pj;
+            p.i = pi;
+            p.k = pk;
+            p.health = phealth;
+            concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
+        }
+        if (status == ROW_FALLBACK) {
+            const uint32_t at = atomicAdd(a.fallbackCount, 1u);
+            a.fallback[at] = slot;
+        }
+    }
+    if (L.steps) warp_sum_steps(L.steps, steps);
+    if (L.conc) warp_count(L.conc, concCell);
+    const unsigned ran = __ballot_sync(__activemask(), run);
+    if ((threadIdx.x & 31) == 0 && ran) atomicAdd(a.runCount, (unsigned long long)__popc(ran));
 }
 
 // ------------------------------------------------------------------ dry-node prefix sums
@@ -941,6 +963,7 @@ cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const M
     a.fallback = s.fallback;
     a.fallbackCount = s.fallbackCount;
     a.runCount = s.runCount;
+    a.rows = s.rows;
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(surrogate_step_kernel,
@@ -951,6 +974,9 @@ cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const M
     long long tiles = ((long long)L.count + TILE - 1) / TILE;
     int blocks = (int)(tiles < smCount ? tiles : smCount);
     surrogate_step_kernel<<<blocks, STEP_THREADS, STEP_SMEM, stream>>>(a, S, L);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    surrogate_post_kernel<<<(L.count + 255) / 256, 256, 0, stream>>>(a, S, L);
     return cudaGetLastError();
 }
 
