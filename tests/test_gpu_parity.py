@@ -212,8 +212,8 @@ def test_host_buffer_entry_matches_resident_path(cuda_device):
 
 @pytest.mark.parametrize("n", [2_200_000, 4_500_001, 9_000_000])
 def test_host_buffer_slabs_match_resident_path(cuda_device, n):
-    """Every slab layout of the host-buffer entry (two slabs; small end slabs around one or two
-    middle slabs) gives the resident path's records and concentration."""
+    """Every slab layout of the host-buffer entry (two slabs; end slabs ramping up to one or
+    several middle slabs) gives the resident path's records and concentration."""
     win = syn.config1_window(n_frames=3)
     p0 = syn.uniform_particles(n, win.eta, win.xi, seed=8)
     cfg = default_config(random=True, randomSeed=4)
@@ -230,6 +230,37 @@ def test_host_buffer_slabs_match_resident_path(cuda_device, n):
         assert e.stats()["particle_steps"] == 120 * n
         assert records_equal(host, resident)
         assert np.array_equal(e.concentration(), conc)
+
+
+def test_sort_sequences_across_host_and_resident_intervals(cuda_device):
+    """Each sort walks the order the previous sort of the same records left (per slab on the host
+    path, whole on the resident one); switching between the two paths, and a graph captured while
+    the sequence held the other layout, still give the records of resident intervals alone."""
+    n = 4_500_001
+    win = syn.config1_window(n_frames=6)
+    p0 = syn.uniform_particles(n, win.eta, win.xi, seed=9)
+    with Engine(cuda_device, arithmetic="fp32") as e:
+        e.load_window(win)
+        e.set_config(default_config(random=False))
+        e.set_particles(p0)
+        for t in range(5):
+            e.move_interval(t)
+        want = e.get_particles()
+        host = p0.copy()
+        e.move_interval_host(0, host)
+        e.move_interval_host(1, host)  # each slab walks its own order from interval 0
+        e.set_particles(host)
+        e.move_interval(2)  # the slab orders do not cover the whole population: slot order
+        after2 = e.get_particles()
+        e.graph_capture(3, 1)
+        scratch = after2.copy()
+        e.move_interval_host(3, scratch)  # the sequence holds slab orders again
+        e.set_particles(after2)
+        e.graph_launch()
+        assert records_equal(e.get_particles(), scratch)
+        e.move_interval(4)  # walks the order the graph's sort left
+        assert records_equal(e.get_particles(), want)
+        e.graph_release()
 
 
 def test_remove_dead_keeps_order(cuda_device):

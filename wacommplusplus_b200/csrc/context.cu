@@ -76,10 +76,13 @@ struct wacomm_b200_context {
     size_t n = 0;
     SoABuffers S, T;
     uint32_t *dKeys = nullptr, *dOrder = nullptr, *dFlags = nullptr, *dPositions = nullptr;
-    // the last full sort's order, the sequence the next sort walks; valid while it is a
-    // permutation of [0, seqN) and seqN is the resident count
+    // The last sorts' orders, the sequence the next sorts walk: for consecutive entries b, e of
+    // seqBounds, dSeq[b, e) is a permutation of [0, e - b) (the work order of the records b..e-1).
+    // Empty: nothing valid. {0, n}: the resident population sorted as one; the slab bounds of
+    // move_interval_host: one permutation per slab. Any permutation gives the same sort; walking
+    // the previous one keeps the histogram atomics from piling up where particles gather.
     uint32_t *dSeq = nullptr;
-    size_t seqN = 0;
+    std::vector<size_t> seqBounds;
     size_t workCap = 0;
     uint32_t *dHist = nullptr, *dOffsets = nullptr;
     size_t binsCap = 0;
@@ -127,7 +130,7 @@ struct wacomm_b200_context {
     cudaGraphExec_t graphExec = nullptr;
     std::vector<uint64_t> graphLayout;
     int graphLaunches = 0;
-    size_t graphSeqN = 0;  // the sort sequence a launch of the graph leaves behind
+    std::vector<size_t> graphSeqBounds;  // the sort sequence a launch of the graph leaves behind
     bool capturing = false;
     // ROMS grid (wacomm_b200_set_roms_grid): rho/u/v masks as bytes in one allocation, the
     // angle's (cos, sin) per rho node (null: earth-relative), and staging for raw records.
@@ -258,7 +261,7 @@ int reserve_work(wacomm_b200_context *ctx, size_t n) {
     size_t cap = std::max(n, ctx->workCap + ctx->workCap / 2);
     size_t c1 = 0, c2 = 0, c3 = 0, c4 = 0, c5 = 0;
     int rc;
-    ctx->seqN = 0;
+    ctx->seqBounds.clear();
     if ((rc = grow(ctx, ctx->dKeys, c1, cap))) return rc;
     if ((rc = grow(ctx, ctx->dOrder, c2, cap))) return rc;
     if ((rc = grow(ctx, ctx->dFlags, c3, cap))) return rc;
@@ -471,28 +474,29 @@ int reserve_sort(wacomm_b200_context *ctx, size_t count) {
 // Orders `count` records by cell into order[]. A sort of the whole resident set walks the records
 // in the previous full sort's order (when that is still a permutation of the slots) and keeps its
 // own result for the next one; a sort of a slab walks its slots in order.
+// Cell sort of `count` records: walks them in seqIn (a permutation of [0, count), or null: slot
+// order) and copies the resulting order to seqOut (or not, if null).
 int sort_work(wacomm_b200_context *ctx, const ParticleSoA &S, size_t count, uint32_t *keys,
-              uint32_t *order, int &launches) {
+              uint32_t *order, const uint32_t *seqIn, uint32_t *seqOut, int &launches) {
     size_t bins = (size_t)ctx->eta * ctx->xi + 1;
     int rc;
     if ((rc = reserve_sort(ctx, count))) return rc;
-    const bool whole = order == ctx->dOrder && count == ctx->n && ctx->dSeq;
-    const uint32_t *seq = whole && ctx->seqN == count ? ctx->dSeq : nullptr;
-    CUDA_TRY(ctx, sort_by_cell(S.j, S.i, (int)count, ctx->eta, ctx->xi, seq, keys, ctx->dHist,
+    CUDA_TRY(ctx, sort_by_cell(S.j, S.i, (int)count, ctx->eta, ctx->xi, seqIn, keys, ctx->dHist,
                                ctx->dOffsets, ctx->dScanTemp, order, ctx->stream));
     size_t blocks = (bins + 8191) / 8192;
     launches += 3 + (blocks > 1 ? 2 : 0);
-    if (whole) {
-        CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dSeq, order, count * sizeof(uint32_t),
+    if (seqOut)
+        CUDA_TRY(ctx, cudaMemcpyAsync(seqOut, order, count * sizeof(uint32_t),
                                       cudaMemcpyDeviceToDevice, ctx->stream));
-        ctx->seqN = count;
-    }
     return WACOMM_B200_OK;
 }
 
 // Moves `count` resident records starting at `offset` over the interval (sort, chunks, count).
+// The first sort walks seqIn (null: slot order); every sort leaves its order in seqOut, which the
+// later chunks walk.
 int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t offset, size_t count,
-                 uint32_t *keys, uint32_t *order, int &launches) {
+                 uint32_t *keys, uint32_t *order, const uint32_t *seqIn, uint32_t *seqOut,
+                 int &launches) {
     if (count == 0) return WACOMM_B200_OK;
     ParticleSoA S = offset_soa(ctx->S.s, offset);
     PackedArgs A = packed_args(ctx);
@@ -515,7 +519,8 @@ int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t of
     if (nChunks < 1) nChunks = 1;
     for (int c = 0; c < nChunks; c++) {
         if (ctx->opt.sort_by_cell) {
-            int rc = sort_work(ctx, S, count, keys, order, launches);
+            int rc = sort_work(ctx, S, count, keys, order, c == 0 ? seqIn : seqOut, seqOut,
+                               launches);
             if (rc) return rc;
             L.order = order;
         }
@@ -576,7 +581,14 @@ int enqueue_interval(wacomm_b200_context *ctx, int time_index, int &launches) {
     if (P.skip || !ctx->n) return WACOMM_B200_OK;
     if (ctx->opt.surrogate) return run_surrogate(ctx, P, launches);
     if ((rc = reserve_work(ctx, ctx->n))) return rc;
-    return run_interval(ctx, P, 0, ctx->n, ctx->dKeys, ctx->dOrder, launches);
+    const std::vector<size_t> whole{0, ctx->n};
+    const uint32_t *seqIn = ctx->seqBounds == whole ? ctx->dSeq : nullptr;
+    ctx->seqBounds.clear();
+    if ((rc = run_interval(ctx, P, 0, ctx->n, ctx->dKeys, ctx->dOrder, seqIn, ctx->dSeq,
+                           launches)))
+        return rc;
+    if (ctx->opt.sort_by_cell) ctx->seqBounds = whole;
+    return WACOMM_B200_OK;
 }
 
 // Surrogate interval: per-cell layer 1 for the forcing pair, cell sort, the tensor-core step, then
@@ -1142,15 +1154,21 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
     if ((rc = grow(ctx, ctx->dAos, ctx->aosCap, n))) return rc;
     ctx->n = n;
     // Slabs: the upload of slab s+1 and the download of slab s-1 overlap the move of slab s. Only
-    // the first upload and the last download are exposed, so the two end slabs are small (1/16 of
-    // the records) and the rest is split into slabs of about 4 M records, whose move outlasts
-    // the copies of their neighbours.
+    // the first upload and the last download are exposed, so the end slabs are small (1/32 of the
+    // records) and the slabs double from there (1/16, 1/8) up to pieces of at most 4 M records in
+    // the middle: a slab's move (about 3 ns per record) outlasts the copy of a neighbour twice its
+    // size (about 1.2 ns per record each way over PCIe), so the compute never waits for a copy.
     std::vector<size_t> bounds{0};
     if (n >= ((size_t)4 << 20)) {
-        const size_t edge = n / 16, rest = n - 2 * edge;
+        const size_t e = n / 32, ramp = 7 * e, rest = n - 2 * ramp;
         const size_t pieces = (rest + ((size_t)4 << 20) - 1) / ((size_t)4 << 20);
-        bounds.push_back(edge);
-        for (size_t q = 1; q <= pieces; q++) bounds.push_back(edge + rest * q / pieces);
+        bounds.push_back(e);
+        bounds.push_back(3 * e);
+        bounds.push_back(ramp);
+        for (size_t q = 1; q < pieces; q++) bounds.push_back(ramp + rest * q / pieces);
+        bounds.push_back(n - ramp);
+        bounds.push_back(n - 3 * e);
+        bounds.push_back(n - e);
         bounds.push_back(n);
     } else {
         const size_t pieces = n >= ((size_t)2 << 20) ? 2 : 1;
@@ -1162,6 +1180,10 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
         cudaEventCreateWithFlags(&up[s], cudaEventDisableTiming);
         cudaEventCreateWithFlags(&done[s], cudaEventDisableTiming);
     }
+    // each slab's sort walks that slab's previous order when the last call had the same slabs
+    const bool sorts = !P.skip && ctx->opt.sort_by_cell;
+    const bool walk = sorts && ctx->seqBounds == bounds;
+    if (sorts) ctx->seqBounds.clear();
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     for (int s = 0; s < slabs; s++) {
         size_t off = bounds[s], cnt = bounds[s + 1] - bounds[s];
@@ -1179,7 +1201,8 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
         CUDA_TRY(ctx, aos_to_soa(ctx->dAos + off, (int)cnt, S, ctx->stream));
         launches++;
         if (!P.skip) {
-            if ((rc = run_interval(ctx, P, off, cnt, ctx->dKeys + off, ctx->dOrder + off, launches)))
+            if ((rc = run_interval(ctx, P, off, cnt, ctx->dKeys + off, ctx->dOrder + off,
+                                   walk ? ctx->dSeq + off : nullptr, ctx->dSeq + off, launches)))
                 return rc;
         }
         CUDA_TRY(ctx, soa_to_aos(S, (int)cnt, ctx->dAos + off, ctx->stream));
@@ -1190,6 +1213,7 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
                                       cnt * sizeof(wacomm_b200_particle), cudaMemcpyDeviceToHost,
                                       ctx->d2h));
     }
+    if (sorts) ctx->seqBounds = bounds;
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     CUDA_TRY(ctx, accumulate_steps(ctx->dSteps, ctx->dSteps + 1, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->d2h));
@@ -1877,7 +1901,10 @@ int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, in
     ctx->pairT0 = ctx->pairT1 = -1;  // the graph packs its own pairs
     CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     ctx->capturing = true;
-    const size_t seqBefore = ctx->seqN;  // the captured sorts' sequence is written only at launch
+    // The captured sorts' sequence is written only at launch, and what dSeq holds when the graph
+    // is launched is not known here: the first captured sort walks slot order.
+    const std::vector<size_t> seqBefore = ctx->seqBounds;
+    ctx->seqBounds.clear();
     int launches = 0;
     cudaError_t e = cudaMemsetAsync(ctx->dSteps, 0, sizeof(unsigned long long), ctx->stream);
     rc = e == cudaSuccess ? WACOMM_B200_OK
@@ -1885,8 +1912,8 @@ int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, in
     for (int n = 0, t = first_time_index; n < n_intervals && !rc; n++, t += dir)
         rc = enqueue_interval(ctx, t, launches);
     ctx->capturing = false;
-    ctx->graphSeqN = ctx->seqN;
-    ctx->seqN = seqBefore;
+    ctx->graphSeqBounds = ctx->seqBounds;
+    ctx->seqBounds = seqBefore;
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(ctx->stream, &graph);
     ctx->pairT0 = ctx->pairT1 = -1;  // nothing captured has run yet
@@ -1922,7 +1949,7 @@ int wacomm_b200_graph_launch(wacomm_b200_context *ctx) {
     ctx->moveTimed = false;
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     CUDA_TRY(ctx, cudaGraphLaunch(ctx->graphExec, ctx->stream));
-    ctx->seqN = ctx->graphSeqN;
+    ctx->seqBounds = ctx->graphSeqBounds;
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     CUDA_TRY(ctx, accumulate_steps(ctx->dSteps, ctx->dSteps + 1, ctx->stream));
     ctx->pairT0 = ctx->pairT1 = -1;
