@@ -117,6 +117,10 @@ typedef struct wacomm_b200_source {
 #define WACOMM_B200_RNG_REFERENCE 0    /* ordered-splitmix64-v2 draws, draw-for-draw with the reference */
 #define WACOMM_B200_RNG_PHILOX 1       /* Philox4x32-10 keyed on (particle id, interval, step time) */
 
+#define WACOMM_B200_LAUNCH_SHAPE_AUTO (-1) /* launch_shape by compiled form: 3 for the deterministic
+                                              form without drift (96 registers, no spills), 2 for
+                                              the others; the default */
+
 typedef struct wacomm_b200_options {
     int semantics;            /* WACOMM_B200_SEMANTICS_* */
     int arithmetic;           /* WACOMM_B200_ARITH_* */
@@ -128,7 +132,8 @@ typedef struct wacomm_b200_options {
     int fuse_concentration;   /* 1: count the concentration in the move kernel's epilogue */
     int launch_shape;         /* FP32 step: 0 = 256 threads, registers unbounded; 1 = 128 threads,
                                  3 blocks/SM; 2 = 256 threads, 2 blocks/SM; 3 = 128 threads,
-                                 5 blocks/SM (fewer registers, more resident warps) */
+                                 5 blocks/SM (fewer registers, more resident warps);
+                                 WACOMM_B200_LAUNCH_SHAPE_AUTO (default): 3 or 2 by form */
     int surrogate;            /* 1: deterministic forward intervals by the learned surrogate
                                  (wacomm_b200_set_surrogate), the rest by the FP32 step */
 } wacomm_b200_options;

@@ -82,6 +82,7 @@ def test_defaults_and_version():
     o = _native.default_options()
     assert (o.semantics, o.arithmetic, o.storage, o.rng) == (0, 1, 0, 0)
     assert (o.block_size, o.substeps_per_launch, o.sort_by_cell, o.fuse_concentration) == (256, 0, 1, 1)
+    assert o.launch_shape == -1  # by compiled form
     assert b"sm_100a" in _native.lib().wacomm_b200_version()
 
 

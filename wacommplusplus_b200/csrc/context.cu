@@ -300,8 +300,8 @@ int validate_options(wacomm_b200_context *ctx, const wacomm_b200_options &o) {
                     o.block_size);
     if (o.substeps_per_launch < 0)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "substeps_per_launch must be >= 0");
-    if (o.launch_shape < 0 || o.launch_shape > 3)
-        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "launch_shape %d out of [0, 3]", o.launch_shape);
+    if (o.launch_shape < WACOMM_B200_LAUNCH_SHAPE_AUTO || o.launch_shape > 3)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "launch_shape %d out of [-1, 3]", o.launch_shape);
     if (o.surrogate != 0 && o.surrogate != 1)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "surrogate %d: 0 or 1", o.surrogate);
     if (o.surrogate && o.arithmetic != WACOMM_B200_ARITH_FP32)
@@ -742,7 +742,7 @@ int wacomm_b200_default_options(wacomm_b200_options *out) {
     out->substeps_per_launch = 0;
     out->sort_by_cell = 1;
     out->fuse_concentration = 1;
-    out->launch_shape = 2;
+    out->launch_shape = WACOMM_B200_LAUNCH_SHAPE_AUTO;
     out->surrogate = 0;
     return WACOMM_B200_OK;
 }

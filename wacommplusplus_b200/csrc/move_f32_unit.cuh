@@ -51,16 +51,25 @@ inline int fast_variant(const wacomm_b200_config &cfg, int direction) {
     return diffuse ? VAR_DIFFUSE : VAR_LEAN;
 }
 
-// Shapes 1 and 2 carry every form; shapes 0 and 3 the full one.
+// Shapes 1, 2 and 3 carry every form; shape 0 the full one. A negative shape picks by form: the
+// lean form fits shape 3's 96 registers without spills and runs 4 % faster there (20 resident
+// warps per SM instead of 16); the others spill at shape 3 and run at shape 2.
 template <int SEM, int STORE>
 cudaError_t move_f32_unit(int shape, const wacomm_b200_config &cfg, const IntervalParams &P,
                           const PackedArgs &A, const ParticleSoA &S, const MoveLaunch &L,
                           cudaStream_t stream) {
     FastView<STORE> F = fast_view<STORE>(A);
     const int variant = fast_variant(cfg, P.direction);
+    if (shape < 0) shape = variant == VAR_LEAN ? 3 : 2;
     switch (shape) {
         case 0: return launch_move_fast<SEM, STORE, 0, VAR_FULL>(cfg, P, F, S, L, stream);
-        case 3: return launch_move_fast<SEM, STORE, 3, VAR_FULL>(cfg, P, F, S, L, stream);
+        case 3:
+            switch (variant) {
+                case VAR_LEAN: return launch_move_fast<SEM, STORE, 3, VAR_LEAN>(cfg, P, F, S, L, stream);
+                case VAR_DIFFUSE: return launch_move_fast<SEM, STORE, 3, VAR_DIFFUSE>(cfg, P, F, S, L, stream);
+                case VAR_DRIFT: return launch_move_fast<SEM, STORE, 3, VAR_DRIFT>(cfg, P, F, S, L, stream);
+                default: return launch_move_fast<SEM, STORE, 3, VAR_FULL>(cfg, P, F, S, L, stream);
+            }
         case 2:
             switch (variant) {
                 case VAR_LEAN: return launch_move_fast<SEM, STORE, 2, VAR_LEAN>(cfg, P, F, S, L, stream);

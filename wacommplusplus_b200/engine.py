@@ -36,7 +36,8 @@ class Engine:
     Options (defaults in brackets): semantics ["host"|"device"], arithmetic ["fp32"|"reference"],
     storage ["fp32"|"fp16"|"bf16"], rng ["reference"|"philox"], block_size [256],
     substeps_per_launch [0 = whole interval], sort_by_cell [True], fuse_concentration [True],
-    launch_shape [2], surrogate [False] (needs set_surrogate).
+    launch_shape [-1: 3 for the lean form, 2 for the others], surrogate [False] (needs
+    set_surrogate).
     """
 
     _SEM = {"host": 0, "device": 1}
