@@ -259,9 +259,12 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
     const uint64_t prefix = fold(fold(mix64(cfg.randomSeed), p.id), (uint64_t)P.intervalKey);
     const uint64_t philoxKey = p.id ^ mix64(cfg.randomSeed);
     const double stop = P.chunkEnd < length ? P.chunkEnd : length;
-    // surface sums at the previous step's destination, valid while the particle still sits there
+    // surface sums, cell and fractional position of the previous step's destination, valid while
+    // the particle still sits there: the next step starts from the same values
     constexpr bool keepStencil = VARIANT == VAR_LEAN;
     SurfaceSums carried{0.f, 0.f};
+    int carriedJ = 0, carriedI = 0;
+    float carriedJF = 0.f, carriedIF = 0.f;
     bool haveCarried = false;
 
     while (elapsed < stop) {
@@ -280,8 +283,22 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
             elapsed = length;
             break;
         }
-        double kc = ceil(p.k), fj0 = floor(p.j), fi0 = floor(p.i);
-        int kI = to_index<SEM>(kc), jI = to_index<SEM>(fj0), iI = to_index<SEM>(fi0);
+        const double kc = ceil(p.k);
+        const int kI = to_index<SEM>(kc);
+        int jI, iI;
+        float jF, iF;
+        if (haveCarried) {
+            jI = carriedJ;
+            iI = carriedI;
+            jF = carriedJF;
+            iF = carriedIF;
+        } else {
+            const double fj0 = floor(p.j), fi0 = floor(p.i);
+            jI = to_index<SEM>(fj0);
+            iI = to_index<SEM>(fi0);
+            jF = (float)(p.j - fj0);
+            iF = (float)(p.i - fi0);
+        }
         if (!valid_cell(jI, iI, eta, xi) || (SEM == SEM_DEVICE && (kI > 0 || kI <= -sW + 1))) {
             p.health = -1;
             lazy = false;
@@ -289,7 +306,7 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
             break;
         }
         steps++;
-        const float kF = (float)(kc - p.k), jF = (float)(p.j - fj0), iF = (float)(p.i - fi0);
+        const float kF = (float)(kc - p.k);
         const float dt = (float)stepDt;
         const float alpha = (float)((elapsed + 0.5 * stepDt) * invLength);
         const float alphaStart = (float)(elapsed * invLength);
@@ -423,11 +440,15 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         double fjd = floor(jdet), fid = floor(idet);
         int jdetI = to_index<SEM>(fjd), idetI = to_index<SEM>(fid);
         if (valid_cell(jdetI, idetI, eta, xi)) {
-            const SurfaceSums there =
-                surface_sums(C, jdetI, idetI, (float)(jdet - fjd), (float)(idet - fid));
+            const float jdF = (float)(jdet - fjd), idF = (float)(idet - fid);
+            const SurfaceSums there = surface_sums(C, jdetI, idetI, jdF, idF);
             float hcdet = there.height(alpha);
             // the next step starts here unless a closure moves the particle
             carried = there;
+            carriedJ = jdetI;
+            carriedI = idetI;
+            carriedJF = jdF;
+            carriedIF = idF;
             haveCarried = hcdet > shore;
             if (hcdet <= shore) {
                 if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
