@@ -45,6 +45,8 @@ extern "C" {
 #define WACOMM_B200_ERR_STATE 3        /* a call out of order (no grid, frame missing ...) */
 #define WACOMM_B200_ERR_DRIFT_OBJECT 4 /* a particle names a drift object outside the catalogue */
 #define WACOMM_B200_ERR_CAPACITY 5     /* a size above a documented maximum */
+#define WACOMM_B200_ERR_IO 6           /* a file could not be opened, written, read or parsed, or a
+                                          restart does not match the run (the message says which) */
 
 /* ------------------------------------------------------------------ records */
 
@@ -422,6 +424,69 @@ int wacomm_b200_cuda_move_particle_noalloc(const wacomm_b200_config *config_devi
                                            const float *stokes_u, const float *stokes_v,
                                            int particle_count, int num_thread, int num_gpu,
                                            void *stream);
+
+/* ------------------------------------------------------------------ history and restart files */
+
+/* Text restart (Particles::saveAsTxt, Particles.cpp:28-55): a "\t<count>" line, then one line per
+ * record: id i j k health age time object side, the reals with 17 significant digits (printf
+ * "%.17g", what the reference's ostream with setprecision(max_digits10) prints), the drift object
+ * and side as integers. Host records; formatted on all host threads. */
+int wacomm_b200_text_write(const char *path, const wacomm_b200_particle *records, size_t n);
+
+/* Reads a text restart (Particles::loadFromTxt, Particles.cpp:320-364): the first line is
+ * skipped; a line of 5 fields is a Fortran record "i j k health age" (id = its line number,
+ * time = -1); a line of 7 or more is "id i j k health age time [object side]"; any other line
+ * is refused. Call with records = NULL to get the count in *n, then with capacity >= *n. */
+int wacomm_b200_text_read(const char *path, wacomm_b200_particle *records, size_t capacity,
+                          size_t *n);
+
+/* Writes the resident records as a text restart: one device-to-host copy, then
+ * wacomm_b200_text_write. */
+int wacomm_b200_save_text(wacomm_b200_context *ctx, const char *path);
+
+/* Provenance and run attributes of a NetCDF history (Provenance.hpp:20-27,
+ * Particles.cpp:154-160); NULL strings are written empty, except proj_version, which is left out
+ * when NULL (a build without PROJ). */
+typedef struct wacomm_b200_history_meta {
+    const char *git_revision, *compiler, *cmake_options;
+    const char *configuration_file, *configuration;  /* the run's configuration path and JSON */
+    const char *proj_version;
+    const char *ocean_model;
+    double checkpoint_time;  /* checkpoint_time attribute and the particle_time value */
+} wacomm_b200_history_meta;
+
+/* NetCDF history / restart of the resident records, schema version 3
+ * (Particles::saveAsNetCDF, Particles.cpp:116-273): the records with j >= 0, i >= 0, k <= 0 and a
+ * position on the grid, in order, as id, object_type, drift_side and lat, lon, depth, k, j, i,
+ * health, age, time [particles][particle_time = 1], with the reference's attributes; tracking
+ * direction and random seed from set_config, lat/lon/depth by kji2deplatlon from set_geo_grid.
+ * Written as a CDF-5 (64-bit data) classic file, the classic variant that carries the schema's
+ * uint64 and uint variables; the reference writes the same schema through NetCDF-4. The device
+ * selects, locates and compacts the records and lays out every variable's big-endian payload;
+ * the host writes the header and the payload. *written receives the number of records stored. */
+int wacomm_b200_save_netcdf(wacomm_b200_context *ctx, const char *path,
+                            const wacomm_b200_history_meta *meta, size_t *written);
+
+/* What a NetCDF restart must match (Particles::loadFromNetCDF, Particles.cpp:380-430). */
+typedef struct wacomm_b200_restart_expect {
+    const char *ocean_model;  /* the configured ocean model */
+    int backward;             /* the configured tracking direction: 0 forward, 1 backward */
+    uint64_t random_seed;     /* the configured seed */
+    int leeway;               /* drift.model = leeway: version 2 files lack the drift state */
+} wacomm_b200_restart_expect;
+
+/* Reads a NetCDF restart (CDF-1, CDF-2 or CDF-5 classic files): when it carries
+ * wacomm_restart_version, the version must be 2 or 3 (2 refused under leeway), its tracking
+ * direction must match, and random_seed, wacomm_random_key_scheme and ocean_model must match
+ * when present. Records from id, i, j, k, health, age, time (first particle_time column) and,
+ * when present, object_type and drift_side. *checkpoint_time and *has_checkpoint receive the
+ * checkpoint_time attribute. Call with records = NULL for the count, then with capacity >= *n. */
+int wacomm_b200_netcdf_read(const char *path, const wacomm_b200_restart_expect *expect,
+                            wacomm_b200_particle *records, size_t capacity, size_t *n,
+                            double *checkpoint_time, int *has_checkpoint);
+
+/* The message of the last failed file call on this thread (text_write, text_read, netcdf_read). */
+const char *wacomm_b200_file_error(void);
 
 #ifdef __cplusplus
 }

@@ -123,6 +123,8 @@ def oracle_lib():
         lib.wo_kji2deplatlon.argtypes = geo
         lib.wo_deplatlon2kji.restype = ctypes.c_int
         lib.wo_deplatlon2kji.argtypes = geo
+        lib.wo_text_restart.restype = ctypes.c_int
+        lib.wo_text_restart.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t]
         _oracle = lib
     return _oracle
 
@@ -366,3 +368,10 @@ def roms_normalize(mask_rho, mask_u, mask_v, angle, zeta, u, v, w, akt):
     rc = fn(eta, xi, s_rho, _dptr(mask_rho), _dptr(mask_u), _dptr(mask_v), _dptr(angle),
             _fptr(zeta), _fptr(u), _fptr(v), _fptr(w), _fptr(akt), *[_fptr(o) for o in outs])
     return (rc, *outs)
+
+
+def text_restart_file(path, records):
+    """The oracle's text restart of ``records`` (Particles.cpp:28-55), written on one thread."""
+    records = np.ascontiguousarray(records, dtype=PARTICLE_DTYPE)
+    if oracle_lib().wo_text_restart(str(path).encode(), records.ctypes.data, len(records)):
+        raise OSError(f"cannot write {path}")

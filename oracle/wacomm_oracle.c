@@ -10,6 +10,7 @@
 #include "wacomm_oracle.h"
 
 #include <float.h>
+#include <stdio.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -1426,4 +1427,19 @@ int wo_roms_normalize(int eta, int xi, int sRho, const double *maskRho, const do
             aktOut[k * plane + n] = wet ? akt[k * plane + n] : 0.0f;
         }
     return 0;
+}
+
+/* Particles::saveAsTxt / writeTxtHeader / writeTxtRecord (Particles.cpp:28-55). */
+int wo_text_restart(const char *path, const wo_particle *records, size_t n) {
+    FILE *f = fopen(path, "w");
+    if (!f) return -1;
+    int ok = fprintf(f, "\t%d\n", (int)n) > 0;
+    for (size_t r = 0; ok && r < n; r++) {
+        const wo_particle *p = records + r;
+        ok = fprintf(f, "%llu %.17g %.17g %.17g %.17g %.17g %.17g %d %d\n",
+                     (unsigned long long)p->id, p->i, p->j, p->k, p->health, p->age, p->time,
+                     (int)p->driftObjectType, (int)p->driftSide) > 0;
+    }
+    if (fclose(f) != 0) ok = 0;
+    return ok ? 0 : -1;
 }

@@ -194,6 +194,12 @@ int wo_roms_normalize(int eta, int xi, int sRho, const double *maskRho, const do
                       const float *v, const float *w, const float *akt, float *zetaOut,
                       float *uOut, float *vOut, float *wOut, float *aktOut);
 
+/* Particles::saveAsTxt (Particles.cpp:28-55): "\t<count>" then one line per record,
+ * "id i j k health age time object side", the reals with printf "%.17g" (the reference's ostream
+ * with setprecision(max_digits10) in the default float format), one record after the other on
+ * one thread as the reference does. Returns 0, or -1 when the file cannot be written. */
+int wo_text_restart(const char *path, const wo_particle *records, size_t n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,6 +18,7 @@ ERR_CUDA = 2
 ERR_STATE = 3
 ERR_DRIFT_OBJECT = 4
 ERR_CAPACITY = 5
+ERR_IO = 6
 
 SEMANTICS_HOST, SEMANTICS_DEVICE = 0, 1
 ARITH_REFERENCE, ARITH_FP32 = 0, 1
@@ -35,6 +36,24 @@ class options_t(ctypes.Structure):
         ("substeps_per_launch", ctypes.c_int), ("sort_by_cell", ctypes.c_int),
         ("fuse_concentration", ctypes.c_int), ("launch_shape", ctypes.c_int),
         ("surrogate", ctypes.c_int),
+    ]
+
+
+class history_meta_t(ctypes.Structure):
+    """wacomm_b200_history_meta: provenance and run attributes of a NetCDF history."""
+    _fields_ = [
+        ("git_revision", ctypes.c_char_p), ("compiler", ctypes.c_char_p),
+        ("cmake_options", ctypes.c_char_p), ("configuration_file", ctypes.c_char_p),
+        ("configuration", ctypes.c_char_p), ("proj_version", ctypes.c_char_p),
+        ("ocean_model", ctypes.c_char_p), ("checkpoint_time", ctypes.c_double),
+    ]
+
+
+class restart_expect_t(ctypes.Structure):
+    """wacomm_b200_restart_expect: what a NetCDF restart must match."""
+    _fields_ = [
+        ("ocean_model", ctypes.c_char_p), ("backward", ctypes.c_int),
+        ("random_seed", ctypes.c_uint64), ("leeway", ctypes.c_int),
     ]
 
 
@@ -92,6 +111,14 @@ SIGNATURES = {
                                        [_i, _i, _i, _vp]),
     "wacomm_b200_cuda_move_particle_noalloc": (_i, [_vp, _vp, _i, _i, _i, _i, _i, _i] +
                                                [_vp] * 15 + [_i, _i, _i, _vp]),
+    "wacomm_b200_text_write": (_i, [ctypes.c_char_p, _vp, _sz]),
+    "wacomm_b200_text_read": (_i, [ctypes.c_char_p, _vp, _sz, ctypes.POINTER(_sz)]),
+    "wacomm_b200_save_text": (_i, [_vp, ctypes.c_char_p]),
+    "wacomm_b200_save_netcdf": (_i, [_vp, ctypes.c_char_p, ctypes.POINTER(history_meta_t),
+                                     ctypes.POINTER(_sz)]),
+    "wacomm_b200_netcdf_read": (_i, [ctypes.c_char_p, ctypes.POINTER(restart_expect_t), _vp, _sz,
+                                     ctypes.POINTER(_sz), _dp, ctypes.POINTER(_i)]),
+    "wacomm_b200_file_error": (ctypes.c_char_p, []),
 }
 
 _lib = None

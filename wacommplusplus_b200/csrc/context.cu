@@ -1326,6 +1326,75 @@ int wacomm_b200_geo_positions(wacomm_b200_context *ctx, double *depth, double *l
     return WACOMM_B200_OK;
 }
 
+int wacomm_b200_save_text(wacomm_b200_context *ctx, const char *path) {
+    if (!ctx || !path) return WACOMM_B200_ERR_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    std::vector<wacomm_b200_particle> host(ctx->n);
+    if (ctx->n) {
+        int rc;
+        if ((rc = grow(ctx, ctx->dAos, ctx->aosCap, ctx->n))) return rc;
+        CUDA_TRY(ctx, soa_to_aos(ctx->S.s, (int)ctx->n, ctx->dAos, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(host.data(), ctx->dAos, ctx->n * sizeof(wacomm_b200_particle),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    if (history_text_write(path, host.data(), host.size()))
+        return fail(ctx, WACOMM_B200_ERR_IO, "%s", wacomm_b200_file_error());
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_save_netcdf(wacomm_b200_context *ctx, const char *path,
+                            const wacomm_b200_history_meta *meta, size_t *written) {
+    if (!ctx || !path || !meta) return WACOMM_B200_ERR_ARGUMENT;
+    if (written) *written = 0;
+    if (!ctx->hasConfig) return fail(ctx, WACOMM_B200_ERR_STATE, "set_config has not been called");
+    if (!ctx->hasGeo) return fail(ctx, WACOMM_B200_ERR_STATE, "set_geo_grid has not been called");
+    cudaSetDevice(ctx->device);
+    const size_t n = ctx->n;
+    size_t kept = 0;
+    std::vector<uint8_t> payload;
+    if (n) {
+        int rc;
+        if ((rc = grow(ctx, ctx->dGeoOut, ctx->geoOutCap, 3 * n))) return rc;
+        if ((rc = reserve_work(ctx, n))) return rc;
+        if ((rc = reserve_scan(ctx, n))) return rc;
+        double *dDep = ctx->dGeoOut, *dLat = dDep + n, *dLon = dLat + n;
+        CUDA_TRY(ctx, geo_positions(ctx->S.s, (int)n, ctx->eta, ctx->xi, ctx->sW, ctx->dGeoLon,
+                                    ctx->dGeoLat, ctx->dH, ctx->dSWValues, dDep, dLat, dLon,
+                                    ctx->stream));
+        CUDA_TRY(ctx, history_select(ctx->S.s, (int)n, dDep, dLat, dLon, ctx->dFlags, ctx->stream));
+        CUDA_TRY(ctx, exclusive_scan(ctx->dFlags, ctx->dPositions, n, ctx->dCount, ctx->dScanTemp,
+                                     ctx->stream));
+        uint32_t total = 0;
+        CUDA_TRY(ctx, cudaMemcpyAsync(&total, ctx->dCount, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        kept = total;
+        if (kept) {
+            uint8_t *dPayload = nullptr;
+            const size_t bytes = history_payload_bytes(kept);
+            CUDA_TRY(ctx, cudaMallocAsync((void **)&dPayload, bytes, ctx->stream));
+            payload.resize(bytes);
+            cudaError_t e = history_pack(ctx->S.s, (int)n, ctx->dFlags, ctx->dPositions, dDep, dLat,
+                                         dLon, kept, dPayload, ctx->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(payload.data(), dPayload, bytes, cudaMemcpyDeviceToHost,
+                                    ctx->stream);
+            cudaError_t f = cudaFreeAsync(dPayload, ctx->stream);
+            if (e == cudaSuccess) e = f;
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            if (e != cudaSuccess)
+                return fail(ctx, WACOMM_B200_ERR_CUDA, "history payload: %s", cudaGetErrorString(e));
+        }
+    }
+    const std::string header = history_header_for(*meta, ctx->cfg.trackingDirection < 0,
+                                                  ctx->cfg.randomSeed, kept);
+    if (history_netcdf_write(path, header, meta->checkpoint_time, payload.data(), payload.size()))
+        return fail(ctx, WACOMM_B200_ERR_IO, "%s", wacomm_b200_file_error());
+    if (written) *written = kept;
+    return check_errors(ctx);
+}
+
 int wacomm_b200_concentration_reset(wacomm_b200_context *ctx, int n_conc_times) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     if (!ctx->hasGrid) return fail(ctx, WACOMM_B200_ERR_STATE, "set_grid has not been called");

@@ -3,6 +3,8 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
+#include <vector>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -231,6 +233,32 @@ cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const M
 // Inclusive 2-D prefix sums [(eta+1)][(xi+1)] of nodes with mask 0 or h <= shore.
 cudaError_t surrogate_dry_prefix(const double *mask, const double *h, double shore, int eta, int xi,
                                  int *pre, cudaStream_t stream);
+
+// history.cu ------------------------------------------------------------------------------
+
+// Text restart of n host records (Particles.cpp:28-55) / the records of a text restart
+// (Particles.cpp:320-364); WACOMM_B200_ERR_IO with wacomm_b200_file_error() on failure.
+int history_text_write(const char *path, const wacomm_b200_particle *records, size_t n);
+int history_text_read(const char *path, std::vector<wacomm_b200_particle> &records);
+
+// NetCDF history: the CDF-5 header for `kept` records, the file (header, particle_time, payload)
+// and a restart read with the reference's checks.
+std::string history_header_for(const wacomm_b200_history_meta &m, int backward, uint64_t seed,
+                               size_t kept);
+int history_netcdf_write(const char *path, const std::string &header, double particleTime,
+                         const uint8_t *payload, size_t payloadBytes);
+int history_netcdf_read(const char *path, const wacomm_b200_restart_expect &expect,
+                        std::vector<wacomm_b200_particle> &records, double &checkpoint,
+                        bool &hasCheckpoint);
+
+// Device side: flags of the stored records (given kji2deplatlon's dep/lat/lon), and the payload of
+// the `kept` records at their scan positions (88 bytes per record, big-endian, file order).
+size_t history_payload_bytes(size_t kept);
+cudaError_t history_select(const ParticleSoA &S, int n, const double *dep, const double *lat,
+                           const double *lon, uint32_t *flags, cudaStream_t stream);
+cudaError_t history_pack(const ParticleSoA &S, int n, const uint32_t *flags,
+                         const uint32_t *positions, const double *dep, const double *lat,
+                         const double *lon, size_t kept, uint8_t *payload, cudaStream_t stream);
 
 // dropin.cu -------------------------------------------------------------------------------
 int dropin_move(const wacomm_b200_config *config, wacomm_b200_particle *particles, int timeIndex,

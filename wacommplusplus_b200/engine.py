@@ -263,6 +263,20 @@ class Engine:
         self._check(self._lib.wacomm_b200_set_geo_grid(self._ctx, self._geo[0][1],
                                                        self._geo[1][1], self._geo[2][1]))
 
+    def save_text(self, path):
+        """Text restart of the resident records (Particles::saveAsTxt)."""
+        self._check(self._lib.wacomm_b200_save_text(self._ctx, str(path).encode()))
+
+    def save_netcdf(self, path, checkpoint_time, **meta):
+        """NetCDF history/restart of the resident records (Particles::saveAsNetCDF); meta are
+        history.history_meta's keywords. Returns the number of records stored."""
+        from .history import history_meta
+        m = history_meta(checkpoint_time, **meta)
+        written = ctypes.c_size_t()
+        self._check(self._lib.wacomm_b200_save_netcdf(self._ctx, str(path).encode(),
+                                                       ctypes.byref(m), ctypes.byref(written)))
+        return written.value
+
     def geo_positions(self):
         """(depth, lat, lon) float64 arrays of the resident records (kji2deplatlon)."""
         n = self.count()
