@@ -17,6 +17,7 @@ the rates are printed for the design notes.
 """
 import ctypes
 import os
+import time
 
 import numpy as np
 import pytest
@@ -132,3 +133,70 @@ def test_reference_kernel_against_this_library(cuda_device):
     # variation), the FP32 step is far ahead
     assert dropin_ms * 1.3 < ref_ms and noalloc_ms * 1.3 < ref_ms
     assert fp32_ms * 4 < ref_ms
+
+
+def _reference_staged():
+    if not os.path.exists(ob.REF_CUDA_SO):
+        return None
+    fn = ctypes.CDLL(ob.REF_CUDA_SO).ref_cuda_interval_staged
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 6 + \
+                  [ctypes.c_void_p] * 11 + [ctypes.c_int]
+    return fn
+
+
+def test_reference_staged_interval_against_the_host_buffer_entry(cuda_device):
+    """One interval end to end from host records, on the same window and particles: the reference's
+    own per-interval GPU staging around its kernel (Wacomm.cpp:386-660: allocate and upload the
+    whole forcing window, upload the records, move, download, free; restated in the oracle's
+    shim) against this library's host-buffer entry (window resident, one new forcing record
+    uploaded per interval, records streamed in slabs), with pageable host records on both sides.
+    The reference-arithmetic run must reproduce the reference's records."""
+    fn = _reference_staged()
+    if fn is None:
+        pytest.skip("reference kernel build absent")
+    win = syn.config1_window(n_frames=25)
+    cfg = default_config(random=False)
+    parts = syn.uniform_particles(N, win.eta, win.xi, seed=3)
+    f64 = lambda a: np.ascontiguousarray(a, np.float64)
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    fields = [f64(win.times), f64(win.mask), f64(win.lonRad), f64(win.latRad),
+              f64(win.depthIntervals), f64(win.h), f32(win.zeta), f32(win.u), f32(win.v),
+              f32(win.w), f32(win.akt)]
+    cfg_bytes = np.frombuffer(bytearray(bytes(cfg)), np.uint8)
+    head = [win.T, win.sW, win.sRho, win.eta, win.xi]
+
+    def reference():
+        host = parts.copy()
+        t0 = time.perf_counter()
+        assert fn(cfg_bytes.ctypes.data, host.ctypes.data, INTERVAL, *head,
+                  *[a.ctypes.data for a in fields], N) == 0
+        return time.perf_counter() - t0, host
+
+    ref_s, want = min((reference() for _ in range(3)), key=lambda r: r[0])
+    frame = {k: np.ascontiguousarray(v) for k, v in win.frame(INTERVAL + 2).items()
+             if k in ("zeta", "u", "v", "w", "akt")}
+    ours = {}
+    for arithmetic in ("reference", "fp32"):
+        with Engine(cuda_device, semantics="device", arithmetic=arithmetic) as e:
+            e.set_config(cfg)
+            e.load_window(win)
+            best = None
+            for _ in range(4):
+                host = parts.copy()
+                t0 = time.perf_counter()
+                e.upload_frame(INTERVAL + 2, **frame)
+                e.move_interval_host(INTERVAL, host)
+                dt = time.perf_counter() - t0
+                best = dt if best is None else min(best, dt)
+            ours[arithmetic] = (best, host)
+    d = max(float(np.abs(ours["reference"][1][f] - want[f]).max()) for f in ("i", "j", "k"))
+    assert d <= 1e-7, d
+    steps = N * SUBSTEPS
+    rate = lambda s: steps / s
+    print(f"\nreference staged interval (window + records up, move, records down): "
+          f"{ref_s * 1e3:.1f} ms ({rate(ref_s):.3g} particle-steps/s); host-buffer entry, "
+          f"reference arithmetic: {ours['reference'][0] * 1e3:.1f} ms "
+          f"({ref_s / ours['reference'][0]:.1f}x); FP32 step: {ours['fp32'][0] * 1e3:.1f} ms "
+          f"({rate(ours['fp32'][0]):.3g}, {ref_s / ours['fp32'][0]:.1f}x)")
+    assert ours["fp32"][0] * 4 < ref_s
