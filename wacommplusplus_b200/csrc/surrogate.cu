@@ -18,10 +18,10 @@
 //   pipeline, its dependent loads overlap across a full SM of warps instead of stalling the row
 //   warps of the step kernel.
 //
-// Warp roles of the step kernel (320 threads): warps 0-7 own the tile's rows (warp w holds rows
-// 32(w%4).. and columns 128(w/4).. of the accumulator, the TMEM lane quarter it may access), warp
-// 8 streams weights, warp 9 issues the MMAs and owns the TMEM allocation. Every wait is bounded;
-// a timeout raises an error flag and the block drains and exits.
+// Warp roles of the step kernel (576 threads): warps 0-15 own the tile's rows (warp w holds rows
+// 32(w%4).. -- the TMEM lane quarter it may access -- and columns 64(w/4).. of the accumulator),
+// warp 16 streams weights, warp 17 issues the MMAs and owns the TMEM allocation. Every wait is bounded; a timeout raises an error flag and the block drains and
+// exits.
 #include <cstring>
 
 #include <cuda_bf16.h>
@@ -329,7 +329,16 @@ struct StepArgs {
     float4 *rows;     // per work item: layer-4 sums (with b4, before the gate), row tag
 };
 
-constexpr int STEP_THREADS = 320;
+// Row warps in column groups of four TMEM lane quarters, a bulk-copy producer warp and an MMA
+// warp. Group g holds accumulator columns [g GROUP_COLS, (g+1) GROUP_COLS), the last group the rest.
+// Sixteen row warps (four groups of 64 columns, 96 registers) run 9 % faster than eight (two
+// groups of 128, 132 registers) and 3 % faster than twelve: the row work per thread shrinks and
+// each scheduler holds four row warps instead of two.
+constexpr int ROW_WARPS = 16, ROW_THREADS = ROW_WARPS * 32, GROUPS = ROW_WARPS / 4;
+constexpr int PRODUCER_WARP = ROW_WARPS, MMA_WARP = ROW_WARPS + 1;
+constexpr int STEP_THREADS = ROW_THREADS + 64;
+constexpr int GROUP_COLS = (HID / 32 + GROUPS - 1) / GROUPS * 32;
+constexpr int LAST_GROUP_COLS = HID - (GROUPS - 1) * GROUP_COLS;
 constexpr int WRING = 2;
 constexpr uint32_t A_BYTES = HID_KB * KBLOCK_A;  // 64 KB: one tile's activations
 constexpr size_t STEP_SMEM = 2 * (size_t)A_BYTES + WRING * (size_t)KBLOCK_W + 1024;
@@ -407,7 +416,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
     __shared__ int abortFlag, rowStop;
     __shared__ __align__(16) float w1ps[HID * 4];  // read as float4 per hidden unit
     __shared__ float b2s[HID], b3s[HID], w4s[3 * HID], b4s[4];
-    __shared__ float red[TILE * 3];
+    __shared__ float red[GROUPS - 1][TILE * 3];  // layer-4 partial sums of column groups 1..
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         for (int s = 0; s < WRING; s++) {
@@ -436,7 +445,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
         for (int c = tid; c < 3 * HID; c += STEP_THREADS) w4s[c] = w4[c];
         if (tid < 3) b4s[tid] = b4[tid];
     }
-    if (warp == 9) tmem_alloc(&tmemSlot, 512);
+    if (warp == MMA_WARP) tmem_alloc(&tmemSlot, 512);
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
@@ -445,7 +454,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
     const int nT = blockIdx.x < nTiles ? (int)((nTiles - 1 - blockIdx.x) / gridDim.x + 1) : 0;
     const uint32_t idesc = idesc_bf16(TILE, HID);
 
-    if (warp == 8) {
+    if (warp == PRODUCER_WARP) {
         // ---------------------------------------------------------- weight producer
         if (lane == 0) {
             int issued0 = -1, issued1 = -1;
@@ -467,7 +476,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             if (issued1 >= 0) mbar_wait_bounded(&full[1], (uint32_t)issued1 & 1);
         }
         __syncwarp();
-    } else if (warp == 9) {
+    } else if (warp == MMA_WARP) {
         // ---------------------------------------------------------- MMA issuer
         if (lane == 0) {
             uint32_t g = 0;
@@ -494,18 +503,19 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
         }
         __syncwarp();
     } else {
-        // ---------------------------------------------------------- rows (warps 0-7)
-        const int quarter = warp & 3, half = warp >> 2;
+        // ---------------------------------------------------------- rows (warps 0-11)
+        const int quarter = warp & 3, group = warp >> 2;
         const int r = quarter * 32 + lane;
         const uint32_t tlane = (uint32_t)(quarter * 32) << 16;
-        const int cBase = half * 128;
+        const int cBase = group * GROUP_COLS;
+        const int chunks = (group == GROUPS - 1 ? LAST_GROUP_COLS : GROUP_COLS) / 32;  // TMEM loads
         const double T0 = a.start, T1 = a.start + a.length;
         const double kLower = -a.sW + 2;
         auto tileOf = [&](int x) { return (long long)blockIdx.x + (long long)x * gridDim.x; };
         auto arrive = [&](int buf) {
             fence_async_shared();
             fence_before_sync();
-            named_sync(1, 256);
+            named_sync(1, ROW_THREADS);
             if (tid == 0) mbar_arrive(&aFull[buf]);
         };
 
@@ -560,13 +570,13 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             uint8_t *A = sA0 + (x & 1) * A_BYTES;
             const uint4 *zrow = reinterpret_cast<const uint4 *>(a.z + (size_t)tag.cl * HID + cBase);
 #pragma unroll 1
-            for (int q0 = 0; q0 < 16; q0 += 8) {
-                uint4 zz[8];
+            for (int q0 = 0; q0 < chunks * 4; q0 += 4) {
+                uint4 zz[4];
 #pragma unroll
-                for (int q = 0; q < 8; q++)
+                for (int q = 0; q < 4; q++)
                     zz[q] = tag.status == ROW_RUN ? __ldg(zrow + q0 + q) : make_uint4(0, 0, 0, 0);
 #pragma unroll
-                for (int q = 0; q < 8; q++) {
+                for (int q = 0; q < 4; q++) {
                     uint4 out = make_uint4(0, 0, 0, 0);
                     if (tag.status == ROW_RUN) {
                         const __half2 *hz = reinterpret_cast<const __half2 *>(&zz[q]);
@@ -605,7 +615,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             uint8_t *A = sA0 + buf * A_BYTES;
             const uint32_t acc = tmem + (uint32_t)(buf * HID) + tlane;
 #pragma unroll 1
-            for (int t = 0; t < 4; t++) {
+            for (int t = 0; t < chunks; t++) {
                 const int c0 = cBase + 32 * t;
                 float v[32];
                 tmem_ld32(acc + (uint32_t)c0, v);
@@ -624,8 +634,8 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             return ok;
         };
 
-        // layer-3 epilogue of tile x with layer 4 folded in; the upper column half leaves its
-        // partial sums in red[]
+        // layer-3 epilogue of tile x with layer 4 folded in; column groups 1.. leave their partial
+        // sums in red[]
         auto epilogue3 = [&](int x, float &o0, float &o1, float &o2) {
             const int buf = x & 1;
             const bool ok = mbar_wait(&accFull[buf], 1, &abortFlag);
@@ -634,7 +644,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             const uint32_t acc = tmem + (uint32_t)(buf * HID) + tlane;
             o0 = o1 = o2 = 0.f;
 #pragma unroll 1
-            for (int t = 0; t < 4; t++) {
+            for (int t = 0; t < chunks; t++) {
                 const int c0 = cBase + 32 * t;
                 float v[32];
                 tmem_ld32(acc + (uint32_t)c0, v);
@@ -646,13 +656,14 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                     o2 = fmaf(h, w4s[2 * HID + c0 + c], o2);
                 }
             }
-            if (half == 1) {
-                red[r * 3 + 0] = o0;
-                red[r * 3 + 1] = o1;
-                red[r * 3 + 2] = o2;
+            if (group > 0) {
+                float *mine = red[group - 1];
+                mine[r * 3 + 0] = o0;
+                mine[r * 3 + 1] = o1;
+                mine[r * 3 + 2] = o2;
             }
             fence_before_sync();
-            named_sync(1, 256);
+            named_sync(1, ROW_THREADS);
             return ok;
         };
 
@@ -666,20 +677,26 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             if (k + 1 < nT) epilogue2(k + 1);
             float o0, o1, o2;
             epilogue3(k, o0, o1, o2);
-            if (half == 0 && cur.status != ROW_EMPTY) {
+            if (group == 0 && cur.status != ROW_EMPTY) {
                 // layer-4 sums and the row tag of the work item, for surrogate_post_kernel
                 const int code = cur.status == ROW_RUN
                                      ? cur.cl
                                      : (cur.status == ROW_FALLBACK ? ROW_CODE_FALLBACK : ROW_CODE_NONE);
+                float s0 = o0, s1 = o1, s2 = o2;
+#pragma unroll
+                for (int g = 0; g < GROUPS - 1; g++) {
+                    s0 += red[g][r * 3 + 0];
+                    s1 += red[g][r * 3 + 1];
+                    s2 += red[g][r * 3 + 2];
+                }
                 a.rows[tileOf(k) * TILE + r] =
-                    make_float4(o0 + red[r * 3 + 0] + b4s[0], o1 + red[r * 3 + 1] + b4s[1],
-                                o2 + red[r * 3 + 2] + b4s[2], __int_as_float(code));
+                    make_float4(s0 + b4s[0], s1 + b4s[1], s2 + b4s[2], __int_as_float(code));
             }
             if (k + 2 < nT) after = prologue(k + 2, ahead);
             // uniform stop decision of the row warps
-            named_sync(1, 256);
+            named_sync(1, ROW_THREADS);
             if (tid == 0) rowStop = abortFlag;
-            named_sync(1, 256);
+            named_sync(1, ROW_THREADS);
             if (rowStop) break;
             cur = next;
             next = after;
@@ -687,7 +704,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
     }
     fence_before_sync();
     __syncthreads();
-    if (warp == 9) {
+    if (warp == MMA_WARP) {
         fence_after_sync();
         tmem_dealloc(tmem, 512);
     }
