@@ -145,3 +145,28 @@ def test_writer_rates(cuda_device, tmp_path):
           f"{n / t_txt:.3g} records/s; oracle one-thread text loop: "
           f"{len(sample) / t_oracle:.3g} records/s")
     assert kept > 0
+
+
+def test_writers_with_no_records_and_their_errors(cuda_device, tmp_path):
+    """No resident records: a header-only text restart and an empty history. A history without
+    the kji2deplatlon grid, or a path that cannot be written, is an error, not a partial file."""
+    from wacommplusplus_b200._native import ERR_IO, ERR_STATE, WacommError
+    win, recs, cfg, _ = _setting(10)
+    with Engine(cuda_device) as e:
+        e.load_window(win)
+        e.set_config(cfg)
+        e.set_particles(recs[:0])
+        with pytest.raises(WacommError) as err:
+            e.save_netcdf(tmp_path / "nogeo.nc", 0.0, **META)
+        assert err.value.code == ERR_STATE
+        e.set_geo_grid(win.lon, win.lat, win.sWValues)
+        e.save_text(tmp_path / "none.txt")
+        assert (tmp_path / "none.txt").read_bytes() == b"\t0\n"
+        assert len(history.load_txt(tmp_path / "none.txt")) == 0
+        assert e.save_netcdf(tmp_path / "none.nc", 1.0, **META) == 0
+        assert oh.read_cdf(tmp_path / "none.nc")["dims"][0] == ("particles", 0)
+        e.set_particles(recs)
+        for call in (lambda p: e.save_text(p), lambda p: e.save_netcdf(p, 0.0, **META)):
+            with pytest.raises(WacommError) as err:
+                call(tmp_path / "missing-dir" / "x")
+            assert err.value.code == ERR_IO
