@@ -150,3 +150,19 @@ def test_not_a_classic_file_is_refused(tmp_path):
     with pytest.raises(WacommError) as e:
         history.load_netcdf(path, "ROMS")
     assert "nccopy" in str(e.value)
+
+
+def test_restart_header_larger_than_its_file_is_refused(tmp_path):
+    """A header that claims more records than the file holds is an error, not an allocation of
+    the claimed size."""
+    path = tmp_path / "restart.nc"
+    oh.reference_test_restart(path)
+    raw = bytearray(path.read_bytes())
+    # CDF-5: magic, numrecs, NC_DIMENSION tag, dimension count, name length, "particles" (12 B)
+    at = 4 + 8 + 4 + 8 + 8 + 12
+    assert int.from_bytes(raw[at:at + 8], "big") == 1
+    raw[at:at + 8] = (10 ** 12).to_bytes(8, "big")
+    path.write_bytes(bytes(raw))
+    with pytest.raises(WacommError) as e:
+        history.load_netcdf(path, "ROMS", random_seed=SEED)
+    assert e.value.code == ERR_IO

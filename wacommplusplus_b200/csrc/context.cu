@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -1326,8 +1327,32 @@ int wacomm_b200_geo_positions(wacomm_b200_context *ctx, double *depth, double *l
     return WACOMM_B200_OK;
 }
 
+static int save_text_impl(wacomm_b200_context *ctx, const char *path);
+static int save_netcdf_impl(wacomm_b200_context *ctx, const char *path,
+                            const wacomm_b200_history_meta *meta, size_t *written);
+
+// The host buffers of the writers are as large as the resident records: an allocation failure
+// ends as an error status, not an exception through the C boundary.
 int wacomm_b200_save_text(wacomm_b200_context *ctx, const char *path) {
     if (!ctx || !path) return WACOMM_B200_ERR_ARGUMENT;
+    try {
+        return save_text_impl(ctx, path);
+    } catch (const std::exception &e) {
+        return fail(ctx, WACOMM_B200_ERR_IO, "text restart: %s", e.what());
+    }
+}
+
+int wacomm_b200_save_netcdf(wacomm_b200_context *ctx, const char *path,
+                            const wacomm_b200_history_meta *meta, size_t *written) {
+    if (!ctx || !path || !meta) return WACOMM_B200_ERR_ARGUMENT;
+    try {
+        return save_netcdf_impl(ctx, path, meta, written);
+    } catch (const std::exception &e) {
+        return fail(ctx, WACOMM_B200_ERR_IO, "NetCDF history: %s", e.what());
+    }
+}
+
+static int save_text_impl(wacomm_b200_context *ctx, const char *path) {
     cudaSetDevice(ctx->device);
     std::vector<wacomm_b200_particle> host(ctx->n);
     if (ctx->n) {
@@ -1343,9 +1368,8 @@ int wacomm_b200_save_text(wacomm_b200_context *ctx, const char *path) {
     return WACOMM_B200_OK;
 }
 
-int wacomm_b200_save_netcdf(wacomm_b200_context *ctx, const char *path,
+static int save_netcdf_impl(wacomm_b200_context *ctx, const char *path,
                             const wacomm_b200_history_meta *meta, size_t *written) {
-    if (!ctx || !path || !meta) return WACOMM_B200_ERR_ARGUMENT;
     if (written) *written = 0;
     if (!ctx->hasConfig) return fail(ctx, WACOMM_B200_ERR_STATE, "set_config has not been called");
     if (!ctx->hasGeo) return fail(ctx, WACOMM_B200_ERR_STATE, "set_geo_grid has not been called");

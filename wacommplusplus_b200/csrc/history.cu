@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
@@ -565,6 +566,10 @@ bool first_column(const CdfFile &f, const CdfVar &v, uint64_t count, std::vector
     if (inner == 0) return false;
     const bool rec = f.record(v);
     const uint64_t stride = rec ? f.recsize() : inner * (uint64_t)size;
+    // the whole column must lie in the file before anything is sized from the header's counts
+    if (count > 0 && (stride == 0 || v.begin > f.bytes.size() ||
+                      (count - 1) > (f.bytes.size() - v.begin) / stride))
+        return false;
     out.resize(count);
     for (uint64_t r = 0; r < count; r++) {
         const uint64_t at = v.begin + r * stride;
@@ -765,17 +770,27 @@ cudaError_t history_pack(const ParticleSoA &S, int n, const uint32_t *flags,
 
 // ------------------------------------------------------------------ context-free file entries
 
+// Exceptions (allocation, thread creation) end as an error status at the C boundary.
+template <class Fn>
+static int guarded(Fn fn) {
+    try {
+        return fn();
+    } catch (const std::exception &e) {
+        return wb::file_fail(std::string("file call failed: ") + e.what());
+    }
+}
+
 extern "C" int wacomm_b200_text_write(const char *path, const wacomm_b200_particle *records,
                                       size_t n) {
     if (!path || (n && !records)) return wb::file_fail("null path or records");
-    return wb::history_text_write(path, records, n);
+    return guarded([&] { return wb::history_text_write(path, records, n); });
 }
 
 extern "C" int wacomm_b200_text_read(const char *path, wacomm_b200_particle *records,
                                      size_t capacity, size_t *n) {
     if (!path || !n) return wb::file_fail("null path or count");
     std::vector<wacomm_b200_particle> got;
-    int rc = wb::history_text_read(path, got);
+    int rc = guarded([&] { return wb::history_text_read(path, got); });
     if (rc) return rc;
     *n = got.size();
     if (!records) return WACOMM_B200_OK;
@@ -793,7 +808,7 @@ extern "C" int wacomm_b200_netcdf_read(const char *path, const wacomm_b200_resta
     std::vector<wacomm_b200_particle> got;
     double checkpoint = 0;
     bool has = false;
-    int rc = wb::history_netcdf_read(path, *expect, got, checkpoint, has);
+    int rc = guarded([&] { return wb::history_netcdf_read(path, *expect, got, checkpoint, has); });
     if (rc) return rc;
     *n = got.size();
     if (checkpoint_time) *checkpoint_time = has ? checkpoint : 0.0;
