@@ -89,6 +89,12 @@ struct wacomm_b200_context {
     size_t binsCap = 0;
     uint32_t *dScanTemp = nullptr;
     size_t scanTempCap = 0;
+    // The second compute lane of the host-buffer path: its stream and sort scratch, swapped in for
+    // the slabs it runs (LaneSwap).
+    cudaStream_t stream2 = nullptr;
+    uint32_t *dHist2 = nullptr, *dOffsets2 = nullptr, *dScanTemp2 = nullptr;
+    size_t binsCap2 = 0, scanTempCap2 = 0;
+    cudaEvent_t evLaneStart = nullptr, evLaneDone = nullptr;
     uint32_t *dCount = nullptr;  // scratch word (compaction result)
 
     wacomm_b200_particle *dAos = nullptr;
@@ -760,6 +766,9 @@ int wacomm_b200_context_create(int device, wacomm_b200_context **out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->evLaneStart, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->evLaneDone, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->evComputeMark, cudaEventDisableTiming);
@@ -813,6 +822,9 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     cudaFree(ctx->dHist);
     cudaFree(ctx->dOffsets);
     cudaFree(ctx->dScanTemp);
+    cudaFree(ctx->dHist2);
+    cudaFree(ctx->dOffsets2);
+    cudaFree(ctx->dScanTemp2);
     cudaFree(ctx->dCount);
     cudaFree(ctx->dAos);
     cudaFree(ctx->dConc);
@@ -847,6 +859,9 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
     if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
+    if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
+    if (ctx->evLaneStart) cudaEventDestroy(ctx->evLaneStart);
+    if (ctx->evLaneDone) cudaEventDestroy(ctx->evLaneDone);
     delete ctx;
     return WACOMM_B200_OK;
 }
@@ -1138,6 +1153,32 @@ int wacomm_b200_move_interval(wacomm_b200_context *ctx, int time_index) {
     return WACOMM_B200_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Runs the enclosed slab work on the second compute lane: its stream and sort scratch take the
+// place of the main ones until the guard ends.
+struct LaneSwap {
+    wacomm_b200_context *ctx;
+    bool active;
+    LaneSwap(wacomm_b200_context *c, bool second) : ctx(c), active(second) { swap(); }
+    ~LaneSwap() { swap(); }
+    void swap() {
+        if (!active) return;
+        std::swap(ctx->stream, ctx->stream2);
+        std::swap(ctx->dHist, ctx->dHist2);
+        std::swap(ctx->dOffsets, ctx->dOffsets2);
+        std::swap(ctx->binsCap, ctx->binsCap2);
+        std::swap(ctx->dScanTemp, ctx->dScanTemp2);
+        std::swap(ctx->scanTempCap, ctx->scanTempCap2);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
 int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
                                    wacomm_b200_particle *particles, size_t n) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
@@ -1186,6 +1227,12 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
     const bool walk = sorts && ctx->seqBounds == bounds;
     if (sorts) ctx->seqBounds.clear();
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    // Slab s runs on compute lane s % 2 (LaneSwap), the last two on the main lane: the next
+    // slab's conversion, sort and move fill the SMs that the previous slab's move releases in its
+    // last wave. The second lane starts after the work enqueued so far on the main stream (the
+    // forcing pair of the interval).
+    CUDA_TRY(ctx, cudaEventRecord(ctx->evLaneStart, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream2, ctx->evLaneStart, 0));
     for (int s = 0; s < slabs; s++) {
         size_t off = bounds[s], cnt = bounds[s + 1] - bounds[s];
         if (cnt == 0) continue;
@@ -1197,6 +1244,13 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
     for (int s = 0; s < slabs; s++) {
         size_t off = bounds[s], cnt = bounds[s + 1] - bounds[s];
         if (cnt == 0) continue;
+        // the ramp-down slabs (the last three) run on the main lane after both lanes are done,
+        // in order, so that each download overlaps the next slab's move
+        if (s == slabs - 3 && s > 0) {
+            CUDA_TRY(ctx, cudaEventRecord(ctx->evLaneDone, ctx->stream2));
+            CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->evLaneDone, 0));
+        }
+        LaneSwap lane(ctx, (s & 1) != 0 && s < slabs - 3);
         CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, up[s], 0));
         ParticleSoA S = offset_soa(ctx->S.s, off);
         CUDA_TRY(ctx, aos_to_soa(ctx->dAos + off, (int)cnt, S, ctx->stream));
@@ -1215,6 +1269,8 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
                                       ctx->d2h));
     }
     if (sorts) ctx->seqBounds = bounds;
+    CUDA_TRY(ctx, cudaEventRecord(ctx->evLaneDone, ctx->stream2));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->evLaneDone, 0));
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     CUDA_TRY(ctx, accumulate_steps(ctx->dSteps, ctx->dSteps + 1, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->d2h));
