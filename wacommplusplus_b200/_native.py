@@ -119,6 +119,8 @@ SIGNATURES = {
     "wacomm_b200_netcdf_read": (_i, [ctypes.c_char_p, ctypes.POINTER(restart_expect_t), _vp, _sz,
                                      ctypes.POINTER(_sz), _dp, ctypes.POINTER(_i)]),
     "wacomm_b200_file_error": (ctypes.c_char_p, []),
+    "wacomm_b200_mlp_train_work_floats": (_sz, [_i]),
+    "wacomm_b200_mlp_train_step": (_i, [_vp] * 4 + [_i] + [_vp] * 6 + [_i, ctypes.c_float, _i, _vp]),
 }
 
 _lib = None

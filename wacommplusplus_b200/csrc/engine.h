@@ -234,6 +234,13 @@ cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const M
 cudaError_t surrogate_dry_prefix(const double *mask, const double *h, double shore, int eta, int xi,
                                  int *pre, cudaStream_t stream);
 
+// mlp_train.cu ----------------------------------------------------------------------------
+size_t mlp_train_work_floats(int batch);
+cudaError_t mlp_train_step(const float *stencil, const float *particle, const float *gate,
+                           const float *target, int batch, float *params, float *grads, float *m,
+                           float *v, float *work, float *loss, int step, float lr, bool update,
+                           cudaStream_t stream);
+
 // history.cu ------------------------------------------------------------------------------
 
 // Text restart of n host records (Particles.cpp:28-55) / the records of a text restart

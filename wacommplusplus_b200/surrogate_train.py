@@ -10,7 +10,9 @@ placed uniformly over seeded synthetic forcing windows -- ROMS-shaped streamfunc
 the analytic grid with random velocities -- a quarter of them released inside the interval.
 Segments whose start or end is within two cells of the grid edge or at a vertical bound are
 dropped (the surrogate hands those cases to the closures or to the plain kernel). Features and
-targets follow ``surrogate.py``; the loss is the mean squared error of the scaled residual.
+targets follow ``surrogate.py``; the loss is the mean squared error of the scaled residual. The
+network is trained by the library's own kernels (wacomm_b200_mlp_train_step: forward, loss,
+backward and Adam in FP32 on the device); torch holds the data and the device buffers.
 """
 import argparse
 import math
@@ -18,6 +20,7 @@ import time
 
 import numpy as np
 
+from . import _native
 from . import surrogate as sg
 from . import synthetic as syn
 from .engine import Engine
@@ -132,56 +135,97 @@ def generate(torch, engine, cfg, seed, n_realistic, n_uniform, frames, per_inter
     return torch.cat(feats), torch.cat(parts), torch.cat(res)
 
 
-class Net:
-    def __init__(self, torch, seed):
-        w = sg.random_weights(seed, scale=1.0)
-        for k in ("b1", "b2", "b3", "b4"):
-            w[k][:] = 0
-        w["w4"] *= 0.1
-        self.p = {k: torch.tensor(v, device="cuda", requires_grad=True) for k, v in w.items()}
+def initial_weights(seed):
+    """He-style weights with zero biases and a small last layer: the correction starts near zero."""
+    w = sg.random_weights(seed, scale=1.0)
+    for k in ("b1", "b2", "b3", "b4"):
+        w[k][:] = 0
+    w["w4"] *= 0.1
+    return w
 
-    def forward(self, torch, S, P, G):
-        p = self.p
-        h = sg.gelu(S @ p["w1"][:, :sg.N_STENCIL].T + P @ p["w1"][:, sg.N_STENCIL:].T + p["b1"])
-        h = sg.gelu(h @ p["w2"].T + p["b2"])
-        h = sg.gelu(h @ p["w3"].T + p["b3"])
-        return (h @ p["w4"].T + p["b4"]) * G[:, None]
+
+class KernelTrainer:
+    """Training of the MLP with the library's own kernels (wacomm_b200_mlp_train_step: forward,
+    loss, backward, Adam, FP32 on the device); torch only holds the device buffers."""
+
+    def __init__(self, torch, weights, batch):
+        self.torch, self.lib, self.batch = torch, _native.lib(), batch
+        flat = np.concatenate([np.asarray(weights[k], np.float32).reshape(-1)
+                               for k, _ in sg.PARAMETERS])
+        self.params = torch.tensor(flat, device="cuda")
+        self.grads = torch.zeros_like(self.params)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.work = torch.empty(self.lib.wacomm_b200_mlp_train_work_floats(batch),
+                                dtype=torch.float32, device="cuda")
+        self.loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        self.step = 0
+
+    def run(self, S, P, G, R, lr=0.0, update=True):
+        """One step on a batch of at most ``batch`` rows (float32 device tensors); returns the
+        device loss of the batch (before the update)."""
+        n = len(S)
+        assert 0 < n <= self.batch
+        S, P, G, R = (x.float().contiguous() for x in (S, P, G, R))
+        if update:
+            self.step += 1
+        status = self.lib.wacomm_b200_mlp_train_step(
+            S.data_ptr(), P.data_ptr(), G.data_ptr(), R.data_ptr(), n, self.params.data_ptr(),
+            self.grads.data_ptr(), self.m.data_ptr(), self.v.data_ptr(), self.work.data_ptr(),
+            self.loss.data_ptr(), max(self.step, 1), float(lr), int(update),
+            self.torch.cuda.current_stream().cuda_stream)
+        if status != 0:
+            raise RuntimeError(f"wacomm_b200_mlp_train_step failed ({status})")
+        return self.loss.clone()
+
+    def weights(self):
+        flat, out, at = self.params.cpu().numpy(), {}, 0
+        for name, shape in sg.PARAMETERS:
+            size = int(np.prod(shape))
+            out[name] = flat[at:at + size].reshape(shape).copy()
+            at += size
+        return out
+
+    def evaluate(self, S, P, G, R):
+        """Mean loss over a set, in batches, without updating."""
+        total = 0.0
+        for c in range(0, len(S), self.batch):
+            k = min(self.batch, len(S) - c)
+            total += float(self.run(S[c:c + k], P[c:c + k], G[c:c + k], R[c:c + k],
+                                    update=False)) * k
+        return total / len(S)
+
+
+def gates(torch, S):
+    return torch.cat([sg.uniformity_gate(S[c:c + (1 << 20)].float()) for c in range(0, len(S), 1 << 20)])
 
 
 def train(torch, S, P, R, epochs, batch, lr, seed):
-    net = Net(torch, seed)
-    G = torch.cat([sg.uniformity_gate(S[c:c + (1 << 20)].float()) for c in range(0, len(S), 1 << 20)])
+    G = gates(torch, S)
     print(f"  gate: {float((G < 1).float().mean()):.3f} of segments below 1, "
           f"{float((G == 0).float().mean()):.3f} at 0", flush=True)
-    opt = torch.optim.Adam(net.p.values(), lr=lr)
+    trainer = KernelTrainer(torch, initial_weights(seed), batch)
     n = len(S)
     steps = epochs * (n // batch)
-    sched = torch.optim.lr_scheduler.LambdaLR(opt, lambda s: 0.5 * (1 + math.cos(math.pi * min(s, steps) / steps)))
     hold = torch.randperm(n, device="cuda")[: min(n // 50, 200000)]
     mask = torch.ones(n, dtype=torch.bool, device="cuda")
     mask[hold] = False
     train_idx = torch.nonzero(mask).flatten()
+    s = 0
     for epoch in range(epochs):
         perm = train_idx[torch.randperm(len(train_idx), device="cuda")]
         t0 = time.time()
-        tot = 0.0
+        tot = torch.zeros(1, device="cuda")
         for b in range(len(perm) // batch):
             ix = perm[b * batch:(b + 1) * batch]
-            with torch.autocast("cuda", dtype=torch.bfloat16):
-                y = net.forward(torch, S[ix].float(), P[ix], G[ix])
-            loss = torch.mean((y.float() - R[ix]) ** 2)
-            opt.zero_grad(set_to_none=True)
-            loss.backward()
-            opt.step()
-            sched.step()
-            tot += float(loss.detach())
-        with torch.no_grad():
-            y = net.forward(torch, S[hold].float(), P[hold], G[hold])
-            val = torch.mean((y - R[hold]) ** 2).item()
-            base = torch.mean(R[hold] ** 2).item()
-        print(f"  epoch {epoch}: train {tot / max(1, len(perm) // batch):.4g} held-out {val:.4g} "
-              f"(zero-residual baseline {base:.4g}) {time.time() - t0:.1f}s", flush=True)
-    return {k: v.detach().float().cpu().numpy() for k, v in net.p.items()}
+            rate = lr * 0.5 * (1 + math.cos(math.pi * min(s, steps) / steps))
+            tot += trainer.run(S[ix], P[ix], G[ix], R[ix], rate)
+            s += 1
+        val = trainer.evaluate(S[hold], P[hold], G[hold], R[hold])
+        base = torch.mean(R[hold].float() ** 2).item()
+        print(f"  epoch {epoch}: train {float(tot) / max(1, len(perm) // batch):.4g} held-out "
+              f"{val:.4g} (zero-residual baseline {base:.4g}) {time.time() - t0:.1f}s", flush=True)
+    return trainer.weights()
 
 
 def evaluate(weights, n_particles=32768, hours=24, seed=1, realistic=False):
