@@ -714,7 +714,9 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
 // Displacement, closures and state update of one work item from its layer-4 sums and row tag
 // (rows[n], written by surrogate_step_kernel): one thread per item, so that the dependent loads
 // of the particle state, the corner record and the dry-node table overlap across many warps.
-__global__ void __launch_bounds__(256) surrogate_post_kernel(const StepArgs a, ParticleSoA S,
+// Five blocks per SM (48 registers, 20 bytes of spill): the dependent gathers overlap across more
+// warps; 0.6 % of the interval faster than four blocks at 64 registers.
+__global__ void __launch_bounds__(256, 5) surrogate_post_kernel(const StepArgs a, ParticleSoA S,
                                                              const MoveLaunch L) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     const double T0 = a.start;
