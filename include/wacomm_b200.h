@@ -331,8 +331,9 @@ int wacomm_b200_get_environment(wacomm_b200_context *ctx, int field, int t, floa
 /* Concentration grid of n_conc_times records [n_conc_times][s_rho][eta][xi] as uint32 counts.
  * reset zeroes it; count adds the resident alive particles at conc_time_index
  * (Concentration.hpp:16-44); get copies it out (uint32) and get_float copies it as the reference
- * float grid, writing 1e37 into land cells (mask != 1) of every level when mask_land is set
- * (Wacomm.cpp:188-196,724-739). */
+ * float grid, writing 1e37 into land cells (mask != 1) of every level when mask_land is set, in
+ * the concentration times counted since the last reset (the solver masks each time it evaluates;
+ * times never counted stay 0, Wacomm.cpp:174-196,722-739). */
 int wacomm_b200_concentration_reset(wacomm_b200_context *ctx, int n_conc_times);
 int wacomm_b200_concentration_count(wacomm_b200_context *ctx, int conc_time_index);
 int wacomm_b200_concentration_get(wacomm_b200_context *ctx, uint32_t *out, size_t n);
@@ -407,11 +408,17 @@ int wacomm_b200_cuda_move_particle(const wacomm_b200_config *config_device,
  * wacomm_b200_cuda_move_particle, whose horizontal-cell ordering it shares, but its working
  * memory (keys, histogram, scan, order) is a fixed array of about 25 MB compiled into the library
  * and held on every GPU that loads it. Limits: particle_count <= 2,097,152 and eta*xi <=
- * 1,048,576; larger calls return -WACOMM_B200_ERR_CAPACITY and do nothing. Otherwise returns 0 or
- * a CUDA error code. Every call on a device shares the array: calls that overlap on the GPU race
- * and must not be issued; calls on one stream are ordered and safe. The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress, with that device current); make it
- * before any stream capture begins. */
+ * 1,048,576 (eta*xi counts only on grids with at least two nodes along each axis; narrower grids
+ * have no interpolation cell and their records are moved in caller order, as the launcher above
+ * does); larger calls return -WACOMM_B200_ERR_CAPACITY and do nothing. Otherwise returns 0 or a
+ * CUDA error code. Every call on a device shares the array: calls that overlap on the GPU race and
+ * must not be issued; calls on one stream are ordered and safe. The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress, with that device current) and the SM
+ * count; under lazy module loading (the CUDA default) it is also the call that loads the library's
+ * kernels and makes the array resident on that device, which allocates and synchronizes once.
+ * Make that first call during set-up, before the allocation-free phase and before any stream
+ * capture begins. The address belongs to the device's context of that moment: a cudaDeviceReset
+ * between calls is not supported. */
 int wacomm_b200_cuda_move_particle_noalloc(const wacomm_b200_config *config_device,
                                            wacomm_b200_particle *particles_device, int time_index,
                                            int ocean_time, int s_w, int s_rho, int eta, int xi,

@@ -109,6 +109,9 @@ def oracle_lib():
         lib.wo_concentration.argtypes = [ctypes.c_void_p, ctypes.c_long, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_void_p]
+        lib.wo_concentration_mask.restype = None
+        lib.wo_concentration_mask.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, _c_double_p]
         lib.wo_source_emission_times.restype = ctypes.c_long
         lib.wo_source_emission_times.argtypes = [ctypes.c_int, d, d, d, d, d, _c_double_p,
                                                  ctypes.c_long]
@@ -212,6 +215,17 @@ def oracle_concentration(particles, conc_time_index, n_times, win):
     conc = np.zeros((n_times, win.sRho, win.eta, win.xi), dtype=np.uint32)
     oracle_lib().wo_concentration(particles.ctypes.data, len(particles), conc_time_index,
                                   n_times, win.sRho, win.eta, win.xi, conc.ctypes.data)
+    return conc
+
+
+def oracle_concentration_float(counts, evaluated, win):
+    """The solver's float concentration grid from uint32 counts [n_times][sRho][eta][xi]: counts
+    as float, land (mask != 1) set to 1e37 in every level of each evaluated time."""
+    conc = np.ascontiguousarray(counts, dtype=np.float32)
+    mask = np.ascontiguousarray(win.mask, dtype=np.float64)
+    for t in evaluated:
+        oracle_lib().wo_concentration_mask(conc.ctypes.data, int(t), win.sRho, win.eta, win.xi,
+                                           _dptr(mask))
     return conc
 
 

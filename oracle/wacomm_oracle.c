@@ -763,6 +763,20 @@ void wo_concentration(const wo_particle *particles, long n, int concTimeIdx, int
     }
 }
 
+/* The solver's float concentration output: the land cells of the particle grid (mask != 1,
+ * Wacomm.cpp:188-196) get 1e37 in every level of the concentration time just evaluated
+ * (Wacomm.cpp:724-737); counts elsewhere are the float grid Concentration::evaluate filled. */
+void wo_concentration_mask(float *conc, int concTimeIdx, int sRho, int eta, int xi,
+                           const double *mask) {
+    size_t plane = (size_t)eta * (size_t)xi;
+    for (int k = -sRho + 1; k <= 0; k++)
+        for (int j = 0; j < eta; j++)
+            for (int i = 0; i < xi; i++)
+                if (mask[(size_t)j * xi + i] != 1)
+                    conc[((size_t)concTimeIdx * sRho + (size_t)(k + sRho - 1)) * plane +
+                         (size_t)j * xi + i] = 1e37f;
+}
+
 /* ---------------------------------------------------------------- emission schedule */
 
 long wo_source_emission_times(int mode, double value, double sourceStart, double sourceEnd,

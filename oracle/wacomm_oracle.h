@@ -114,6 +114,11 @@ int wo_move_batch(const wo_config *config, wo_particle *particles, long n,
 void wo_concentration(const wo_particle *particles, long n, int concTimeIdx, int Tc, int sRho,
                       int eta, int xi, uint32_t *conc);
 
+/* Land mask of the float concentration grid conc[][sRho][eta][xi] at one evaluated time
+ * (Wacomm.cpp:188-196,724-737): 1e37 in every level of each cell whose mask is not 1. */
+void wo_concentration_mask(float *conc, int concTimeIdx, int sRho, int eta, int xi,
+                           const double *mask);
+
 /* sourceEmissionTimes (SourceEmission.hpp:38-79): mode 0 uniform_rate, 1 forcing_interval_batch,
  * 2 single_pulse. Returns the count (writing at most cap values) or -1 on an invalid schedule. */
 long wo_source_emission_times(int mode, double value, double sourceStart, double sourceEnd,

@@ -127,6 +127,41 @@ def test_fixture_cases_reference_arithmetic(case, rules, engine_host, engine_dev
     assert_close(engine.get_particles(), want, win, what=f"{case['name']} backward")
 
 
+def test_concentration_float_land_mask(engine_host):
+    """The float concentration grid with the land mask (Wacomm.cpp:188-196,724-737): counts as
+    float in water, 1e37 in every level of each land cell of the concentration times evaluated,
+    times never evaluated left at 0; equal, value for value, to the oracle's restatement applied
+    to the oracle's count of the kernel's own positions."""
+    win = syn.config1_window(n_frames=6, eta=64, xi=64, s_rho=10)
+    land = np.zeros((win.eta, win.xi), dtype=bool)
+    land[20:30, 40:52] = True
+    land[50:, :6] = True
+    win.mask = np.where(land, 0.0, 1.0)
+    win.h = np.where(land, 0.0, win.h)
+    p0 = syn.uniform_particles(8192, win.eta, win.xi, seed=7)
+    wet = ~land[np.floor(p0["j"]).astype(int), np.floor(p0["i"]).astype(int)]
+    wet &= ~land[np.floor(p0["j"]).astype(int) + 1, np.floor(p0["i"]).astype(int) + 1]
+    p0 = p0[wet]
+    e = engine_host
+    e.load_window(win)
+    e.set_config(default_config(random=True))
+    e.set_particles(p0)
+    e.concentration_reset(win.T)
+    e.move_interval(0)
+    e.move_interval(1)
+    got = e.get_particles()
+    counts = e.concentration()
+    assert np.array_equal(counts[2], ob.oracle_concentration(got, 2, win.T, win)[2])
+    plain = e.concentration_float(mask_land=False)
+    assert np.array_equal(plain, counts.astype(np.float32))
+    masked = e.concentration_float(mask_land=True)
+    want = ob.oracle_concentration_float(counts, [1, 2], win)
+    assert np.array_equal(masked, want)
+    assert np.all(masked[1:3][:, :, land] == np.float32(1e37))
+    assert np.all(masked[[0, 3, 4, 5]] == 0)
+    assert masked[1:3][:, :, ~land].sum() > 0
+
+
 def _config1(n_particles=16384, frames=6):
     win = syn.config1_window(n_frames=frames)
     return win, syn.uniform_particles(n_particles, win.eta, win.xi, seed=1)

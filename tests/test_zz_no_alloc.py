@@ -75,3 +75,28 @@ def test_noalloc_refuses_sizes_beyond_its_limit(cuda_device):
     status = _native.lib().wacomm_b200_cuda_move_particle_noalloc(
         None, None, 0, win.T, win.sW, win.sRho, 2048, 1024, *([None] * 15), 10, 1, 1, None)
     assert status == -_native.ERR_CAPACITY
+
+
+def test_noalloc_moves_records_of_a_grid_without_cells(cuda_device):
+    """A grid one node wide has no interpolation cell: the allocation-free launcher moves its
+    records in caller order without the cell sort, as the drop-in launcher does (both kill every
+    record on its first substep, before any forcing read)."""
+    T, eta, xi = 2, 1, 5
+    lon = np.linspace(14.0, 14.1, xi)[None, :]
+    lat = np.full((eta, xi), 40.8)
+    win = syn.Window(times=np.array([0.0, 3600.0]), mask=np.ones((eta, xi)), lon=lon, lat=lat,
+                     lonRad=lon * syn.ADAPTER_DEG2RAD, latRad=lat * syn.ADAPTER_DEG2RAD,
+                     h=np.full((eta, xi), 50.0), sWValues=np.array([-1.0, -.5, 0.0]),
+                     depthIntervals=np.array([.5, .5]), zeta=np.zeros((T, eta, xi), np.float32),
+                     u=np.full((T, 2, eta, xi), .2, np.float32),
+                     v=np.zeros((T, 2, eta, xi), np.float32),
+                     w=np.zeros((T, 3, eta, xi), np.float32),
+                     akt=np.full((T, 3, eta, xi), 1e-4, np.float32))
+    p = syn.uniform_particles(300, 2, xi, seed=44)
+    p["j"] = 0.0
+    cfg = default_config(random=True)
+    want = call_dropin(cfg, p, win, 0)
+    got = call_dropin(cfg, p, win, 0, launcher=_noalloc)
+    for f in got.dtype.names:
+        assert np.array_equal(got[f], want[f], equal_nan=True), f
+    assert not np.any(got["health"] > 0)

@@ -102,6 +102,9 @@ struct wacomm_b200_context {
 
     uint32_t *dConc = nullptr;
     int concTimes = 0;
+    // Concentration times counted since the last reset: the float grid masks land in these only,
+    // as the solver masks each time it evaluates (Wacomm.cpp:722-737).
+    std::vector<uint8_t> concEvaluated;
 
     wacomm_b200_source *dSources = nullptr;  // emission: the sources of the last call
     size_t sourcesCap = 0;
@@ -516,6 +519,7 @@ int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t of
     bool count_here = ctx->opt.fuse_concentration && ctx->dConc && concTime >= 0 &&
                       concTime < ctx->concTimes;
     L.conc = count_here ? ctx->dConc : nullptr;
+    if (count_here) ctx->concEvaluated[concTime] = 1;
     L.concTimeIndex = concTime;
     L.concTimes = ctx->concTimes;
     L.steps = ctx->dSteps;
@@ -654,6 +658,7 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     const bool countHere = ctx->opt.fuse_concentration && ctx->dConc && concTime >= 0 &&
                            concTime < ctx->concTimes;
     L.conc = countHere ? ctx->dConc : nullptr;
+    if (countHere) ctx->concEvaluated[concTime] = 1;
     L.concTimeIndex = concTime;
     L.concTimes = ctx->concTimes;
     L.steps = ctx->dSteps;
@@ -1489,6 +1494,7 @@ int wacomm_b200_concentration_reset(wacomm_b200_context *ctx, int n_conc_times) 
         ctx->concTimes = n_conc_times;
     }
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->dConc, 0, cells * sizeof(uint32_t), ctx->stream));
+    ctx->concEvaluated.assign((size_t)n_conc_times, 0);
     return WACOMM_B200_OK;
 }
 
@@ -1500,6 +1506,7 @@ int wacomm_b200_concentration_count(wacomm_b200_context *ctx, int conc_time_inde
     cudaSetDevice(ctx->device);
     CUDA_TRY(ctx, count_concentration(ctx->S.s, (int)ctx->n, conc_time_index, ctx->sRho, ctx->eta,
                                       ctx->xi, ctx->dConc, ctx->stream));
+    ctx->concEvaluated[conc_time_index] = 1;
     return WACOMM_B200_OK;
 }
 
@@ -1533,9 +1540,15 @@ int wacomm_b200_concentration_get_float(wacomm_b200_context *ctx, float *out, si
     cudaSetDevice(ctx->device);
     float *dOut = nullptr;
     CUDA_TRY(ctx, cudaMallocAsync((void **)&dOut, cells * sizeof(float), ctx->stream));
-    cudaError_t e = concentration_to_float(ctx->dConc, cells, ctx->concTimes, ctx->sRho, ctx->eta,
-                                           ctx->xi, mask_land ? ctx->dMask : nullptr, dOut,
-                                           ctx->stream);
+    // one time at a time: land is masked only in the times counted since the last reset
+    const size_t perTime = (size_t)ctx->sRho * ctx->eta * ctx->xi;
+    cudaError_t e = cudaSuccess;
+    for (int t = 0; t < ctx->concTimes && e == cudaSuccess; t++) {
+        const bool mask = mask_land && ctx->concEvaluated[t];
+        e = concentration_to_float(ctx->dConc + t * perTime, perTime, 1, ctx->sRho, ctx->eta,
+                                   ctx->xi, mask ? ctx->dMask : nullptr, dOut + t * perTime,
+                                   ctx->stream);
+    }
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(out, dOut, cells * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
     cudaFreeAsync(dOut, ctx->stream);

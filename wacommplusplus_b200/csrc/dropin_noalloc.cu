@@ -16,16 +16,23 @@
 //
 // Limits: at most NOALLOC_MAX_PARTICLES records and NOALLOC_MAX_CELLS horizontal cells (eta*xi)
 // per call; larger calls are refused with -WACOMM_B200_ERR_CAPACITY before any work. The array
-// (about 25 MB) is held on every GPU that loads the library until the process exits.
+// (about 25 MB) is held on every GPU that loads the library until the process exits. A grid with
+// fewer than two nodes along an axis has no interpolation cell: its records are moved in caller
+// order without the sort (every one of them leaves the grid), as the drop-in launcher does.
 //
 // Sharing: every call on a device uses the same array and leaves its contents behind; the
 // histogram is cleared at the start of each call. Two calls whose work overlaps on the GPU (on
 // different streams, or from different host threads without ordering) race on the array and
 // must not be issued; calls on one stream are ordered and safe.
 //
-// Set-up: the device address of the array is looked up with cudaGetSymbolAddress once per
-// device, with that device current, on the first call made on that device; make that first call
-// before any stream capture begins on the device.
+// Set-up: the first call made on a device, with that device current, looks up the array's
+// device address with cudaGetSymbolAddress and the device's SM count, once; later calls reuse
+// them. Under lazy module loading (the CUDA default) that first call is also the one that loads
+// the library's kernels on the device and makes the array resident there, which allocates device
+// memory and synchronizes once: make it during the caller's own set-up, before its
+// allocation-free phase and before any stream capture begins on the device. The looked-up address
+// belongs to the device's context of that moment; a cudaDeviceReset between calls is not
+// supported.
 //
 // Compiled with -fmad=false like dropin.cu, so the moved records are the same as that entry
 // point's, bit for bit.
@@ -48,23 +55,35 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 // keys[MAXP] | order[MAXP] | histogram[BINS] | offsets[BINS] | scan partials
 static __device__ __align__(256) uint32_t noalloc_scratch[NOALLOC_WORDS];
 
-std::mutex setup_mutex;
-uint32_t *scratch_address[NOALLOC_MAX_DEVICES] = {};
+// What the first call on a device looks up: the array's device address and the SM count that
+// sizes the grid-stride launches.
+struct DeviceSetup {
+    uint32_t *scratch = nullptr;
+    int smCount = 0;
+};
 
-// Device address of noalloc_scratch on the current device (looked up once per device).
-cudaError_t scratch_for_current_device(uint32_t **out) {
+std::mutex setup_mutex;
+DeviceSetup device_setup[NOALLOC_MAX_DEVICES];
+
+// Set-up of the current device (done once per device, on its first call).
+cudaError_t setup_for_current_device(DeviceSetup *out) {
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return e;
     if (device < 0 || device >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(setup_mutex);
-    if (!scratch_address[device]) {
+    DeviceSetup &d = device_setup[device];
+    if (!d.scratch) {
+        int sms = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e != cudaSuccess) return e;
         void *ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, noalloc_scratch);
         if (e != cudaSuccess) return e;
-        scratch_address[device] = static_cast<uint32_t *>(ptr);
+        d.smCount = sms > 0 ? sms : 1;
+        d.scratch = static_cast<uint32_t *>(ptr);
     }
-    *out = scratch_address[device];
+    *out = d;
     return cudaSuccess;
 }
 
@@ -102,7 +121,7 @@ __global__ void noalloc_scatter_kernel(const uint32_t *keys, int n, uint32_t *cu
     }
 }
 
-// The drop-in step over the records in cell order.
+// The drop-in step over the records in cell order (order null: caller order).
 __global__ void __launch_bounds__(256) noalloc_move_kernel(
     const wacomm_b200_config *__restrict__ config, wacomm_b200_particle *particles,
     const uint32_t *__restrict__ order, int timeIndex, int oceanTime,
@@ -116,7 +135,7 @@ __global__ void __launch_bounds__(256) noalloc_move_kernel(
     RawView view = V;
     view.t0 = P.t0;
     view.t1 = P.t1;
-    uint32_t idx = order[t];
+    uint32_t idx = order ? order[t] : (uint32_t)t;
     wacomm_b200_particle rec = particles[idx];
     ParticleState p;
     p.id = rec.id;
@@ -144,7 +163,7 @@ __global__ void __launch_bounds__(256) noalloc_move_kernel(
 
 // See the file comment. Same arguments and meaning as wacomm_b200_cuda_move_particle; returns 0,
 // a CUDA error code, or -WACOMM_B200_ERR_CAPACITY (nothing done) when particle_count exceeds
-// 2,097,152 or eta*xi exceeds 1,048,576.
+// 2,097,152 or eta*xi exceeds 1,048,576 (on a grid with at least two nodes along each axis).
 extern "C" int wacomm_b200_cuda_move_particle_noalloc(
     const wacomm_b200_config *config_device, wacomm_b200_particle *particles_device,
     int time_index, int ocean_time, int s_w, int s_rho, int eta, int xi, const double *times,
@@ -158,31 +177,36 @@ extern "C" int wacomm_b200_cuda_move_particle_noalloc(
     (void)num_thread;
     (void)num_gpu;
     if (particle_count <= 0) return (int)cudaGetLastError();
-    if (particle_count > NOALLOC_MAX_PARTICLES || eta < 2 || xi < 2 ||
-        (size_t)eta * (size_t)xi > (size_t)NOALLOC_MAX_CELLS)
+    const bool sorted = eta >= 2 && xi >= 2;  // else no interpolation cell: caller order
+    if (particle_count > NOALLOC_MAX_PARTICLES ||
+        (sorted && (size_t)eta * (size_t)xi > (size_t)NOALLOC_MAX_CELLS))
         return -WACOMM_B200_ERR_CAPACITY;
-    size_t bins = (size_t)eta * xi + 1;
-    if (scan_temp_words(bins) > NOALLOC_SCAN_WORDS) return -WACOMM_B200_ERR_CAPACITY;
+    size_t bins = sorted ? (size_t)eta * xi + 1 : 0;
+    if (sorted && scan_temp_words(bins) > NOALLOC_SCAN_WORDS) return -WACOMM_B200_ERR_CAPACITY;
     cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
-    uint32_t *scratch = nullptr;
-    cudaError_t e = scratch_for_current_device(&scratch);
+    DeviceSetup setup;
+    cudaError_t e = setup_for_current_device(&setup);
     if (e != cudaSuccess) return (int)e;
-    uint32_t *keys = scratch;
-    uint32_t *order = keys + NOALLOC_MAX_PARTICLES;
-    uint32_t *hist = order + NOALLOC_MAX_PARTICLES;
-    uint32_t *offsets = hist + NOALLOC_BINS;
-    uint32_t *partials = offsets + NOALLOC_BINS;
-
-    int blocks = (particle_count + 255) / 256;
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    int clearBlocks = (int)((bins + 255) / 256);
-    if (clearBlocks > 148 * 16) clearBlocks = 148 * 16;
-    noalloc_clear_kernel<<<clearBlocks, 256, 0, stream>>>(hist, bins);
-    noalloc_key_kernel<<<blocks, 256, 0, stream>>>(particles_device, particle_count, eta, xi, keys,
-                                                   hist);
-    e = exclusive_scan(hist, offsets, bins, offsets + bins, partials, stream);
-    if (e != cudaSuccess) return (int)e;
-    noalloc_scatter_kernel<<<blocks, 256, 0, stream>>>(keys, particle_count, offsets, order);
+    uint32_t *order = nullptr;
+    if (sorted) {
+        uint32_t *keys = setup.scratch;
+        uint32_t *hist = keys + 2 * (size_t)NOALLOC_MAX_PARTICLES;
+        uint32_t *offsets = hist + NOALLOC_BINS;
+        uint32_t *partials = offsets + NOALLOC_BINS;
+        order = keys + NOALLOC_MAX_PARTICLES;
+        // grid-stride kernels: at most 16 blocks of 256 threads per SM
+        const int cap = setup.smCount * 16;
+        int blocks = (particle_count + 255) / 256;
+        if (blocks > cap) blocks = cap;
+        int clearBlocks = (int)((bins + 255) / 256);
+        if (clearBlocks > cap) clearBlocks = cap;
+        noalloc_clear_kernel<<<clearBlocks, 256, 0, stream>>>(hist, bins);
+        noalloc_key_kernel<<<blocks, 256, 0, stream>>>(particles_device, particle_count, eta, xi,
+                                                       keys, hist);
+        e = exclusive_scan(hist, offsets, bins, offsets + bins, partials, stream);
+        if (e != cudaSuccess) return (int)e;
+        noalloc_scatter_kernel<<<blocks, 256, 0, stream>>>(keys, particle_count, offsets, order);
+    }
 
     RawView V;
     V.g = GridShape{eta, xi, s_w, s_rho};
