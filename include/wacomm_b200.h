@@ -136,8 +136,9 @@ typedef struct wacomm_b200_options {
                                  3 blocks/SM; 2 = 256 threads, 2 blocks/SM; 3 = 128 threads,
                                  5 blocks/SM (fewer registers, more resident warps);
                                  WACOMM_B200_LAUNCH_SHAPE_AUTO (default): 3 or 2 by form */
-    int surrogate;            /* 1: deterministic forward intervals by the learned surrogate
-                                 (wacomm_b200_set_surrogate), the rest by the FP32 step */
+    int surrogate;            /* 1: forward intervals by the learned surrogate
+                                 (wacomm_b200_set_surrogate), with the plain stochastic operator
+                                 per substep when the random walk is on; the rest by the FP32 step */
 } wacomm_b200_options;
 
 /* ------------------------------------------------------------------ context */
@@ -244,9 +245,12 @@ int wacomm_b200_move_interval(wacomm_b200_context *ctx, int time_index);
  * holds the particle count, the buffer addresses, the forcing times, the config and the options
  * of the capture: new record values (upload_frame into existing slots, set_particles with the
  * same count, a new batch of scenarios) are picked up by the next launch, while any change of
- * those is refused at launch with WACOMM_B200_ERR_STATE (capture again). Not with the surrogate
- * option (its per-interval timing and statistics are kept per call). last_interval_stats after a
- * launch reports the whole run (device ms, particle-steps). No reference counterpart. */
+ * those is refused at launch with WACOMM_B200_ERR_STATE (capture again). With the surrogate option
+ * the per-cell layer 1, the tensor-core step, the displacement (or walk) kernel and the fallback
+ * step of every interval are captured as well (the fallback step reads its list length on the
+ * device); last_surrogate_stats then gives the counts of the last captured interval, without
+ * kernel times. last_interval_stats after a launch reports the whole run (device ms,
+ * particle-steps). No reference counterpart. */
 int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, int n_intervals);
 int wacomm_b200_graph_launch(wacomm_b200_context *ctx);
 int wacomm_b200_graph_release(wacomm_b200_context *ctx);
@@ -357,6 +361,15 @@ int wacomm_b200_particle_steps_total(wacomm_b200_context *ctx, int reset, double
 /* Statistics of the last move_interval: device milliseconds of all its kernels (CUDA events on
  * the context stream around pack, sort and move), of the move kernel launches alone, how many
  * kernels it launched and how many particle-steps (substeps of active particles) it took. */
+/* Device milliseconds of the dominant kernels of the eager intervals enqueued since the last call
+ * (at most the last 256; captured runs are not included), oldest first, three values per
+ * interval: plain step [move kernel, 0, 0]; surrogate [step kernel (tensor cores), post or walk
+ * kernel, fallback step]. Events are recorded around the kernels of every interval, so intervals
+ * enqueued back to back are timed without a host wait; this call waits for the stream. Writes at
+ * most `capacity` intervals (3 * capacity floats), the newest ones, and their number to *count.
+ * No reference counterpart. */
+int wacomm_b200_kernel_times(wacomm_b200_context *ctx, float *ms, int capacity, int *count);
+
 int wacomm_b200_last_interval_stats(const wacomm_b200_context *ctx, float *device_ms,
                                     float *move_ms, int *kernel_launches, double *particle_steps);
 
@@ -364,9 +377,12 @@ int wacomm_b200_last_interval_stats(const wacomm_b200_context *ctx, float *devic
  * count = 231,939 FP32 values: w1 [256][388] (inputs: the 4x4x4 u, v, w stencil at both records,
  * then jF, iF, kF and the activation fraction), b1 [256], w2 [256][256], b2, w3 [256][256], b3,
  * w4 [3][256], b4 [3]. With the surrogate option on, move_interval moves each active particle of
- * a deterministic forward interval by one MLP evaluation (BF16 tensor-core GEMMs) plus the
- * closures in closed form; random walk, backward tracking, drifting objects, restart-clipped
- * intervals, starts outside the valid cells and paths near dry nodes use the FP32 step. */
+ * a forward interval by one MLP evaluation (BF16 tensor-core GEMMs). Deterministic intervals
+ * apply the displacement with the closures in closed form (paths near dry nodes use the FP32
+ * step); with the random walk on, the displacement is spread evenly over the substeps and the
+ * plain stochastic operator (Particle.cpp:518-533), the vertical cap and the closures run every
+ * substep. Backward tracking, drifting objects, jibing, restart-clipped intervals and starts
+ * outside the valid cells use the FP32 step. */
 int wacomm_b200_set_surrogate(wacomm_b200_context *ctx, const float *parameters, size_t count);
 
 /* Of the last move_interval with the surrogate on: particles it moved, particles handed to the

@@ -107,9 +107,44 @@ def test_graph_launch_refused_after_changes(cuda_device, setting):
     with pytest.raises(WacommError):
         g.graph_launch()
     g.set_options(surrogate=1)
-    g.set_surrogate()
     with pytest.raises(WacommError):
-        g.graph_capture(0, 2)
+        g.graph_capture(0, 2)   # the surrogate option without weights
+    g.close()
+
+
+@pytest.mark.parametrize("random", [False, True])
+def test_graph_of_surrogate_intervals_equals_eager(cuda_device, random):
+    """The learned form needs no host round trip inside an interval (the fallback step reads
+    its list length on the device), so its intervals are captured too: deterministic (closed-form
+    displacement) and diffusive (the plain stochastic operator per substep), with fallback
+    particles (drifting objects) in the same run; captured equals eager bit for bit."""
+    win = syn.config1_window(n_frames=INTERVALS + 2)
+    cfg = default_config(random=random, randomSeed=23, driftModel=1, windU10=6.0, windV10=-2.0,
+                         hasWind=True)
+    parts = batch(30000, 8, win)
+    parts["driftObjectType"][parts["driftObjectType"] % 3 != 0] = 0  # two thirds passive
+
+    def build():
+        e = Engine(0, arithmetic="fp32", storage="fp16", surrogate=1, rng="philox")
+        e.set_config(cfg)
+        e.load_window(win)
+        e.set_surrogate()
+        e.concentration_reset(win.T)
+        e.set_particles(parts)
+        return e
+
+    ref = build()
+    ref_steps = eager(ref)
+    sst = ref.surrogate_stats()
+    assert sst["fallback"] > 0 and sst["run"] > 0
+    g = build()
+    g.graph_capture(0, INTERVALS)
+    g.graph_launch()
+    g.synchronize()
+    assert g.stats()["particle_steps"] == ref_steps > 0
+    assert g.surrogate_stats()["run"] == sst["run"]
+    same(g, ref)
+    ref.close()
     g.close()
 
 

@@ -213,3 +213,164 @@ def test_fused_concentration_and_steps(cuda_device):
     assert st["particle_steps"] == 48900 * 120 + 1000 * 60
     want = ob.oracle_concentration(got, 1, win.T, win)
     assert np.array_equal(conc, want)
+
+
+# ---------------------------------------------------------------- diffusive intervals
+#
+# With the random walk on, the surrogate keeps its deterministic displacement (spread evenly over
+# the substeps) and the plain stochastic operator runs every substep with the plain step's draws,
+# vertical cap and closures (surrogate_walk_kernel). On the uniform flow of the analytic grid the
+# gate zeroes the correction, so the walk is the plain Euler step with the same draws: it must
+# equal the FP64 oracle draw for draw (reference keys), and the FP32 step (Philox streams), to the
+# FP32 rounding of 240 substeps on a cell fraction: 5e-5 grid units at most (7 mm on 150 m cells).
+
+WALK_MAX = 5e-5
+
+
+def walk_engine(win, cfg, rng="reference", storage="fp32"):
+    e = Engine(0, arithmetic="fp32", storage=storage, surrogate=1, rng=rng)
+    e.set_config(cfg)
+    e.load_window(win)
+    e.set_surrogate()
+    return e
+
+
+def land_window(n_frames=3):
+    """The analytic grid with two land blocks (h = 0, mask 0): shore closures every interval."""
+    win = syn.config1_window(n_frames=n_frames)
+    land = np.zeros((win.eta, win.xi), dtype=bool)
+    land[40:70, 60:75] = True
+    land[90:, 100:] = True
+    win.mask = np.where(land, 0.0, 1.0)
+    win.h = np.where(land, 0.0, win.h)
+    return win, land
+
+
+def wet_particles(win, land, n, seed):
+    p = syn.uniform_particles(n, win.eta, win.xi, time=win.times[0], seed=seed)
+    j0, i0 = np.floor(p["j"]).astype(int), np.floor(p["i"]).astype(int)
+    box = land[j0, i0] | land[j0 + 1, i0] | land[j0, i0 + 1] | land[j0 + 1, i0 + 1]
+    p = p[~box]
+    late = np.arange(len(p)) % 5 == 0
+    p["time"][late] = win.times[0] + 1800.0 + 7.0   # released inside the interval
+    return p
+
+
+def near(got, want, bound):
+    """Fraction of records whose k, j, i are within `bound` grid units and whose alive/dead status
+    agrees."""
+    d = np.max(np.stack([np.abs(got[f] - want[f]) for f in ("j", "i", "k")]), axis=0)
+    return np.mean((d <= bound) & ((got["health"] > 0) == (want["health"] > 0)))
+
+
+@pytest.mark.parametrize("scene", ["open", "land"])
+@pytest.mark.parametrize("closure", [1, 2, 3])
+def test_diffusive_walk_matches_the_oracle_draw_for_draw(cuda_device, scene, closure):
+    if scene == "open":
+        win = syn.config1_window(n_frames=3)
+        p = syn.uniform_particles(20000, win.eta, win.xi, time=win.times[0], seed=closure)
+    else:
+        win, land = land_window()
+        p = wet_particles(win, land, 24000, seed=10 + closure)
+    cfg = default_config(random=True, integrator=1, horizontalClosure=closure,
+                         upperClosure=closure, lowerClosure=3, sigma=12.0)
+    e = walk_engine(win, cfg)
+    e.set_particles(p)
+    want = p.copy()
+    for t in (0, 1):
+        e.move_interval(t)
+        ob.oracle_move(cfg, want, win, t, ob.SEMANTICS_HOST, threads=0)
+        stats = e.surrogate_stats()
+        assert stats["fallback"] == 0 and stats["run"] > 0.9 * len(p)
+    got = e.get_particles()
+    e.close()
+    for f in ("id", "time", "driftObjectType", "driftSide"):
+        assert np.array_equal(got[f], want[f]), f
+    # decisions taken within a few ulp of a shore or an edge may differ; everything else agrees
+    assert near(got, want, WALK_MAX) >= 0.999
+    both = (got["health"] > 0) & (want["health"] > 0)
+    assert np.allclose(got["age"][both], want["age"][both], rtol=0, atol=1e-9)
+    assert np.allclose(got["health"][both], want["health"][both], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("storage,bound", [("fp32", WALK_MAX), ("fp16", 3e-3)])
+def test_diffusive_walk_matches_the_fp32_step_on_philox_streams(cuda_device, storage, bound):
+    """Philox streams keyed on (particle, interval, step time), the same in both kernels. With
+    FP16 storage the plain step advects with u rounded to half precision (0.2 -> 0.19995 m/s:
+    1.3e-3 grid units per hour) while the surrogate's start-point velocity comes from the FP32
+    records, hence the wider bound."""
+    win = syn.config1_window(n_frames=2)
+    cfg = default_config(random=True, integrator=1, sigma=12.0)
+    p = syn.uniform_particles(30000, win.eta, win.xi, time=win.times[0], seed=31)
+    p["time"][::7] = win.times[0] + 1234.5
+    e = walk_engine(win, cfg, rng="philox", storage=storage)
+    e.set_particles(p)
+    e.move_interval(0)
+    got = e.get_particles()
+    e.close()
+    x = Engine(0, arithmetic="fp32", storage=storage, rng="philox")
+    x.set_config(cfg)
+    x.load_window(win)
+    x.set_particles(p)
+    x.move_interval(0)
+    want = x.get_particles()
+    x.close()
+    assert near(got, want, bound) >= 0.999
+    assert np.array_equal(got["age"], want["age"])
+
+
+def test_diffusive_walk_on_a_realistic_flow(cuda_device):
+    """Non-uniform flow: every wet particle stays with the surrogate (no fallback); the walk's
+    mean displacement from the deterministic surrogate run is zero within its sampling error, and
+    its spread is the plain operator's sigma (1 - k/kb) sqrt(n dt/dti) in metres."""
+    forcing = syn.RealisticForcing(eta=96, xi=96, s_rho=10, n_frames=2, seed=21,
+                                   land_fraction=0.0, water_border=0)
+    win = forcing.window()
+    n = 40000
+    rng = np.random.default_rng(5)
+    p = np.zeros(n, dtype=PARTICLE_DTYPE)
+    p["id"] = np.arange(n, dtype=np.uint64)
+    p["j"] = rng.uniform(30.0, 60.0, n)
+    p["i"] = rng.uniform(30.0, 60.0, n)
+    p["k"] = -rng.uniform(0.2, 0.8, n)
+    p["health"] = 1.0
+    p["time"] = win.times[0]
+    sigma = 6.0
+    det = walk_engine(win, default_config(random=False, sigma=sigma))
+    det.set_particles(p)
+    det.move_interval(0)
+    base = det.get_particles()
+    det.close()
+    e = walk_engine(win, default_config(random=True, sigma=sigma), rng="philox")
+    e.set_particles(p)
+    e.move_interval(0)
+    got = e.get_particles()
+    stats = e.surrogate_stats()
+    e.close()
+    assert stats["fallback"] == 0 and stats["run"] == n
+    err = great_circle_m(win.lon, win.lat, got, base)
+    # the walk's own spread: sigma (1 - k/kb) per substep, 120 substeps, on both axes
+    kb = -(win.sW - 2)
+    spread = sigma * (1 - p["k"] / kb) * np.sqrt(120.0)
+    ratio = np.mean(err ** 2) / np.mean(2 * spread ** 2)
+    assert 0.8 < ratio < 1.25, ratio
+    dj = (got["j"] - base["j"]).mean()
+    di = (got["i"] - base["i"]).mean()
+    assert abs(dj) < 0.02 and abs(di) < 0.02, (dj, di)
+
+
+def test_kernel_times_of_back_to_back_intervals(cuda_device):
+    """Per-interval kernel times recorded inside back-to-back runs: one record per interval, the
+    surrogate's three kernels timed, each no longer than its interval."""
+    win = syn.config1_window(n_frames=4)
+    p = syn.uniform_particles(200000, win.eta, win.xi, time=win.times[0], seed=2)
+    e = walk_engine(win, default_config(random=True), rng="philox", storage="fp16")
+    e.set_particles(p)
+    e.kernel_times()
+    for t in range(3):
+        e.move_interval(t)
+    kt = e.kernel_times()
+    assert kt.shape == (3, 3)
+    assert np.all(kt[:, :2] > 0) and np.all(kt[:, 2] >= 0)
+    assert len(e.kernel_times()) == 0
+    e.close()

@@ -129,7 +129,8 @@ struct wacomm_b200_context {
     size_t surrRowsCap = 0;
     unsigned long long *dSurrCounts = nullptr;  // [0]: fallback count (low 32 bits), [1]: run count
     cudaEvent_t evCell0 = nullptr, evCell1 = nullptr, evStep0 = nullptr, evStep1 = nullptr;
-    bool surrTimed = false;
+    bool surrTimed = false;  // the events of the last eager surrogate interval can be read
+    bool surrRan = false;    // dSurrCounts holds the counts of a surrogate interval (eager or captured)
     int smCount = 148;
 
     double *dGeoLon = nullptr, *dGeoLat = nullptr, *dSWValues = nullptr;  // kji2deplatlon grid
@@ -158,6 +159,17 @@ struct wacomm_b200_context {
     int *dErr = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evMove0 = nullptr, evMove1 = nullptr;
     cudaEvent_t evComputeMark = nullptr;  // orders asynchronous frame copies after enqueued kernels
+    // Kernel times of eager intervals (wacomm_b200_kernel_times): a ring of event marks around
+    // each interval's dominant kernels, so that intervals enqueued back to back are timed without
+    // a host wait. Plain step: [move start, move end]; surrogate: [step kernel start, step kernel
+    // end, walk or post kernel end, fallback step end].
+    struct TimedInterval {
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+        int marks = 0;
+    };
+    std::vector<TimedInterval> timing;
+    size_t timingNext = 0, timingCount = 0;
+    TimedInterval *timingCur = nullptr;
     bool moveTimed = false;
     float lastMs = 0;
     int lastLaunches = 0;
@@ -192,6 +204,32 @@ int grow(wacomm_b200_context *ctx, T *&ptr, size_t &cap, size_t need) {
     cap = 0;
     CUDA_TRY(ctx, cudaMalloc((void **)&ptr, bytes));
     cap = std::max<size_t>(need, 1);
+    return WACOMM_B200_OK;
+}
+
+constexpr size_t TIMING_RING = 256;
+
+// Opens the timing record of an eager interval (none while capturing).
+int timing_begin(wacomm_b200_context *ctx) {
+    ctx->timingCur = nullptr;
+    if (ctx->capturing) return WACOMM_B200_OK;
+    if (ctx->timing.empty()) ctx->timing.resize(TIMING_RING);
+    wacomm_b200_context::TimedInterval &t = ctx->timing[ctx->timingNext];
+    for (cudaEvent_t &e : t.ev)
+        if (!e) CUDA_TRY(ctx, cudaEventCreate(&e));
+    t.marks = 0;
+    ctx->timingCur = &t;
+    ctx->timingNext = (ctx->timingNext + 1) % TIMING_RING;
+    ctx->timingCount = std::min(ctx->timingCount + 1, TIMING_RING);
+    return WACOMM_B200_OK;
+}
+
+// Next mark of the open timing record, on the compute stream.
+int timing_mark(wacomm_b200_context *ctx) {
+    wacomm_b200_context::TimedInterval *t = ctx->timingCur;
+    if (!t || t->marks >= 4) return WACOMM_B200_OK;
+    CUDA_TRY(ctx, cudaEventRecord(t->ev[t->marks], ctx->stream));
+    t->marks++;
     return WACOMM_B200_OK;
 }
 
@@ -539,6 +577,11 @@ int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t of
             CUDA_TRY(ctx, cudaEventRecord(ctx->evMove0, ctx->stream));
             ctx->moveTimed = true;
         }
+        if (c == 0) {
+            int rc = timing_begin(ctx);
+            if (!rc) rc = timing_mark(ctx);
+            if (rc) return rc;
+        }
         P.firstChunk = c == 0;
         P.lastChunk = c == nChunks - 1;
         P.chunkEnd = P.lastChunk ? INFINITY : (c + 1) * chunk;
@@ -554,7 +597,7 @@ int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t of
         launches++;
         if (!ctx->capturing) CUDA_TRY(ctx, cudaEventRecord(ctx->evMove1, ctx->stream));
     }
-    return WACOMM_B200_OK;
+    return timing_mark(ctx);
 }
 
 int prepare_interval(wacomm_b200_context *ctx, int time_index, IntervalParams &P, int &launches) {
@@ -582,6 +625,40 @@ int prepare_interval(wacomm_b200_context *ctx, int time_index, IntervalParams &P
 }
 
 int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launches);
+
+// Buffers and tables a surrogate interval uses, sized (and the dry-node table built) before the
+// interval, so that a captured run allocates nothing: the dry-node prefix sums of the current
+// shore limit, the per-cell-level layer-1 sums and corner records, the fallback list and the rows.
+int reserve_surrogate(wacomm_b200_context *ctx, int *launches = nullptr) {
+    int rc;
+    const size_t dryNeed = (size_t)(ctx->eta + 1) * (ctx->xi + 1);
+    if (!ctx->dryValid || !(ctx->dryShore == ctx->cfg.shoreLimit)) {
+        if ((rc = grow(ctx, ctx->dDry, ctx->dryCap, dryNeed))) return rc;
+        CUDA_TRY(ctx, surrogate_dry_prefix(ctx->hasMask ? ctx->dMask : nullptr, ctx->dH,
+                                           ctx->cfg.shoreLimit, ctx->eta, ctx->xi, ctx->dDry,
+                                           ctx->stream));
+        if (launches) *launches += 2;
+        ctx->dryShore = ctx->cfg.shoreLimit;
+        ctx->dryValid = true;
+    }
+    const long long nCL = surrogate_cell_levels(ctx->eta, ctx->xi, ctx->sW);
+    if ((size_t)nCL > ctx->zCap) {
+        cudaFree(ctx->dZ);
+        cudaFree(ctx->dCorners);
+        ctx->dZ = nullptr;
+        ctx->dCorners = nullptr;
+        ctx->zCap = 0;
+        ctx->zT0 = ctx->zT1 = -1;
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dZ, (size_t)nCL * 256 * sizeof(__half)));
+        CUDA_TRY(ctx, cudaMalloc(&ctx->dCorners, (size_t)nCL * surrogate_corner_bytes()));
+        ctx->zCap = (size_t)nCL;
+    }
+    if (ctx->n) {
+        if ((rc = grow(ctx, ctx->dFallback, ctx->fallbackCap, ctx->n))) return rc;
+        if ((rc = grow(ctx, ctx->dSurrRows, ctx->surrRowsCap, ctx->n))) return rc;
+    }
+    return WACOMM_B200_OK;
+}
 
 // The work of one interval on the compute stream (pair packing, sort, move, fused count).
 int enqueue_interval(wacomm_b200_context *ctx, int time_index, int &launches) {
@@ -611,31 +688,10 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     if (count == 0) return WACOMM_B200_OK;
     int rc;
     const FrameDevice a = frame_of(ctx, P.t0), b = frame_of(ctx, P.t1);
-    // dry-node table
-    const size_t dryNeed = (size_t)(ctx->eta + 1) * (ctx->xi + 1);
-    if (!ctx->dryValid || !(ctx->dryShore == ctx->cfg.shoreLimit)) {
-        if ((rc = grow(ctx, ctx->dDry, ctx->dryCap, dryNeed))) return rc;
-        CUDA_TRY(ctx, surrogate_dry_prefix(ctx->hasMask ? ctx->dMask : nullptr, ctx->dH,
-                                           ctx->cfg.shoreLimit, ctx->eta, ctx->xi, ctx->dDry,
-                                           ctx->stream));
-        launches += 2;
-        ctx->dryShore = ctx->cfg.shoreLimit;
-        ctx->dryValid = true;
-    }
+    if ((rc = reserve_surrogate(ctx, &launches))) return rc;
     // layer 1 per cell-level
-    const long long nCL = surrogate_cell_levels(ctx->eta, ctx->xi, ctx->sW);
     CUDA_TRY(ctx, cudaEventRecord(ctx->evCell0, ctx->stream));
     if (ctx->zT0 != P.t0 || ctx->zT1 != P.t1 || ctx->zSemantics != ctx->metricSemantics) {
-        if ((size_t)nCL > ctx->zCap) {
-            cudaFree(ctx->dZ);
-            cudaFree(ctx->dCorners);
-            ctx->dZ = nullptr;
-            ctx->dCorners = nullptr;
-            ctx->zCap = 0;
-            CUDA_TRY(ctx, cudaMalloc(&ctx->dZ, (size_t)nCL * 256 * sizeof(__half)));
-            CUDA_TRY(ctx, cudaMalloc(&ctx->dCorners, (size_t)nCL * surrogate_corner_bytes()));
-            ctx->zCap = (size_t)nCL;
-        }
         CUDA_TRY(ctx, surrogate_cells(ctx->eta, ctx->xi, ctx->sW, ctx->sRho, a, b,
                                       ctx->dH, ctx->dDepth, ctx->dMetric, ctx->dSurrogate, ctx->dZ,
                                       ctx->dCorners, ctx->dErr, ctx->smCount, ctx->stream));
@@ -648,8 +704,6 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     // Work in slot order, unsorted: the per-cell data the step kernel gathers (FP16 layer-1 sums
     // and corner records) stays in L2, while the particle state is read and written coalesced.
     if ((rc = reserve_work(ctx, count))) return rc;
-    if ((rc = grow(ctx, ctx->dFallback, ctx->fallbackCap, count))) return rc;
-    if ((rc = grow(ctx, ctx->dSurrRows, ctx->surrRowsCap, count))) return rc;
     CUDA_TRY(ctx, cudaMemsetAsync(ctx->dSurrCounts, 0, 2 * sizeof(unsigned long long), ctx->stream));
     MoveLaunch L;
     L.count = (int)count;
@@ -671,9 +725,26 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     st.start = P.start;
     st.length = P.length;
     st.cfg = ctx->cfg;
+    // Diffusive forward intervals keep the surrogate's displacement and add the plain stochastic
+    // operator per substep (the walk kernel); backward, restart-clipped, empty and jibing intervals
+    // go to the plain step whole.
     const bool diffuse = ctx->cfg.random && (P.direction > 0 || ctx->cfg.backwardDiffusion);
-    st.fallbackAll = diffuse || P.direction < 0 || P.elapsed0 != 0 || P.length <= 0 ||
+    st.fallbackAll = P.direction < 0 || P.elapsed0 != 0 || P.length <= 0 ||
                      ctx->cfg.leewayJibeProbabilityHourly > 0;
+    IntervalParams Q = P;
+    Q.rng = ctx->opt.rng;
+    Q.firstChunk = 1;
+    Q.lastChunk = 1;
+    Q.chunkEnd = INFINITY;
+    const PackedArgs A = packed_args(ctx);
+    st.walk = diffuse ? 1 : 0;
+    st.semantics = ctx->opt.semantics;
+    st.storage = ctx->opt.storage;
+    st.interval = &Q;
+    st.cells = A.cells;
+    st.cellSurface = A.cellSurface;
+    st.invMetric = A.invMetric;
+    st.depthF = A.depthIntervalsF;
     st.dry = ctx->dDry;
     st.z = ctx->dZ;
     st.corners = ctx->dCorners;
@@ -685,32 +756,29 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     CUDA_TRY(ctx, cudaEventRecord(ctx->evMove0, ctx->stream));
     CUDA_TRY(ctx, cudaEventRecord(ctx->evStep0, ctx->stream));
     ctx->moveTimed = true;
+    if ((rc = timing_begin(ctx)) || (rc = timing_mark(ctx))) return rc;
+    st.midEvent = ctx->timingCur ? ctx->timingCur->ev[1] : nullptr;
+    if (ctx->timingCur) ctx->timingCur->marks = 2;  // ev[1] is recorded between the two kernels
     CUDA_TRY(ctx, surrogate_step(st, ctx->S.s, L, ctx->smCount, ctx->stream));
     launches += 2;
     CUDA_TRY(ctx, cudaEventRecord(ctx->evStep1, ctx->stream));
-    unsigned long long counts[2] = {0, 0};
-    CUDA_TRY(ctx, cudaMemcpyAsync(counts, ctx->dSurrCounts, sizeof(counts), cudaMemcpyDeviceToHost,
-                                  ctx->stream));
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    const size_t nFallback = (size_t)(counts[0] & 0xffffffffull);
-    ctx->surrTimed = true;
-    if (nFallback) {
-        IntervalParams Q = P;
-        Q.rng = ctx->opt.rng;
-        Q.firstChunk = 1;
-        Q.lastChunk = 1;
-        Q.chunkEnd = INFINITY;
-        MoveLaunch F = L;
-        F.count = (int)nFallback;
-        F.order = ctx->dFallback;
-        cudaError_t e = move_f32_dispatch(ctx->opt.semantics, ctx->opt.storage, ctx->opt.launch_shape,
-                                          ctx->cfg, Q, packed_args(ctx), ctx->S.s, F, ctx->stream);
-        if (e != cudaSuccess)
-            return fail(ctx, WACOMM_B200_ERR_CUDA, "fallback move launch: %s", cudaGetErrorString(e));
-        launches++;
-    }
+    if ((rc = timing_mark(ctx))) return rc;
+    ctx->surrTimed = !ctx->capturing;
+    ctx->surrRan = true;
+    // The plain FP32 step over the fallback list, whose length the kernels above left on the
+    // device: the launch covers every particle and the blocks past the list exit at once, so the
+    // host never waits for the count and the interval can be captured.
+    MoveLaunch F = L;
+    F.count = (int)count;
+    F.order = ctx->dFallback;
+    F.countDevice = reinterpret_cast<const uint32_t *>(ctx->dSurrCounts);
+    cudaError_t e = move_f32_dispatch(ctx->opt.semantics, ctx->opt.storage, ctx->opt.launch_shape,
+                                      ctx->cfg, Q, A, ctx->S.s, F, ctx->stream);
+    if (e != cudaSuccess)
+        return fail(ctx, WACOMM_B200_ERR_CUDA, "fallback move launch: %s", cudaGetErrorString(e));
+    launches++;
     CUDA_TRY(ctx, cudaEventRecord(ctx->evMove1, ctx->stream));
-    return WACOMM_B200_OK;
+    return timing_mark(ctx);
 }
 
 int check_errors(wacomm_b200_context *ctx) {
@@ -861,6 +929,9 @@ int wacomm_b200_context_destroy(wacomm_b200_context *ctx) {
     if (ctx->evComputeMark) cudaEventDestroy(ctx->evComputeMark);
     if (ctx->evMove0) cudaEventDestroy(ctx->evMove0);
     if (ctx->evMove1) cudaEventDestroy(ctx->evMove1);
+    for (auto &t : ctx->timing)
+        for (cudaEvent_t e : t.ev)
+            if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->h2d) cudaStreamDestroy(ctx->h2d);
     if (ctx->d2h) cudaStreamDestroy(ctx->d2h);
@@ -1577,6 +1648,7 @@ int wacomm_b200_set_surrogate(wacomm_b200_context *ctx, const float *parameters,
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     if (!ctx->dSurrogate) CUDA_TRY(ctx, cudaMalloc(&ctx->dSurrogate, image.size()));
     CUDA_TRY(ctx, cudaMemcpy(ctx->dSurrogate, image.data(), image.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(ctx, surrogate_prepare());
     ctx->hasSurrogate = true;
     ctx->zT0 = ctx->zT1 = -1;
     return WACOMM_B200_OK;
@@ -1587,18 +1659,42 @@ int wacomm_b200_last_surrogate_stats(const wacomm_b200_context *ctx, size_t *run
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     unsigned long long counts[2] = {0, 0};
     float c = 0.f, s = 0.f;
-    if (ctx->surrTimed) {
+    if (ctx->surrRan) {
         cudaSetDevice(ctx->device);
         wacomm_b200_context *m = const_cast<wacomm_b200_context *>(ctx);
-        CUDA_TRY(m, cudaEventSynchronize(ctx->evStep1));
+        CUDA_TRY(m, cudaStreamSynchronize(ctx->stream));
         CUDA_TRY(m, cudaMemcpy(counts, ctx->dSurrCounts, sizeof(counts), cudaMemcpyDeviceToHost));
-        if (cudaEventElapsedTime(&c, ctx->evCell0, ctx->evCell1) != cudaSuccess) c = 0.f;
-        if (cudaEventElapsedTime(&s, ctx->evStep0, ctx->evStep1) != cudaSuccess) s = 0.f;
+        if (ctx->surrTimed) {
+            if (cudaEventElapsedTime(&c, ctx->evCell0, ctx->evCell1) != cudaSuccess) c = 0.f;
+            if (cudaEventElapsedTime(&s, ctx->evStep0, ctx->evStep1) != cudaSuccess) s = 0.f;
+        }
     }
     if (run) *run = (size_t)counts[1];
     if (fallback) *fallback = (size_t)(counts[0] & 0xffffffffull);
     if (cell_ms) *cell_ms = c;
     if (step_ms) *step_ms = s;
+    return WACOMM_B200_OK;
+}
+
+int wacomm_b200_kernel_times(wacomm_b200_context *ctx, float *ms, int capacity, int *count) {
+    if (!ctx || !count || (capacity > 0 && !ms)) return WACOMM_B200_ERR_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    const size_t n = std::min(ctx->timingCount, (size_t)std::max(capacity, 0));
+    const size_t first = (ctx->timingNext + TIMING_RING - ctx->timingCount) % TIMING_RING;
+    const size_t skip = ctx->timingCount - n;  // the oldest records that do not fit
+    for (size_t q = 0; q < n; q++) {
+        const wacomm_b200_context::TimedInterval &t = ctx->timing[(first + skip + q) % TIMING_RING];
+        if (t.marks > 0) CUDA_TRY(ctx, cudaEventSynchronize(t.ev[t.marks - 1]));
+        for (int m = 0; m < 3; m++) {
+            float v = 0.f;
+            if (m + 1 < t.marks) CUDA_TRY(ctx, cudaEventElapsedTime(&v, t.ev[m], t.ev[m + 1]));
+            ms[3 * q + m] = v;
+        }
+    }
+    *count = (int)n;
+    ctx->timingCount = 0;
+    ctx->timingCur = nullptr;
     return WACOMM_B200_OK;
 }
 
@@ -2032,9 +2128,8 @@ int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, in
     if (n_intervals < 1 || first_time_index < 0 || first_time_index >= T || last < 0 || last >= T)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "intervals %d..%d out of [0, %d)",
                     first_time_index, last, T);
-    if (ctx->opt.surrogate)
-        return fail(ctx, WACOMM_B200_ERR_STATE,
-                    "runs with the surrogate option are not captured");
+    if (ctx->opt.surrogate && !ctx->hasSurrogate)
+        return fail(ctx, WACOMM_B200_ERR_STATE, "the surrogate option needs set_surrogate weights");
     cudaSetDevice(ctx->device);
     release_graph(ctx);
     // Uploads in flight finish first (their ready events lie outside the capture), and every
@@ -2059,8 +2154,10 @@ int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, in
         if ((rc = reserve_work(ctx, ctx->n))) return rc;
         if (ctx->opt.sort_by_cell && (rc = reserve_sort(ctx, ctx->n))) return rc;
     }
+    if (ctx->opt.surrogate && (rc = reserve_surrogate(ctx))) return rc;
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->pairT0 = ctx->pairT1 = -1;  // the graph packs its own pairs
+    ctx->zT0 = ctx->zT1 = -1;        // and evaluates its own per-cell layer 1
     CUDA_TRY(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     ctx->capturing = true;
     // The captured sorts' sequence is written only at launch, and what dSeq holds when the graph
@@ -2079,6 +2176,7 @@ int wacomm_b200_graph_capture(wacomm_b200_context *ctx, int first_time_index, in
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(ctx->stream, &graph);
     ctx->pairT0 = ctx->pairT1 = -1;  // nothing captured has run yet
+    ctx->zT0 = ctx->zT1 = -1;
     if (!rc && e != cudaSuccess)
         rc = fail(ctx, WACOMM_B200_ERR_CUDA, "capture: %s", cudaGetErrorString(e));
     if (!rc) {
@@ -2115,6 +2213,8 @@ int wacomm_b200_graph_launch(wacomm_b200_context *ctx) {
     CUDA_TRY(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
     CUDA_TRY(ctx, accumulate_steps(ctx->dSteps, ctx->dSteps + 1, ctx->stream));
     ctx->pairT0 = ctx->pairT1 = -1;
+    ctx->zT0 = ctx->zT1 = -1;
+    ctx->surrTimed = false;
     ctx->lastLaunches = ctx->graphLaunches;
     return WACOMM_B200_OK;
 }

@@ -213,8 +213,20 @@ struct SurrogateStep {
     uint32_t *fallback, *fallbackCount;
     unsigned long long *runCount;
     float4 *rows;  // per work item (count): layer-4 sums and row tag, step kernel -> post kernel
+    // Diffusive forward intervals: the surrogate's displacement spread over the substeps plus the
+    // plain stochastic operator and closures of every substep (surrogate_walk_kernel), over the
+    // cell-column pair of the FP32 step; otherwise the closed-form post kernel.
+    int walk = 0;
+    int semantics = 0, storage = 0;
+    const IntervalParams *interval = nullptr;
+    const void *cells = nullptr, *cellSurface = nullptr;
+    const float2 *invMetric = nullptr;
+    const float *depthF = nullptr;
+    cudaEvent_t midEvent = nullptr;  // recorded between the step kernel and the post/walk kernel
 };
 
+// Kernel attributes of the tensor-core kernels (once per device; outside stream capture).
+cudaError_t surrogate_prepare();
 size_t surrogate_packed_bytes();
 size_t surrogate_corner_bytes();
 size_t surrogate_parameter_count();
@@ -227,7 +239,8 @@ cudaError_t surrogate_cells(int eta, int xi, int sW, int sRho, const FrameDevice
                             const double2 *metric, const uint8_t *weights, __half *z, void *corners,
                             int *err, int smCount, cudaStream_t stream);
 // The step kernel (layers 1-4 of every work item into s.rows) and the post kernel (displacement,
-// closures, state, concentration, fallback list): two launches.
+// closures, state, concentration, fallback list) or, for diffusive intervals, the walk kernel
+// (displacement with the plain stochastic operator per substep): two launches.
 cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const MoveLaunch &L,
                            int smCount, cudaStream_t stream);
 // Inclusive 2-D prefix sums [(eta+1)][(xi+1)] of nodes with mask 0 or h <= shore.

@@ -22,7 +22,17 @@ struct MoveLaunch {
     int concTimeIndex, concTimes;
     unsigned long long *steps;    // particle-step counter, or null
     int *err;
+    // When set, the work items are the first min(count, *countDevice): a list whose length a
+    // kernel earlier on the stream wrote (the launch covers `count`, blocks past the list exit).
+    const uint32_t *countDevice = nullptr;
 };
+
+// Work items of a launch: count, or the device-side length of its list.
+__device__ __forceinline__ int launch_count(const MoveLaunch &L) {
+    if (!L.countDevice) return L.count;
+    const uint32_t listed = *L.countDevice;
+    return listed < (uint32_t)L.count ? (int)listed : L.count;
+}
 
 // Linear index of the concentration cell of an alive particle, or -1
 // (Concentration.hpp:28-41: round-half-away indices, bounds 0<=j<eta, 0<=i<xi, -sRho<k<=0).
@@ -114,10 +124,12 @@ __global__ void __launch_bounds__(LaunchShape<SHAPE>::threads, LaunchShape<SHAPE
                                                         const IntervalParams P,
                                                         const FastView<STORE> F, ParticleSoA S,
                                                         const MoveLaunch L) {
+    const int count = launch_count(L);
+    if ((int)(blockIdx.x * blockDim.x) >= count) return;  // whole blocks past a device-side list
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     long long cell = -1;
     int steps = 0;
-    if (t < L.count) {
+    if (t < count) {
         uint32_t slot = L.order ? L.order[t] : (uint32_t)t;
         ParticleState p;
         p.id = S.id[slot];

@@ -23,6 +23,7 @@
 // warp 16 streams weights, warp 17 issues the MMAs and owns the TMEM allocation. Every wait is bounded; a timeout raises an error flag and the block drains and
 // exits.
 #include <cstring>
+#include <type_traits>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -835,6 +836,271 @@ __global__ void __launch_bounds__(256, 5) surrogate_post_kernel(const StepArgs a
     if ((threadIdx.x & 31) == 0 && ran) atomicAdd(a.runCount, (unsigned long long)__popc(ran));
 }
 
+// ------------------------------------------------------------------ learned advection + plain diffusion
+
+// The cell-column forcing pair the plain FP32 step reads, for the per-substep operator.
+template <int STORE>
+struct WalkView {
+    const CellQuad<STORE> *columns;  // [cell][sW][2] (A, B)
+    const CellSurface *surface;      // [cell]
+    const float2 *invMetric;         // [cell] {1/xdist, 1/ydist}
+    const float *depth;              // [sW-1] FP32 depthIntervals
+};
+
+__device__ __forceinline__ CellSurface load_surface(const CellSurface *s, int cell) {
+    const float4 *q = reinterpret_cast<const float4 *>(s + cell);
+    return CellSurface{__ldg(q), __ldg(q + 1)};
+}
+
+// One particle over the rest of a forward interval: the surrogate's deterministic displacement,
+// spread evenly over the substeps as constant rates (m/s), plus the plain stochastic operator and
+// closures of every substep, as the FP32 Euler step applies them (Particle.cpp:505-533,644-814;
+// kernel.cu:262-364): sigma (1 - k/kb) Z sqrt(dt/dti) horizontally, the same times AKT crid
+// vertically, the vertical cap, the vertical and horizontal closures, survival and age.
+//
+// The position is kept as a cell (or level) index plus an FP32 fraction, with the FP64 remainder
+// of the start position carried alongside: a substep that stays in its cell and level and needs
+// no closure is FP32 work on the fraction, with the cell's AKT, surface, metric and layer
+// thickness held in registers since the last move to another cell or level; any other substep
+// (a cell change, a closure) runs in FP64 as the plain step does. Returns the substeps taken.
+template <int SEM, int STORE>
+__device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams &P,
+                             const WalkView<STORE> &W, int eta, int xi, int sW, ParticleState &p,
+                             float rateX, float rateY, float rateZ) {
+    const double length = P.length, invLength = 1.0 / length, kLower = P.kLower;
+    const float shore = (float)cfg.shoreLimit, kLowerF = (float)kLower;
+    const float invKLower = (float)P.invKLower, sigma = (float)cfg.sigma, crid = (float)cfg.crid;
+    const float dtiF = (float)cfg.dti;
+    const bool philox = P.rng == WACOMM_B200_RNG_PHILOX;
+    const uint64_t prefix = fold(fold(mix64(cfg.randomSeed), p.id), (uint64_t)P.intervalKey);
+    const uint64_t philoxKey = p.id ^ mix64(cfg.randomSeed);
+    bool lazy = false;
+    int steps = 0;
+    double elapsed = p.time > P.start ? fmin(length, p.time - P.start) : 0.0;  // activation
+
+    const double fj = floor(p.j), fi = floor(p.i), ck = ceil(p.k);
+    int jI = to_index<SEM>(fj), iI = to_index<SEM>(fi), kI = to_index<SEM>(ck);
+    float jF = (float)(p.j - fj), iF = (float)(p.i - fi), kF = (float)(ck - p.k);
+    double jLo = (p.j - fj) - (double)jF, iLo = (p.i - fi) - (double)iF;
+    double kLo = (ck - p.k) - (double)kF;
+
+    int keptCell = -1, keptK = 1;
+    CellSurface surf{};
+    float2 inv{0.f, 0.f};
+    QuadPair aUp{}, aLo{};
+    float depth = 0.f;
+
+    while (elapsed < length) {
+        const double stepDt = fmin(cfg.dti, length - elapsed);
+        const bool dead = lazy ? (p.age >= P.ageKillHi ||
+                                  (p.age > P.ageKillLo && exp(-p.age / cfg.tau0) < cfg.survprob))
+                               : p.health < cfg.survprob;
+        if (dead) {
+            p.health = -1;
+            lazy = false;
+            break;
+        }
+        if (!valid_cell(jI, iI, eta, xi) || (SEM == SEM_DEVICE && (kI > 0 || kI <= -sW + 1))) {
+            p.health = -1;
+            lazy = false;
+            break;
+        }
+        steps++;
+        const int kM = mem_level(kI, sW);
+        const int cell = jI * xi + iI;
+        if (cell != keptCell) {
+            surf = load_surface(W.surface, cell);
+            inv = __ldg(W.invMetric + cell);
+            keptCell = cell;
+            keptK = 1;
+        }
+        if (kM != keptK) {
+            const CellQuad<STORE> *col = W.columns + ((size_t)cell * sW + (size_t)(kM + sW - 1)) * 2;
+            load_second<STORE>(col - 1, aLo);  // akt of W level kI-1
+            load_second<STORE>(col + 1, aUp);  // akt of W level kI
+            depth = __ldg(W.depth + (kM + sW - 2));
+            keptK = kM;
+        }
+        const float dt = (float)stepDt;
+        const float alpha = (float)((elapsed + 0.5 * stepDt) * invLength);
+        const float hc = surface_from(surf, jF, iF).height(alpha);
+        if (hc <= shore && cfg.horizontalClosure == CLOSURE_KILL) {
+            p.health = -1;
+            lazy = false;
+            if (SEM == SEM_DEVICE) break;
+        }
+        const Weights8 wa = weights8(jF, iF, alpha);
+        const float au = blend(aUp, wa), al = blend(aLo, wa);
+        const float aa = fmaf(al - au, kF, au);
+        float n0, n1, n2;
+        if (philox) {
+            philox_normals3(philoxKey, P.intervalKey, (uint64_t)__double_as_longlong(elapsed), n0, n1,
+                            n2);
+        } else {
+            const uint64_t stepKey = fold(prefix, (uint64_t)floor(elapsed / cfg.dti));
+            n0 = (float)prefix_normal(stepKey, 0);
+            n1 = (float)prefix_normal(stepKey, 1);
+            n2 = (float)prefix_normal(stepKey, 2);
+        }
+        const float kNow = (float)kI - kF;
+        const float sigmaDepth = sigma * (1.f - kNow * invKLower);
+        const float scale = stepDt == cfg.dti ? 1.f : sqrtf(dt / dtiF);
+        const float rx = sigmaDepth * n0 * scale, ry = sigmaDepth * n1 * scale;
+        const float rz = sigmaDepth * n2 * aa * crid * scale;
+        const float zdist = hc * depth;
+        const float rzdist = __frcp_rn(zdist);
+        const float dI = fmaf(rateX, dt, rx) * inv.x, dJ = fmaf(rateY, dt, ry) * inv.y;
+        float zleap = fmaf(rateZ, dt, rz);
+        if (fabsf(zleap) > zdist) zleap = signf_of(zdist, zleap);
+        const float jN = jF + dJ, iN = iF + dI, kN = fmaf(-zleap, rzdist, kF);
+        const bool vertical = (float)kI - kN > 0.f || (float)kI - kN < kLowerF;
+        bool done = false;
+        if (!vertical && jN >= 0.f && jN < 1.f && iN >= 0.f && iN < 1.f) {
+            // same cell, no vertical closure: the shore test at the destination in the kept surface
+            if (surface_from(surf, jN, iN).height(alpha) > shore) {
+                jF = jN;
+                iF = iN;
+                const float c = floorf(kN);  // level crossing
+                kI -= (int)c;
+                kF = kN - c;
+                done = true;
+            }
+        }
+        if (!done) {
+            // the plain step's FP64 landing and closures (cell change, shore, closures)
+            const double pj = (double)jI + (double)jF + jLo, pi = (double)iI + (double)iF + iLo;
+            const double pk = (double)kI - (double)kF - kLo;
+            double jdet = pj + (double)dJ, idet = pi + (double)dI;
+            double kdet = pk + (double)(zleap * rzdist);
+            if (kdet > 0.) close_upper(cfg, kdet, p.health, lazy);
+            if (kdet < kLower) close_lower(cfg, kLower, kdet, p.health, lazy);
+            double nj = pj, ni = pi, nk = pk;
+            const double fjd = floor(jdet), fid = floor(idet);
+            const int jdetI = to_index<SEM>(fjd), idetI = to_index<SEM>(fid);
+            if (valid_cell(jdetI, idetI, eta, xi)) {
+                const int dcell = jdetI * xi + idetI;
+                const CellSurface there = dcell == keptCell ? surf : load_surface(W.surface, dcell);
+                const float hcdet =
+                    surface_from(there, (float)(jdet - fjd), (float)(idet - fid)).height(alpha);
+                if (hcdet <= shore) {
+                    if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
+                        idet = pi;
+                        jdet = pj;
+                    } else if (cfg.horizontalClosure == CLOSURE_KILL) {
+                        p.health = -1;
+                        lazy = false;
+                    } else if (cfg.horizontalClosure == CLOSURE_REFLECTION) {
+                        idet = reflect_cell(pi, iI, idet, idetI);
+                        jdet = reflect_cell(pj, jI, jdet, jdetI);
+                    }
+                }
+                ni = idet;
+                nj = jdet;
+                nk = kdet;
+            } else {
+                if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
+                    nk = kdet;
+                } else if (cfg.horizontalClosure == CLOSURE_KILL) {
+                    p.health = -1;
+                    lazy = false;
+                } else if (cfg.horizontalClosure == CLOSURE_REFLECTION) {
+                    ni = reflect_domain(idet, xi - 1);
+                    nj = reflect_domain(jdet, eta - 1);
+                    nk = kdet;
+                }
+            }
+            const double gj = floor(nj), gi = floor(ni), gk = ceil(nk);
+            jI = to_index<SEM>(gj);
+            iI = to_index<SEM>(gi);
+            kI = to_index<SEM>(gk);
+            jF = (float)(nj - gj);
+            iF = (float)(ni - gi);
+            kF = (float)(gk - nk);
+            jLo = (nj - gj) - (double)jF;
+            iLo = (ni - gi) - (double)iF;
+            kLo = (gk - nk) - (double)kF;
+        }
+        const bool alive = lazy ? (p.age < P.ageUnder || exp(-p.age / cfg.tau0) > 0) : p.health > 0;
+        if (alive) {
+            p.age = p.age + stepDt;
+            lazy = true;
+        }
+        elapsed += stepDt;
+    }
+    if (lazy) p.health = exp(-p.age / cfg.tau0);
+    p.j = (double)jI + (double)jF + jLo;
+    p.i = (double)iI + (double)iF + iLo;
+    p.k = (double)kI - (double)kF - kLo;
+    return steps;
+}
+
+// Learned advection with the plain stochastic operator per substep (diffusive forward intervals):
+// one thread per work item in slot order. The rates come from the item's layer-4 outputs and the
+// start-point velocity of its corner record, as in surrogate_post_kernel; the particle then takes
+// every substep of the interval by walk_particle. Rows the step kernel handed back go to the
+// fallback list.
+template <int SEM, int STORE>
+__global__ void __launch_bounds__(128, 4)
+    surrogate_walk_kernel(const StepArgs a, const wacomm_b200_config cfg, const IntervalParams P,
+                          const WalkView<STORE> W, ParticleSoA S, const MoveLaunch L) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool write = n < L.count && !(L.err && (*L.err & ERR_SURROGATE_WAIT));
+    long long concCell = -1;
+    int steps = 0;
+    bool run = false;
+    if (write) {
+        const float4 row = a.rows[n];
+        const int code = __float_as_int(row.w);
+        const int status = code >= 0 ? ROW_RUN : (code == ROW_CODE_FALLBACK ? ROW_FALLBACK : ROW_NONE);
+        const uint32_t slot = L.order ? L.order[n] : (uint32_t)n;
+        ParticleState p;
+        p.j = S.j[slot];
+        p.i = S.i[slot];
+        p.k = S.k[slot];
+        p.health = S.health[slot];
+        p.time = S.time[slot];
+        if (status == ROW_RUN) {
+            p.id = S.id[slot];
+            p.age = S.age[slot];
+            const float4 *cf = reinterpret_cast<const float4 *>(a.corners + code);
+            const float4 cu0 = __ldg(cf + 0), cu1 = __ldg(cf + 1), cv0 = __ldg(cf + 2),
+                         cv1 = __ldg(cf + 3), cwU0 = __ldg(cf + 4), cwU1 = __ldg(cf + 5),
+                         cwL0 = __ldg(cf + 6), cwL1 = __ldg(cf + 7);
+            const float gate = __ldg(reinterpret_cast<const float *>(cf + 12) + 2);
+            const double fj = floor(p.j), fi = floor(p.i), ck = ceil(p.k);
+            const float jF = (float)(p.j - fj), iF = (float)(p.i - fi), kF = (float)(ck - p.k);
+            const double da0 = p.time > a.start ? (p.time - a.start) * a.invLength : 0.0;
+            const float am = (float)(0.5 * (da0 + 1.0));
+            const float invTrem = (float)(1.0 / ((1.0 - da0) * a.length));
+            const float ub = blend(bil4(cu0, jF, iF), bil4(cu1, jF, iF), am);
+            const float vb = blend(bil4(cv0, jF, iF), bil4(cv1, jF, iF), am);
+            const float wb = blend(blend(bil4(cwU0, jF, iF), bil4(cwL0, jF, iF), kF),
+                                   blend(bil4(cwU1, jF, iF), bil4(cwL1, jF, iF), kF), am);
+            const float rateX = fmaf(OUT_H * row.x * gate, invTrem, ub);
+            const float rateY = fmaf(OUT_H * row.y * gate, invTrem, vb);
+            const float rateZ = fmaf(OUT_V * row.z * gate, invTrem, wb + (float)a.sv);
+            steps = walk_particle<SEM, STORE>(cfg, P, W, a.eta, a.xi, a.sW, p, rateX, rateY, rateZ);
+            S.j[slot] = p.j;
+            S.i[slot] = p.i;
+            S.k[slot] = p.k;
+            S.age[slot] = p.age;
+            S.health[slot] = p.health;
+            if (L.conc) concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
+            run = true;
+        } else if (status == ROW_NONE && L.conc) {
+            concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
+        }
+        if (status == ROW_FALLBACK) {
+            const uint32_t at = atomicAdd(a.fallbackCount, 1u);
+            a.fallback[at] = slot;
+        }
+    }
+    if (L.steps) warp_sum_steps(L.steps, steps);
+    if (L.conc) warp_count(L.conc, concCell);
+    const unsigned ran = __ballot_sync(__activemask(), run);
+    if ((threadIdx.x & 31) == 0 && ran) atomicAdd(a.runCount, (unsigned long long)__popc(ran));
+}
+
 // ------------------------------------------------------------------ dry-node prefix sums
 
 __global__ void dry_rows_kernel(const double *mask, const double *h, double shore, int eta, int xi,
@@ -867,6 +1133,23 @@ __global__ void dry_cols_kernel(int eta, int xi, int *pre) {
 }  // namespace
 
 // ------------------------------------------------------------------ host side
+
+// The shared-memory sizes of the two tensor-core kernels, set once per device (the current one; a
+// set-up step, kept out of stream capture).
+cudaError_t surrogate_prepare() {
+    static bool done[64] = {};
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    if (device >= 0 && device < 64 && done[device]) return cudaSuccess;
+    e = cudaFuncSetAttribute(surrogate_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)CELL_SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(surrogate_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)STEP_SMEM);
+    if (e == cudaSuccess && device >= 0 && device < 64) done[device] = true;
+    return e;
+}
 
 size_t surrogate_packed_bytes() { return PACKED_BYTES; }
 
@@ -940,13 +1223,8 @@ cudaError_t surrogate_cells(int eta, int xi, int sW, int sRho, const FrameDevice
     a.corners = static_cast<CellCorners *>(corners);
     a.err = err;
     if (a.nCL <= 0) return cudaSuccess;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(surrogate_cell_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CELL_SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    cudaError_t e = surrogate_prepare();
+    if (e != cudaSuccess) return e;
     long long tiles = (a.nCL + TILE - 1) / TILE;
     int blocks = (int)(tiles < smCount ? tiles : smCount);
     surrogate_cell_kernel<<<blocks, 128, CELL_SMEM, stream>>>(a);
@@ -983,20 +1261,42 @@ cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const M
     a.fallbackCount = s.fallbackCount;
     a.runCount = s.runCount;
     a.rows = s.rows;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(surrogate_step_kernel,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)STEP_SMEM);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    cudaError_t e = surrogate_prepare();
+    if (e != cudaSuccess) return e;
     long long tiles = ((long long)L.count + TILE - 1) / TILE;
     int blocks = (int)(tiles < smCount ? tiles : smCount);
     surrogate_step_kernel<<<blocks, STEP_THREADS, STEP_SMEM, stream>>>(a, S, L);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    surrogate_post_kernel<<<(L.count + 255) / 256, 256, 0, stream>>>(a, S, L);
-    return cudaGetLastError();
+    if (s.midEvent && (e = cudaEventRecord(s.midEvent, stream)) != cudaSuccess) return e;
+    if (!s.walk) {
+        surrogate_post_kernel<<<(L.count + 255) / 256, 256, 0, stream>>>(a, S, L);
+        return cudaGetLastError();
+    }
+    const int blocks128 = (L.count + 127) / 128;
+    auto walk = [&](auto semTag, auto storeTag) {
+        constexpr int SEM = decltype(semTag)::value, STORE = decltype(storeTag)::value;
+        WalkView<STORE> W;
+        W.columns = static_cast<const CellQuad<STORE> *>(s.cells);
+        W.surface = static_cast<const CellSurface *>(s.cellSurface);
+        W.invMetric = s.invMetric;
+        W.depth = s.depthF;
+        surrogate_walk_kernel<SEM, STORE><<<blocks128, 128, 0, stream>>>(a, s.cfg, *s.interval, W, S, L);
+        return cudaGetLastError();
+    };
+    using Host = std::integral_constant<int, SEM_HOST>;
+    using Device = std::integral_constant<int, SEM_DEVICE>;
+    using F32 = std::integral_constant<int, STORE_F32>;
+    using F16 = std::integral_constant<int, STORE_F16>;
+    using BF16 = std::integral_constant<int, STORE_BF16>;
+    if (s.semantics == SEM_HOST) {
+        if (s.storage == STORE_F16) return walk(Host{}, F16{});
+        if (s.storage == STORE_BF16) return walk(Host{}, BF16{});
+        return walk(Host{}, F32{});
+    }
+    if (s.storage == STORE_F16) return walk(Device{}, F16{});
+    if (s.storage == STORE_BF16) return walk(Device{}, BF16{});
+    return walk(Device{}, F32{});
 }
 
 cudaError_t surrogate_dry_prefix(const double *mask, const double *h, double shore, int eta, int xi,

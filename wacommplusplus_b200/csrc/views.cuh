@@ -252,6 +252,31 @@ __device__ __forceinline__ void load_first<STORE_BF16>(const CellQuad<STORE_BF16
     a.t1 = quad_bf(x.z, x.w);
 }
 
+// The second field of a CellQuad only (akt of a B record, without w).
+template <int STORE>
+__device__ __forceinline__ void load_second(const CellQuad<STORE> *p, QuadPair &b);
+
+template <>
+__device__ __forceinline__ void load_second<STORE_F32>(const CellQuad<STORE_F32> *p, QuadPair &b) {
+    const float4 *q = reinterpret_cast<const float4 *>(p);
+    b.t0 = quad_of(__ldg(q + 2));
+    b.t1 = quad_of(__ldg(q + 3));
+}
+
+template <>
+__device__ __forceinline__ void load_second<STORE_F16>(const CellQuad<STORE_F16> *p, QuadPair &b) {
+    uint4 y = __ldg(reinterpret_cast<const uint4 *>(p) + 1);
+    b.t0 = quad_h(y.x, y.y);
+    b.t1 = quad_h(y.z, y.w);
+}
+
+template <>
+__device__ __forceinline__ void load_second<STORE_BF16>(const CellQuad<STORE_BF16> *p, QuadPair &b) {
+    uint4 y = __ldg(reinterpret_cast<const uint4 *>(p) + 1);
+    b.t0 = quad_bf(y.x, y.y);
+    b.t1 = quad_bf(y.z, y.w);
+}
+
 struct CellSurface {  // FP32 at the 4 corners: h + zeta@t0, and zeta@t1 - zeta@t0
     float4 s0, dz;
 };

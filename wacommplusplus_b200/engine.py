@@ -342,6 +342,17 @@ class Engine:
         return {"device_ms": ms.value, "move_ms": move_ms.value, "launches": launches.value,
                 "particle_steps": steps.value}
 
+    def kernel_times(self, capacity=256):
+        """(n, 3) array of device ms of the dominant kernels of the eager intervals enqueued since
+        the last call, oldest first: [move, 0, 0] for the plain step, [step kernel, post or walk
+        kernel, fallback step] with the surrogate."""
+        out = np.zeros((capacity, 3), dtype=np.float32)
+        n = ctypes.c_int()
+        self._check(self._lib.wacomm_b200_kernel_times(
+            self._ctx, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), capacity,
+            ctypes.byref(n)))
+        return out[:n.value].copy()
+
     @property
     def stream(self):
         """Address of the context's cudaStream_t (for torch.cuda.ExternalStream)."""
