@@ -10,15 +10,25 @@ interval of every particle. Synthetic, seeded inputs stand in for the unavailabl
 
 Prints one JSON line (rank 0). `value` is device-timed with the particles resident in HBM;
 `e2e` moves the same particles through the public host-buffer entry point with the copies in the
-timed region; `cpu_baseline` times the reference's own CPU path on a bounded sample. `surrogate`
-is the second arm of the metric: the same workload with FP16 forcing storage and the learned
-surrogate (tcgen05 MLP per particle-interval), device-timed the same way, with its position error
-after 24 hours against the FP64 reference-arithmetic kernel on a 1,048,576-particle subset and its
-tensor-core roofline.
+timed region; `cpu_baseline` times the reference's own CPU path (move and concentration) on a
+bounded sample. `surrogate` is the second arm of the metric, the learned form: the same workload
+with FP16 forcing storage, the tcgen05 MLP's one-interval displacement and the plain stochastic
+operator every substep (Philox streams), device-timed the same way, beside the plain FP32 step with
+the same random walk and the deterministic surrogate; with the tensor-core roofline of its step
+kernel and its position error after 24 hours against the FP64 reference-arithmetic kernel, on the
+analytic grid (1,048,576-particle subset) and on a non-uniform streamfunction flow. `precision`
+gives the plain step with FP32, FP16 and BF16 forcing storage (throughput and 24-hour error) and
+the FP64 reference-arithmetic kernel's throughput. Kernel times come from per-interval events
+recorded inside the timed loops.
 """
 import argparse
 import json
 import os
+
+# The reference's CPU path is timed as its solver runs it: OpenMP threads bound one per physical
+# core, packed (set before any OpenMP runtime is loaded).
+os.environ.setdefault("OMP_PLACES", "cores")
+os.environ.setdefault("OMP_PROC_BIND", "close")
 import statistics
 import subprocess
 import sys
@@ -110,6 +120,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def physical_cores():
+    """Physical cores among the CPUs this process may run on (one per (package, core) pair)."""
+    seen = set()
+    for cpu in sorted(os.sched_getaffinity(0)):
+        base = f"/sys/devices/system/cpu/cpu{cpu}/topology/"
+        try:
+            with open(base + "core_id") as a, open(base + "physical_package_id") as b:
+                seen.add((b.read().strip(), a.read().strip()))
+        except OSError:
+            seen.add(("cpu", str(cpu)))
+    return max(1, len(seen))
+
+
 def physical_gpu(local_rank):
     visible = os.environ.get("CUDA_VISIBLE_DEVICES")
     if visible:
@@ -129,21 +152,31 @@ def workload(n_particles, rank, frames=25):
     return win, particles, cfg
 
 
+def cpu_interval(kind, cfg, recs, win, t, threads):
+    """One interval of the reference CPU path on `recs`: Particle::move under OpenMP dynamic,64
+    (Wacomm.cpp:501-525), then Concentration::evaluate (Wacomm.cpp:722) into the float grid (the
+    oracle port of both where the reference build is absent). Returns seconds."""
+    from oracle import bindings as ob
+    t0 = time.perf_counter()
+    if kind == "reference":
+        ob.ref_move(cfg, recs, win, t, threads=threads)
+        ob.ref_concentration(recs, t + 1, win.T, win, threads=threads)
+    else:
+        ob.oracle_move(cfg, recs, win, t, threads=threads)
+        ob.oracle_concentration(recs, t + 1, win.T, win)
+    return time.perf_counter() - t0
+
+
 def cpu_reference_rate(win, particles, cfg, threads, repeats=3, sample=262144):
-    """Particle-steps/s of the reference CPU path (Particle::move under OpenMP dynamic,64, or the
-    oracle port where the reference build is absent) on `sample` particles for one interval."""
+    """Particle-steps/s of the reference CPU path (move + concentration of one interval) on
+    `sample` particles; median of `repeats` after a warm-up."""
     from oracle import bindings as ob
     kind = "reference" if ob.ref_available() else "port"
     sample = min(sample, len(particles))
     rates = []
     for r in range(repeats + 1):
         recs = particles[:sample].copy()
-        t0 = time.perf_counter()
-        if kind == "reference":
-            ob.ref_move(cfg, recs, win, r % (win.T - 1), threads=threads)
-        else:
-            ob.oracle_move(cfg, recs, win, r % (win.T - 1), threads=threads)
-        dt = time.perf_counter() - t0
+        dt = cpu_interval(kind, cfg, recs, win, r % (win.T - 1), threads)
         steps = sample * int(round(3600.0 / cfg.dti))
         if r > 0:  # first run warms caches and the thread pool
             rates.append(steps / dt)
@@ -154,21 +187,17 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    threads = len(os.sched_getaffinity(0))
+    threads = physical_cores()
     win, particles, cfg = workload(1 << 18, 0)
     from oracle import bindings as ob
     kind = "reference" if ob.ref_available() else "port"
     sample = len(particles)
     steps_per = sample * 120
     for _ in range(args.warmup):
-        recs = particles.copy()
-        (ob.ref_move if kind == "reference" else ob.oracle_move)(cfg, recs, win, 0, threads=threads)
-    t0 = time.perf_counter()
+        cpu_interval(kind, cfg, particles.copy(), win, 0, threads)
+    dt = 0.0
     for s in range(args.steps):
-        recs = particles.copy()
-        (ob.ref_move if kind == "reference" else ob.oracle_move)(cfg, recs, win, s % (win.T - 1),
-                                                                 threads=threads)
-    dt = time.perf_counter() - t0
+        dt += cpu_interval(kind, cfg, particles.copy(), win, s % (win.T - 1), threads)
     value = steps_per * args.steps / dt
     line = {
         "impl": "reference", "metric": "particle-steps/s", "value": value,
@@ -180,7 +209,9 @@ def run_reference(args):
                    "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads,
                          "kind": kind,
-                         "sample": f"{sample} particles x 120 substeps per step, OpenMP dynamic,64"},
+                         "sample": f"{sample} particles x 120 substeps per step (Particle::move, "
+                                   "OpenMP dynamic,64) + Concentration::evaluate, one thread per "
+                                   "physical core (OMP_PLACES=cores, OMP_PROC_BIND=close)"},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -257,11 +288,12 @@ def run_realistic(args):
         live = engine.get_particles()
         sample = live[np.random.default_rng(0).permutation(len(live))[:65536]]
         sample = np.ascontiguousarray(np.sort(sample, order="id"))
-        threads = len(os.sched_getaffinity(0))
+        threads = physical_cores()
         rate, kind, n = cpu_reference_rate(win2, sample, cfg, threads, repeats=2, sample=65536)
         cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": kind,
-               "sample": f"{n} live particles x 240 substeps, one interval, OpenMP dynamic,64, "
-                         "median of 2 after a warm-up"}
+               "sample": f"{n} live particles x 240 substeps, one interval, Particle::move "
+                         "(OpenMP dynamic,64) + Concentration::evaluate, one thread per physical "
+                         "core, median of 2 after a warm-up"}
     line = {
         "metric": "particle-steps/s", "value": steps_total / (elapsed_ms / 1000.0),
         "unit": "particle-steps/s", "n_gpus": 1, "steps": n_steps, "warmup": warm,
@@ -364,11 +396,13 @@ def run_batched(args):
         win2.stokesV = np.ascontiguousarray([w[1] for w in stokes])
         sample = records[np.random.default_rng(0).permutation(n)[:65536]]
         sample = np.ascontiguousarray(np.sort(sample, order="id"))
-        threads = len(os.sched_getaffinity(0))
+        threads = physical_cores()
         rate, kind, m = cpu_reference_rate(win2, sample, cfg, threads, repeats=2, sample=65536)
         cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": kind,
                "sample": f"{m} records of the batch x 120 substeps, one interval with leeway "
-                         "drift, wind and Stokes, OpenMP dynamic,64, median of 2 after a warm-up"}
+                         "drift, wind and Stokes, Particle::move (OpenMP dynamic,64) + "
+                         "Concentration::evaluate, one thread per physical core, median of 2 "
+                         "after a warm-up"}
     line = {
         "metric": "particle-steps/s", "value": per_step / (mean_ms / 1000.0),
         "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps,
@@ -399,100 +433,206 @@ def run_batched(args):
     engine.close()
 
 
-def surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, dist, exchange):
-    """The FP16+surrogate arm: device-timed throughput on the same workload, the 24-hour error
-    against the FP64 reference-arithmetic kernel on a subset (rank 0), and the tensor roofline of
-    the per-particle kernel."""
+def timed_run(engine, args, n_intervals, exchange, barrier, steps=None, warmup=None):
+    """W untimed intervals, then K intervals enqueued back to back and device-timed with CUDA
+    events on the engine's stream (a barrier and a synchronize on both sides). The engine records
+    its dominant kernels' times per interval inside the same loop. Returns (elapsed ms,
+    particle-steps counted by the kernels, per-interval kernel times [K][3], kernel launches of
+    one interval)."""
     import torch
-    from wacommplusplus_b200.engine import Engine
-    from wacommplusplus_b200 import surrogate as sg
-
-    engine = Engine(local_rank, arithmetic="fp32", storage="fp16", surrogate=1)
-    engine.set_config(cfg)
-    engine.load_window(win)
-    engine.set_surrogate()
-    engine.set_particles(particles)
-    engine.concentration_reset(win.T)
-    n_intervals = win.T - 1
-    for s in range(args.warmup):
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    for s in range(warmup):
         engine.move_interval(s % n_intervals)
         exchange(engine, s % n_intervals)
-        engine.stats()
     ext = torch.cuda.ExternalStream(engine.stream)
     barrier()
     torch.cuda.synchronize()
+    engine.kernel_times()  # drop the warm-up records
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     engine.steps_total(reset=True)
     start.record(ext)
-    for s in range(args.steps):
-        t = (args.warmup + s) % n_intervals
+    for s in range(steps):
+        t = (warmup + s) % n_intervals
         engine.move_interval(t)
         exchange(engine, t)
     end.record(ext)
     torch.cuda.synchronize()
     barrier()
-    elapsed_ms = start.elapsed_time(end)
-    steps_total = engine.steps_total()
-    # per-launch kernel times and surrogate counts from three further intervals, one at a time
-    launches, step_ms, cell_ms, run, fallback = 0, [], [], 0, 0
-    for s in range(3):
-        t = (args.warmup + args.steps + s) % n_intervals
-        engine.move_interval(t)
-        exchange(engine, t)
-        st = engine.stats()
-        ss = engine.surrogate_stats()
-        launches = st["launches"] + 1  # + the device-side step accumulation
-        step_ms.append(ss["step_ms"])
-        cell_ms.append(ss["cell_ms"])
-        run += ss["run"] / 3
-        fallback += ss["fallback"] / 3
-    launches *= args.steps
-    if world > 1:
-        t = torch.tensor([elapsed_ms, steps_total], dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        elapsed_ms, steps_total = float(mx[0]), float(t[1])
-    engine.close()
-    kernel_ms = statistics.mean(step_ms)
-    per_launch_run = run
-    achieved = per_launch_run * SURROGATE_FLOP / (kernel_ms / 1000.0) / 1e12
+    launches = engine.stats()["launches"] + 1  # + the device-side step accumulation
+    return start.elapsed_time(end), engine.steps_total(), engine.kernel_times(), launches
+
+
+def over_ranks(dist, world, elapsed_ms, count):
+    """Max of the elapsed time and sum of the work over the ranks."""
+    if world <= 1:
+        return elapsed_ms, count
+    import torch
+    t = torch.tensor([elapsed_ms, count], dtype=torch.float64, device="cuda")
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(t[1])
+
+
+def error_stats(win, got, want, hours, against):
+    from wacommplusplus_b200 import surrogate as sg
+    err = sg.geo_error_m(win, got, want)
+    err = err[np.isfinite(err)]
+    return {"mean": float(err.mean()), "p99": float(np.quantile(err, 0.99)),
+            "max": float(err.max()), "hours": hours, "particles": int(len(got)),
+            "against": against}
+
+
+def run_hours(win, cfg, records, hours, local_rank, surrogate=False, **options):
+    """Records after `hours` intervals of one engine configuration."""
+    from wacommplusplus_b200.engine import Engine
+    e = Engine(local_rank, surrogate=int(surrogate), **options)
+    e.set_config(cfg)
+    e.load_window(win)
+    if surrogate:
+        e.set_surrogate()
+    e.set_particles(records)
+    for t in range(hours):
+        e.move_interval(t)
+    out = e.get_particles()
+    e.close()
+    return out
+
+
+FP64 = "FP64 reference-arithmetic kernel (parity-pinned to the oracle)"
+
+
+def nonuniform_error(local_rank, hours=24, n=65536):
+    """The surrogate's 24-hour error where its network acts: a streamfunction flow (64 Fourier
+    modes, rms 0.3 m/s, 256x256x12 Vtransform-2 grid at 0.0015 degrees, no land, seed held out
+    of training), deterministic, against the FP64 kernel; the plain FP32 step beside it."""
+    from wacommplusplus_b200 import synthetic as syn
+    from wacommplusplus_b200.surrogate_train import segment_particles, training_config
+    win = syn.RealisticForcing(eta=256, xi=256, s_rho=12, n_frames=hours + 1, seed=4242,
+                               dlon=0.0015, dlat=0.0015, land_fraction=0.0,
+                               water_border=0).window()
+    start = segment_particles(np.random.default_rng(1), win, 0, n)
+    start["time"] = win.times[0]
+    cfg = training_config()
+    truth = run_hours(win, cfg, start, hours, local_rank, arithmetic="reference")
+    surr = run_hours(win, cfg, start, hours, local_rank, surrogate=True, arithmetic="fp32",
+                     storage="fp16")
+    plain = run_hours(win, cfg, start, hours, local_rank, arithmetic="fp32", storage="fp16")
+    out = error_stats(win, surr, truth, hours, FP64)
+    out["flow"] = ("streamfunction of 64 Fourier modes, rms 0.3 m/s, wavelengths 2-50 km, "
+                   "256x256x12 grid at 0.0015 deg, no land")
+    out["plain_fp32_fp16_storage"] = error_stats(win, plain, truth, hours, FP64)
+    return out
+
+
+def surrogate_leg(args, win, particles, local_rank, world, rank, barrier, dist, exchange):
+    """The learned form (config 5 as specified): FP16 forcing storage, the tensor-core surrogate's
+    one-interval displacement and the plain stochastic operator every substep (Philox streams),
+    device-timed like the headline; beside it, on the same workload, the plain FP32 step with the
+    same random walk (the comparator of the >= 3x target) and the deterministic surrogate. Per-
+    interval kernel times come from the engine's event ring inside the timed loop."""
+    from wacommplusplus_b200.engine import Engine
+    from wacommplusplus_b200.types import default_config
+
+    n_intervals = win.T - 1
+
+    def arm(cfg, surrogate, **options):
+        e = Engine(local_rank, surrogate=int(surrogate), **options)
+        e.set_config(cfg)
+        e.load_window(win)
+        if surrogate:
+            e.set_surrogate()
+        e.set_particles(particles)
+        e.concentration_reset(win.T)
+        ms, count, kt, launches = timed_run(e, args, n_intervals, exchange, barrier)
+        ss = e.surrogate_stats() if surrogate else None
+        e.close()
+        ms, count = over_ranks(dist, world, ms, count)
+        return {"value": count / (ms / 1000.0), "ms_per_step": ms / args.steps,
+                "gpu_launches": launches * args.steps}, kt, ss, count / args.steps / world
+
+    rw = default_config(random=True)
+    walk, kt, ss, per_step = arm(rw, True, arithmetic="fp32", storage="fp16", rng="philox")
+    plain_rw, _, _, _ = arm(rw, False, arithmetic="fp32", storage="fp16", rng="philox")
+    det, kt_det, ss_det, _ = arm(default_config(random=False), True, arithmetic="fp32",
+                                 storage="fp16")
+    step_ms, walk_ms, fallback_ms = (float(x) for x in kt.mean(axis=0))
+    run = float(ss["run"])
     peak, peak_kind = measured_peaks("bf16_tflops", 1590.0)
+    achieved = run * SURROGATE_FLOP / (step_ms / 1000.0) / 1e12
+    hbm, hbm_kind = measured_peaks()
+    walk_gbs = per_step * B_ALG / (walk_ms / 1000.0) / 1e9
     per_particle = profile_traffic("surrogate_step_kernel_config3.md",
                                    "traffic_bytes_per_particle_interval")
-    traffic = None if per_particle is None else per_particle * per_launch_run
-    out = {"value": steps_total / (elapsed_ms / 1000.0), "unit": "particle-steps/s",
-           "ms_per_step": elapsed_ms / args.steps, "storage": "fp16",
-           "moved_by_surrogate_per_step": per_launch_run, "fallback_per_step": fallback,
-           "gpu_launches": launches,
-           "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                        "frac": achieved / peak, "peak_source": peak_kind,
-                        "kernel": "surrogate_step_kernel + surrogate_post_kernel",
-                        "kernel_ms": kernel_ms,
-                        "flop_per_particle_interval": SURROGATE_FLOP,
-                        "cell_kernel_ms": statistics.mean(cell_ms),
-                        "traffic": traffic}}
+    out = dict(walk)
+    out.update({
+        "unit": "particle-steps/s", "storage": "fp16", "rng": "philox",
+        "diffusion": "plain stochastic operator per substep (sigma 3.46 m, AKT-scaled vertical), "
+                     "surrogate displacement spread evenly over the substeps",
+        "moved_by_surrogate_per_step": run, "fallback_per_step": float(ss["fallback"]),
+        "vs_plain_random_walk": walk["value"] / plain_rw["value"],
+        "plain_random_walk": dict(plain_rw, note="plain FP32 step, same workload, storage, random "
+                                                 "walk and Philox streams"),
+        "deterministic": dict(det, note="random walk off: the closed-form displacement kernel",
+                              kernel_ms=[float(x) for x in kt_det.mean(axis=0)]),
+        "kernel_ms": {"step": step_ms, "walk": walk_ms, "fallback": fallback_ms,
+                      "timing": "per-interval events inside the timed loop, mean over K"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "kernel": "surrogate_step_kernel", "kernel_ms": step_ms,
+                     "flop_per_particle_interval": SURROGATE_FLOP,
+                     "traffic": None if per_particle is None else per_particle * run},
+        "walk_roofline": {"bound": "hbm", "achieved": walk_gbs, "peak": hbm, "unit": "GB/s",
+                          "frac": walk_gbs / hbm, "peak_source": hbm_kind,
+                          "kernel": "surrogate_walk_kernel", "kernel_ms": walk_ms,
+                          "algorithmic_bytes_per_particle_step": B_ALG},
+    })
     if rank == 0:
         n = min(len(particles), 1 << 20)
         sub = particles[:n].copy()
-        s_eng = Engine(local_rank, arithmetic="fp32", storage="fp16", surrogate=1)
-        x_eng = Engine(local_rank, arithmetic="reference")
-        for e in (s_eng, x_eng):
-            e.set_config(cfg)
-            e.load_window(win)
-            e.set_particles(sub)
-        s_eng.set_surrogate()
         hours = min(24, n_intervals)
-        for t in range(hours):
-            s_eng.move_interval(t)
-            x_eng.move_interval(t)
-        err = sg.geo_error_m(win, s_eng.get_particles(), x_eng.get_particles())
-        s_eng.close()
-        x_eng.close()
-        err = err[np.isfinite(err)]
-        out["error_m"] = {"mean": float(err.mean()), "p99": float(np.quantile(err, 0.99)),
-                          "max": float(err.max()), "hours": hours, "particles": n,
-                          "against": "FP64 reference-arithmetic kernel (parity-pinned to the oracle)"}
+        cfg = default_config(random=False)
+        truth = run_hours(win, cfg, sub, hours, local_rank, arithmetic="reference")
+        got = run_hours(win, cfg, sub, hours, local_rank, surrogate=True, arithmetic="fp32",
+                        storage="fp16")
+        out["error_m"] = error_stats(win, got, truth, hours, FP64)
+        out["error_m_nonuniform"] = nonuniform_error(local_rank)
+        out["_truth"] = truth
+    return out
+
+
+def precision_leg(args, win, particles, local_rank, truth, exchange, barrier):
+    """The precision form: the plain FP32 step with FP32, FP16 and BF16 forcing storage, each
+    device-timed on the full workload (a shorter run) with its 24-hour error on the 1,048,576-
+    particle subset against the FP64 kernel; and the FP64 reference-arithmetic kernel's own
+    throughput on the full workload."""
+    from wacommplusplus_b200.engine import Engine
+    from wacommplusplus_b200.types import default_config
+    cfg = default_config(random=False)
+    n_intervals = win.T - 1
+    hours = min(24, n_intervals)
+    sub = particles[:len(truth)]
+    out = {}
+    for storage, arithmetic in (("fp32", "fp32"), ("fp16", "fp32"), ("bf16", "fp32"),
+                                ("fp32", "reference")):
+        e = Engine(local_rank, arithmetic=arithmetic, storage=storage)
+        e.set_config(cfg)
+        e.load_window(win)
+        e.set_particles(particles)
+        steps = min(args.steps, 10 if arithmetic == "fp32" else 4)
+        ms, count, kt, _ = timed_run(e, args, n_intervals, exchange, barrier, steps=steps,
+                                     warmup=3)
+        e.close()
+        key = f"{storage}_storage" if arithmetic == "fp32" else "fp64_mode"
+        entry = {"value": count / (ms / 1000.0), "ms_per_step": ms / steps, "steps": steps,
+                 "kernel_ms": float(kt[:, 0].mean())}
+        if arithmetic == "fp32":
+            got = run_hours(win, cfg, sub, hours, local_rank, arithmetic="fp32", storage=storage)
+            entry["error_m"] = error_stats(win, got, truth, hours, FP64)
+        else:
+            entry["note"] = "reference arithmetic (FP64, parity to 1e-9 deg), FP32 storage"
+        out[key] = entry
     return out
 
 
@@ -508,6 +648,7 @@ def main():
     parser.add_argument("--no-e2e", action="store_true")
     parser.add_argument("--no-cpu", action="store_true")
     parser.add_argument("--no-surrogate", action="store_true")
+    parser.add_argument("--no-precision", action="store_true")
     parser.add_argument("--scenarios", type=int, default=256,
                         help="batched workload: number of scenarios")
     parser.add_argument("--workload", default="precision",
@@ -543,12 +684,13 @@ def main():
     win, particles, cfg = workload(args.particles, rank)
     cpu = None
     if rank == 0 and not args.no_cpu:
-        threads = len(os.sched_getaffinity(0))
+        threads = physical_cores()
         rate, kind, sample = cpu_reference_rate(win, particles, cfg, threads)
         rate1, _, sample1 = cpu_reference_rate(win, particles, cfg, 1, repeats=1, sample=16384)
         cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": kind,
-               "sample": f"{sample} particles x 120 substeps, one interval, OpenMP dynamic,64, "
-                         f"median of 3 after a warm-up",
+               "sample": f"{sample} particles x 120 substeps, one interval: Particle::move "
+                         "(OpenMP dynamic,64) + Concentration::evaluate, one thread per physical "
+                         "core (OMP_PLACES=cores, OMP_PROC_BIND=close), median of 3 after a warm-up",
                "value_1core": rate1}
 
     from wacommplusplus_b200 import sharding
@@ -569,58 +711,28 @@ def main():
         if world > 1:
             sharding.allreduce_concentration(eng, t + 1)
 
-    for s in range(args.warmup):
-        engine.move_interval(s % n_intervals)
-        exchange(engine, s % n_intervals)
-        engine.stats()
-    ext = torch.cuda.ExternalStream(engine.stream)
     sampler = ClockSampler(physical_gpu(local_rank))
     sampler.start()
-    barrier()
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # the K intervals are enqueued back to back; the kernels count their particle-steps on the
-    # device, read once after the timed region
-    engine.steps_total(reset=True)
-    start.record(ext)
-    for s in range(args.steps):
-        t = (args.warmup + s) % n_intervals
-        engine.move_interval(t)
-        exchange(engine, t)
-    end.record(ext)
-    torch.cuda.synchronize()
-    barrier()
+    # device, read once after the timed region, and the move kernel of every interval is timed by
+    # events recorded inside the same loop
+    elapsed_ms, steps_total, kt, launches = timed_run(engine, args, n_intervals, exchange, barrier)
     clocks = sampler.stop()
-    elapsed_ms = start.elapsed_time(end)
-    steps_total = engine.steps_total()
-    # per-launch kernel times for the roofline, from three further intervals read one at a time
-    launches, move_ms, move_steps = 0, [], []
-    for s in range(3):
-        t = (args.warmup + args.steps + s) % n_intervals
-        engine.move_interval(t)
-        exchange(engine, t)
-        st = engine.stats()
-        launches = st["launches"] + 1  # + the device-side step accumulation
-        move_ms.append(st["move_ms"])
-        move_steps.append(st["particle_steps"])
     launches *= args.steps
-    if world > 1:
-        t = torch.tensor([elapsed_ms, steps_total], dtype=torch.float64, device="cuda")
-        mx = t.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        elapsed_ms, steps_total = float(mx[0]), float(t[1])
+    per_launch_steps = steps_total / args.steps
+    elapsed_ms, steps_total = over_ranks(dist, world, elapsed_ms, steps_total)
     value = steps_total / (elapsed_ms / 1000.0)
 
-    kernel_ms = statistics.mean(move_ms)
-    per_launch_steps = statistics.mean(move_steps)
+    kernel_ms = float(kt[:, 0].mean())
     achieved = per_launch_steps * B_ALG / (kernel_ms / 1000.0) / 1e9
     peak, peak_kind = measured_peaks()
     traffic_per_step = profile_traffic()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": None if traffic_per_step is None else traffic_per_step * per_launch_steps,
-                "kernel": "move_fast_kernel (FP32 step)" if args.arithmetic == "fp32" else "move_soa_kernel (reference arithmetic)", "kernel_ms": kernel_ms,
+                "kernel": "move_fast_kernel (FP32 step)" if args.arithmetic == "fp32" else "move_soa_kernel (reference arithmetic)",
+                "kernel_ms": kernel_ms,
+                "kernel_ms_timing": "per-interval events inside the timed loop, mean over K",
                 "algorithmic_bytes_per_particle_step": B_ALG}
 
     e2e = None
@@ -665,10 +777,16 @@ def main():
                "timing": "wall clock around K steps of upload_frame_async (record of the interval after "
                          "next, from page-locked memory) + move_interval_host"}
 
-    surrogate = None
+    engine.close()
+    surrogate = precision = None
     if not args.no_surrogate:
-        surrogate = surrogate_leg(args, win, particles, cfg, local_rank, world, rank, barrier, dist,
+        surrogate = surrogate_leg(args, win, particles, local_rank, world, rank, barrier, dist,
                                   exchange)
+        truth = surrogate.pop("_truth", None)
+        if rank == 0 and not args.no_precision:
+            # rank 0 alone, no collectives: the other ranks wait at the final barrier
+            precision = precision_leg(args, win, particles, local_rank, truth,
+                                      lambda eng, t: None, lambda: None)
 
     if rank == 0:
         line = {
@@ -690,14 +808,15 @@ def main():
                                       "per interval"},
             "roofline": roofline,
             "surrogate": surrogate,
+            "precision": precision,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
-    engine.close()
     if world > 1:
+        dist.barrier()
         dist.destroy_process_group()
 
 
