@@ -2,8 +2,10 @@
 // the way a WaComM++ build would after replacing its per-interval staging (Wacomm.cpp:386-610):
 // one context, a rectilinear grid, two forcing records of a uniform eastward current, particles
 // in, one interval in reference arithmetic, particles out. Every particle must end where the
-// uniform current puts it: i + u * 3600 / xdist(row), with xdist the haversine cell width the
-// reference uses (kernel.cu:145-149); j, k and the age as they were plus one hour.
+// uniform current puts it, i + u * 3600 / xdist(row) with xdist the haversine cell width
+// (kernel.cu:145-149), within 1e-6 grid units (0.2 mm: the reference's per-cell metric and
+// midpoint rescaling differ from this closed form in the ninth digit); j and k unchanged and
+// the age one hour.
 // Build: g++ -std=c++17 abi_caller.cpp -I include -L <lib dir> -lwacomm_b200. Exit 0: passed;
 // 77: no CUDA device; 1: a call failed or a record is off.
 #include <cmath>
@@ -95,7 +97,7 @@ int main() {
         const int row = (int)std::floor(p[q].j);
         const double xdist = haversine(lat[row * xi], lon[row * xi], lat[row * xi + 1], lon[row * xi + 1]);
         const double want = p[q].i + u0 * 3600.0 / xdist;
-        const bool ok = std::fabs(out[q].i - want) <= 1e-9 && out[q].j == p[q].j &&
+        const bool ok = std::fabs(out[q].i - want) <= 1e-6 && out[q].j == p[q].j &&
                         out[q].k == p[q].k && out[q].age == 3600.0 && out[q].health > 0 &&
                         out[q].id == p[q].id;
         if (!ok && bad++ < 5)

@@ -955,15 +955,40 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
         const float jN = jF + dJ, iN = iF + dI, kN = fmaf(-zleap, rzdist, kF);
         const bool vertical = (float)kI - kN > 0.f || (float)kI - kN < kLowerF;
         bool done = false;
-        if (!vertical && jN >= 0.f && jN < 1.f && iN >= 0.f && iN < 1.f) {
-            // same cell, no vertical closure: the shore test at the destination in the kept surface
-            if (surface_from(surf, jN, iN).height(alpha) > shore) {
-                jF = jN;
-                iF = iN;
+        if (!vertical) {
+            // no vertical closure: a landing in water (this cell or another valid one) stays FP32
+            // work on the fraction; a cell change is taken here too, so that the lanes of a warp
+            // stay together on the frequent crossings
+            const float cj = floorf(jN), ci = floorf(iN);
+            if (cj == 0.f && ci == 0.f) {
+                if (surface_from(surf, jN, iN).height(alpha) > shore) done = true;
+            } else {
+                const int nj = jI + (int)cj, ni = iI + (int)ci;
+                if (valid_cell(nj, ni, eta, xi)) {
+                    const int ncell = nj * xi + ni;
+                    const CellSurface there = load_surface(W.surface, ncell);
+                    const float fj = jN - cj, fi = iN - ci;
+                    if (surface_from(there, fj, fi).height(alpha) > shore) {
+                        jI = nj;
+                        iI = ni;
+                        surf = there;
+                        inv = __ldg(W.invMetric + ncell);
+                        keptCell = ncell;
+                        keptK = 1;  // the new cell's AKT at the next substep
+                        jF = fj;
+                        iF = fi;
+                        done = true;
+                    }
+                }
+            }
+            if (done) {
+                if (cj == 0.f && ci == 0.f) {
+                    jF = jN;
+                    iF = iN;
+                }
                 const float c = floorf(kN);  // level crossing
                 kI -= (int)c;
                 kF = kN - c;
-                done = true;
             }
         }
         if (!done) {
