@@ -847,6 +847,8 @@ struct WalkView {
     const float *depth;              // [sW-1] FP32 depthIntervals
 };
 
+constexpr int WALK_BLOCKS = 5;  // resident blocks of 128 threads per SM the registers allow
+
 __device__ __forceinline__ CellSurface load_surface(const CellSurface *s, int cell) {
     const float4 *q = reinterpret_cast<const float4 *>(s + cell);
     return CellSurface{__ldg(q), __ldg(q + 1)};
@@ -859,14 +861,16 @@ __device__ __forceinline__ CellSurface load_surface(const CellSurface *s, int ce
 // vertically, the vertical cap, the vertical and horizontal closures, survival and age.
 //
 // The position is kept as a cell (or level) index plus an FP32 fraction, with the FP64 remainder
-// of the start position carried alongside: a substep that stays in its cell and level and needs
-// no closure is FP32 work on the fraction, with the cell's AKT, surface, metric and layer
-// thickness held in registers since the last move to another cell or level; any other substep
-// (a cell change, a closure) runs in FP64 as the plain step does. Returns the substeps taken.
+// of the start position carried alongside. Every substep reads its cell's surface, metric and AKT
+// records and its destination's surface unconditionally (a particle stays in a cell for tens of
+// substeps, so these hit L1), and a landing in water without a closure is FP32 work on the
+// fraction, whether or not it changes cell: the lanes of a warp take the same path. Only a
+// closure (shore, domain edge, surface, bottom) runs the plain step's FP64 landing. Returns the
+// substeps taken.
 template <int SEM, int STORE>
 __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams &P,
-                             const WalkView<STORE> &W, int eta, int xi, int sW, ParticleState &p,
-                             float rateX, float rateY, float rateZ) {
+                             const WalkView<STORE> &W, const float *depthS, int eta, int xi,
+                             int sW, ParticleState &p, float rateX, float rateY, float rateZ) {
     const double length = P.length, invLength = 1.0 / length, kLower = P.kLower;
     const float shore = (float)cfg.shoreLimit, kLowerF = (float)kLower;
     const float invKLower = (float)P.invKLower, sigma = (float)cfg.sigma, crid = (float)cfg.crid;
@@ -883,12 +887,6 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
     float jF = (float)(p.j - fj), iF = (float)(p.i - fi), kF = (float)(ck - p.k);
     double jLo = (p.j - fj) - (double)jF, iLo = (p.i - fi) - (double)iF;
     double kLo = (ck - p.k) - (double)kF;
-
-    int keptCell = -1, keptK = 1;
-    CellSurface surf{};
-    float2 inv{0.f, 0.f};
-    QuadPair aUp{}, aLo{};
-    float depth = 0.f;
 
     while (elapsed < length) {
         const double stepDt = fmin(cfg.dti, length - elapsed);
@@ -908,19 +906,13 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
         steps++;
         const int kM = mem_level(kI, sW);
         const int cell = jI * xi + iI;
-        if (cell != keptCell) {
-            surf = load_surface(W.surface, cell);
-            inv = __ldg(W.invMetric + cell);
-            keptCell = cell;
-            keptK = 1;
-        }
-        if (kM != keptK) {
-            const CellQuad<STORE> *col = W.columns + ((size_t)cell * sW + (size_t)(kM + sW - 1)) * 2;
-            load_second<STORE>(col - 1, aLo);  // akt of W level kI-1
-            load_second<STORE>(col + 1, aUp);  // akt of W level kI
-            depth = __ldg(W.depth + (kM + sW - 2));
-            keptK = kM;
-        }
+        const CellSurface surf = load_surface(W.surface, cell);
+        const float2 inv = __ldg(W.invMetric + cell);
+        QuadPair aUp, aLo;
+        const CellQuad<STORE> *col = W.columns + ((size_t)cell * sW + (size_t)(kM + sW - 1)) * 2;
+        load_second<STORE>(col - 1, aLo);  // akt of W level kI-1
+        load_second<STORE>(col + 1, aUp);  // akt of W level kI
+        const float depth = depthS[kM + sW - 2];
         const float dt = (float)stepDt;
         const float alpha = (float)((elapsed + 0.5 * stepDt) * invLength);
         const float hc = surface_from(surf, jF, iF).height(alpha);
@@ -953,60 +945,36 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
         float zleap = fmaf(rateZ, dt, rz);
         if (fabsf(zleap) > zdist) zleap = signf_of(zdist, zleap);
         const float jN = jF + dJ, iN = iF + dI, kN = fmaf(-zleap, rzdist, kF);
+        // the destination's cell and its surface (this cell's, read again, in the common case)
+        const float cj = floorf(jN), ci = floorf(iN);
+        const int nj = jI + (int)cj, ni = iI + (int)ci;
+        const bool inside = valid_cell(nj, ni, eta, xi);
+        const float jD = jN - cj, iD = iN - ci;
+        const CellSurface there = load_surface(W.surface, inside ? nj * xi + ni : cell);
         const bool vertical = (float)kI - kN > 0.f || (float)kI - kN < kLowerF;
-        bool done = false;
-        if (!vertical) {
-            // no vertical closure: a landing in water (this cell or another valid one) stays FP32
-            // work on the fraction; a cell change is taken here too, so that the lanes of a warp
-            // stay together on the frequent crossings
-            const float cj = floorf(jN), ci = floorf(iN);
-            if (cj == 0.f && ci == 0.f) {
-                if (surface_from(surf, jN, iN).height(alpha) > shore) done = true;
-            } else {
-                const int nj = jI + (int)cj, ni = iI + (int)ci;
-                if (valid_cell(nj, ni, eta, xi)) {
-                    const int ncell = nj * xi + ni;
-                    const CellSurface there = load_surface(W.surface, ncell);
-                    const float fj = jN - cj, fi = iN - ci;
-                    if (surface_from(there, fj, fi).height(alpha) > shore) {
-                        jI = nj;
-                        iI = ni;
-                        surf = there;
-                        inv = __ldg(W.invMetric + ncell);
-                        keptCell = ncell;
-                        keptK = 1;  // the new cell's AKT at the next substep
-                        jF = fj;
-                        iF = fi;
-                        done = true;
-                    }
-                }
-            }
-            if (done) {
-                if (cj == 0.f && ci == 0.f) {
-                    jF = jN;
-                    iF = iN;
-                }
-                const float c = floorf(kN);  // level crossing
-                kI -= (int)c;
-                kF = kN - c;
-            }
-        }
-        if (!done) {
-            // the plain step's FP64 landing and closures (cell change, shore, closures)
+        if (inside && !vertical && surface_from(there, jD, iD).height(alpha) > shore) {
+            jI = nj;
+            iI = ni;
+            jF = jD;
+            iF = iD;
+            const float c = floorf(kN);  // level crossing
+            kI -= (int)c;
+            kF = kN - c;
+        } else {
+            // a closure: the plain step's FP64 landing (Particle.cpp:644-791)
             const double pj = (double)jI + (double)jF + jLo, pi = (double)iI + (double)iF + iLo;
             const double pk = (double)kI - (double)kF - kLo;
             double jdet = pj + (double)dJ, idet = pi + (double)dI;
             double kdet = pk + (double)(zleap * rzdist);
             if (kdet > 0.) close_upper(cfg, kdet, p.health, lazy);
             if (kdet < kLower) close_lower(cfg, kLower, kdet, p.health, lazy);
-            double nj = pj, ni = pi, nk = pk;
+            double nJ = pj, nI = pi, nK = pk;
             const double fjd = floor(jdet), fid = floor(idet);
             const int jdetI = to_index<SEM>(fjd), idetI = to_index<SEM>(fid);
             if (valid_cell(jdetI, idetI, eta, xi)) {
-                const int dcell = jdetI * xi + idetI;
-                const CellSurface there = dcell == keptCell ? surf : load_surface(W.surface, dcell);
+                const CellSurface at = load_surface(W.surface, jdetI * xi + idetI);
                 const float hcdet =
-                    surface_from(there, (float)(jdet - fjd), (float)(idet - fid)).height(alpha);
+                    surface_from(at, (float)(jdet - fjd), (float)(idet - fid)).height(alpha);
                 if (hcdet <= shore) {
                     if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
                         idet = pi;
@@ -1019,31 +987,31 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
                         jdet = reflect_cell(pj, jI, jdet, jdetI);
                     }
                 }
-                ni = idet;
-                nj = jdet;
-                nk = kdet;
+                nI = idet;
+                nJ = jdet;
+                nK = kdet;
             } else {
                 if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
-                    nk = kdet;
+                    nK = kdet;
                 } else if (cfg.horizontalClosure == CLOSURE_KILL) {
                     p.health = -1;
                     lazy = false;
                 } else if (cfg.horizontalClosure == CLOSURE_REFLECTION) {
-                    ni = reflect_domain(idet, xi - 1);
-                    nj = reflect_domain(jdet, eta - 1);
-                    nk = kdet;
+                    nI = reflect_domain(idet, xi - 1);
+                    nJ = reflect_domain(jdet, eta - 1);
+                    nK = kdet;
                 }
             }
-            const double gj = floor(nj), gi = floor(ni), gk = ceil(nk);
+            const double gj = floor(nJ), gi = floor(nI), gk = ceil(nK);
             jI = to_index<SEM>(gj);
             iI = to_index<SEM>(gi);
             kI = to_index<SEM>(gk);
-            jF = (float)(nj - gj);
-            iF = (float)(ni - gi);
-            kF = (float)(gk - nk);
-            jLo = (nj - gj) - (double)jF;
-            iLo = (ni - gi) - (double)iF;
-            kLo = (gk - nk) - (double)kF;
+            jF = (float)(nJ - gj);
+            iF = (float)(nI - gi);
+            kF = (float)(gk - nK);
+            jLo = (nJ - gj) - (double)jF;
+            iLo = (nI - gi) - (double)iF;
+            kLo = (gk - nK) - (double)kF;
         }
         const bool alive = lazy ? (p.age < P.ageUnder || exp(-p.age / cfg.tau0) > 0) : p.health > 0;
         if (alive) {
@@ -1065,9 +1033,12 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
 // every substep of the interval by walk_particle. Rows the step kernel handed back go to the
 // fallback list.
 template <int SEM, int STORE>
-__global__ void __launch_bounds__(128, 4)
+__global__ void __launch_bounds__(128, WALK_BLOCKS)
     surrogate_walk_kernel(const StepArgs a, const wacomm_b200_config cfg, const IntervalParams P,
                           const WalkView<STORE> W, ParticleSoA S, const MoveLaunch L) {
+    __shared__ float depthS[64];  // FP32 layer thicknesses (sW - 1 <= 64 levels)
+    for (int q = threadIdx.x; q < a.sW - 1 && q < 64; q += blockDim.x) depthS[q] = W.depth[q];
+    __syncthreads();
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     const bool write = n < L.count && !(L.err && (*L.err & ERR_SURROGATE_WAIT));
     long long concCell = -1;
@@ -1104,7 +1075,9 @@ __global__ void __launch_bounds__(128, 4)
             const float rateX = fmaf(OUT_H * row.x * gate, invTrem, ub);
             const float rateY = fmaf(OUT_H * row.y * gate, invTrem, vb);
             const float rateZ = fmaf(OUT_V * row.z * gate, invTrem, wb + (float)a.sv);
-            steps = walk_particle<SEM, STORE>(cfg, P, W, a.eta, a.xi, a.sW, p, rateX, rateY, rateZ);
+            const float *depth = a.sW - 1 <= 64 ? depthS : W.depth;  // deeper grids: global copy
+            steps = walk_particle<SEM, STORE>(cfg, P, W, depth, a.eta, a.xi, a.sW, p, rateX, rateY,
+                                              rateZ);
             S.j[slot] = p.j;
             S.i[slot] = p.i;
             S.k[slot] = p.k;
