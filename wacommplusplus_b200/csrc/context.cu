@@ -745,6 +745,17 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     st.cellSurface = A.cellSurface;
     st.invMetric = A.invMetric;
     st.depthF = A.depthIntervalsF;
+    if (diffuse && ctx->opt.sort_by_cell) {
+        // the walk takes its particles in cell order; the sort walks the previous order
+        const std::vector<size_t> whole{0, ctx->n};
+        const uint32_t *seqIn = ctx->seqBounds == whole ? ctx->dSeq : nullptr;
+        ctx->seqBounds.clear();
+        if ((rc = sort_work(ctx, ctx->S.s, count, ctx->dKeys, ctx->dOrder, seqIn, ctx->dSeq,
+                            launches)))
+            return rc;
+        ctx->seqBounds = whole;
+        st.walkOrder = ctx->dOrder;
+    }
     st.dry = ctx->dDry;
     st.z = ctx->dZ;
     st.corners = ctx->dCorners;

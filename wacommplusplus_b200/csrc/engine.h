@@ -223,6 +223,7 @@ struct SurrogateStep {
     const float2 *invMetric = nullptr;
     const float *depthF = nullptr;
     cudaEvent_t midEvent = nullptr;  // recorded between the step kernel and the post/walk kernel
+    const uint32_t *walkOrder = nullptr;  // cell order of the walk kernel's work (null: slot order)
 };
 
 // Kernel attributes of the tensor-core kernels (once per device; outside stream capture).

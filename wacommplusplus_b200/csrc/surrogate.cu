@@ -1028,7 +1028,8 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
 }
 
 // Learned advection with the plain stochastic operator per substep (diffusive forward intervals):
-// one thread per work item in slot order. The rates come from the item's layer-4 outputs and the
+// one thread per work item, taken in cell order (the engine's cell sort) so that the lanes of a
+// warp share their cell's records and meet the same closures. The rates come from the item's layer-4 outputs and the
 // start-point velocity of its corner record, as in surrogate_post_kernel; the particle then takes
 // every substep of the interval by walk_particle. Rows the step kernel handed back go to the
 // fallback list.
@@ -1045,10 +1046,10 @@ __global__ void __launch_bounds__(128, WALK_BLOCKS)
     int steps = 0;
     bool run = false;
     if (write) {
-        const float4 row = a.rows[n];
+        const uint32_t slot = L.order ? L.order[n] : (uint32_t)n;  // cell order of the walk
+        const float4 row = a.rows[slot];  // the step kernel's rows follow the slots
         const int code = __float_as_int(row.w);
         const int status = code >= 0 ? ROW_RUN : (code == ROW_CODE_FALLBACK ? ROW_FALLBACK : ROW_NONE);
-        const uint32_t slot = L.order ? L.order[n] : (uint32_t)n;
         ParticleState p;
         p.j = S.j[slot];
         p.i = S.i[slot];
@@ -1279,7 +1280,9 @@ cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const M
         W.surface = static_cast<const CellSurface *>(s.cellSurface);
         W.invMetric = s.invMetric;
         W.depth = s.depthF;
-        surrogate_walk_kernel<SEM, STORE><<<blocks128, 128, 0, stream>>>(a, s.cfg, *s.interval, W, S, L);
+        MoveLaunch LW = L;
+        LW.order = s.walkOrder;
+        surrogate_walk_kernel<SEM, STORE><<<blocks128, 128, 0, stream>>>(a, s.cfg, *s.interval, W, S, LW);
         return cudaGetLastError();
     };
     using Host = std::integral_constant<int, SEM_HOST>;
