@@ -121,16 +121,22 @@ class ClockSampler:
 
 
 def physical_cores():
-    """Physical cores among the CPUs this process may run on (one per (package, core) pair)."""
+    """(count, how) of the physical cores among the CPUs this process may run on: one per
+    (package, core) pair of the CPU topology. Where the topology is not exposed (a virtual machine
+    may report every CPU as core 0, or more than two CPUs per core), the logical CPUs are counted
+    and `how` says so."""
+    cpus = sorted(os.sched_getaffinity(0))
     seen = set()
-    for cpu in sorted(os.sched_getaffinity(0)):
+    for cpu in cpus:
         base = f"/sys/devices/system/cpu/cpu{cpu}/topology/"
         try:
             with open(base + "core_id") as a, open(base + "physical_package_id") as b:
                 seen.add((b.read().strip(), a.read().strip()))
         except OSError:
-            seen.add(("cpu", str(cpu)))
-    return max(1, len(seen))
+            return len(cpus), "logical CPUs (no CPU topology exposed)"
+    if not seen or len(cpus) > 2 * len(seen):
+        return len(cpus), "logical CPUs (the CPU topology reports fewer cores than plausible)"
+    return len(seen), "physical cores (CPU topology)"
 
 
 def physical_gpu(local_rank):
@@ -187,7 +193,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    threads = physical_cores()
+    threads, how = physical_cores()
     win, particles, cfg = workload(1 << 18, 0)
     from oracle import bindings as ob
     kind = "reference" if ob.ref_available() else "port"
@@ -208,7 +214,7 @@ def run_reference(args):
                                f"{sample} particles per step (bounded CPU sample), midpoint, dt=30 s",
                    "l2": "inputs larger than L2"},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads,
-                         "kind": kind,
+                         "cores_counted_as": how, "kind": kind,
                          "sample": f"{sample} particles x 120 substeps per step (Particle::move, "
                                    "OpenMP dynamic,64) + Concentration::evaluate, one thread per "
                                    "physical core (OMP_PLACES=cores, OMP_PROC_BIND=close)"},
@@ -288,9 +294,10 @@ def run_realistic(args):
         live = engine.get_particles()
         sample = live[np.random.default_rng(0).permutation(len(live))[:65536]]
         sample = np.ascontiguousarray(np.sort(sample, order="id"))
-        threads = physical_cores()
+        threads, how = physical_cores()
         rate, kind, n = cpu_reference_rate(win2, sample, cfg, threads, repeats=2, sample=65536)
-        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": kind,
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads,
+               "cores_counted_as": how, "kind": kind,
                "sample": f"{n} live particles x 240 substeps, one interval, Particle::move "
                          "(OpenMP dynamic,64) + Concentration::evaluate, one thread per physical "
                          "core, median of 2 after a warm-up"}
@@ -396,9 +403,10 @@ def run_batched(args):
         win2.stokesV = np.ascontiguousarray([w[1] for w in stokes])
         sample = records[np.random.default_rng(0).permutation(n)[:65536]]
         sample = np.ascontiguousarray(np.sort(sample, order="id"))
-        threads = physical_cores()
+        threads, how = physical_cores()
         rate, kind, m = cpu_reference_rate(win2, sample, cfg, threads, repeats=2, sample=65536)
-        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": kind,
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads,
+               "cores_counted_as": how, "kind": kind,
                "sample": f"{m} records of the batch x 120 substeps, one interval with leeway "
                          "drift, wind and Stokes, Particle::move (OpenMP dynamic,64) + "
                          "Concentration::evaluate, one thread per physical core, median of 2 "
@@ -684,10 +692,11 @@ def main():
     win, particles, cfg = workload(args.particles, rank)
     cpu = None
     if rank == 0 and not args.no_cpu:
-        threads = physical_cores()
+        threads, how = physical_cores()
         rate, kind, sample = cpu_reference_rate(win, particles, cfg, threads)
         rate1, _, sample1 = cpu_reference_rate(win, particles, cfg, 1, repeats=1, sample=16384)
-        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads, "kind": kind,
+        cpu = {"value": rate, "unit": "particle-steps/s", "cores": threads,
+               "cores_counted_as": how, "kind": kind,
                "sample": f"{sample} particles x 120 substeps, one interval: Particle::move "
                          "(OpenMP dynamic,64) + Concentration::evaluate, one thread per physical "
                          "core (OMP_PLACES=cores, OMP_PROC_BIND=close), median of 3 after a warm-up",
