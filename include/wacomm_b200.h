@@ -385,6 +385,14 @@ int wacomm_b200_last_interval_stats(const wacomm_b200_context *ctx, float *devic
  * outside the valid cells use the FP32 step. */
 int wacomm_b200_set_surrogate(wacomm_b200_context *ctx, const float *parameters, size_t count);
 
+/* No counterpart in the reference. A trust limit for the surrogate, in metres per interval: a
+ * particle whose estimated one-interval error exceeds it goes to the FP32 step instead. The
+ * estimate is the start-point method's error |grad u| |u| t^2 / 2 over the remaining time t, with
+ * the velocity gradient taken from the RMS deviation of the particle's 4x4x4 stencil over 1.5
+ * cells; a uniform stencil always stays with the surrogate (its start-point displacement is
+ * exact there). metres > 0; INFINITY (the default) turns the limit off. */
+int wacomm_b200_set_surrogate_error_limit(wacomm_b200_context *ctx, double metres);
+
 /* Of the last move_interval with the surrogate on: particles it moved, particles handed to the
  * FP32 step, and device milliseconds of the per-cell layer-1 kernel and of the particle kernel. */
 int wacomm_b200_last_surrogate_stats(const wacomm_b200_context *ctx, size_t *run, size_t *fallback,

@@ -104,6 +104,7 @@ SIGNATURES = {
     "wacomm_b200_synchronize": (_i, [_vp]),
     "wacomm_b200_last_interval_stats": (_i, [_vp, _fp, _fp, ctypes.POINTER(_i), _dp]),
     "wacomm_b200_kernel_times": (_i, [_vp, _fp, _i, ctypes.POINTER(_i)]),
+    "wacomm_b200_set_surrogate_error_limit": (_i, [_vp, ctypes.c_double]),
     "wacomm_b200_stream": (_i, [_vp, ctypes.POINTER(_vp)]),
     "wacomm_b200_set_surrogate": (_i, [_vp, _fp, _sz]),
     "wacomm_b200_last_surrogate_stats": (_i, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz), _fp,

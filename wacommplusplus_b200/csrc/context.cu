@@ -131,6 +131,7 @@ struct wacomm_b200_context {
     cudaEvent_t evCell0 = nullptr, evCell1 = nullptr, evStep0 = nullptr, evStep1 = nullptr;
     bool surrTimed = false;  // the events of the last eager surrogate interval can be read
     bool surrRan = false;    // dSurrCounts holds the counts of a surrogate interval (eager or captured)
+    float surrMaxError = INFINITY;  // wacomm_b200_set_surrogate_error_limit
     int smCount = 148;
 
     double *dGeoLon = nullptr, *dGeoLat = nullptr, *dSWValues = nullptr;  // kji2deplatlon grid
@@ -738,6 +739,7 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     Q.chunkEnd = INFINITY;
     const PackedArgs A = packed_args(ctx);
     st.walk = diffuse ? 1 : 0;
+    st.maxError = ctx->surrMaxError;
     st.semantics = ctx->opt.semantics;
     st.storage = ctx->opt.storage;
     st.interval = &Q;
@@ -1665,6 +1667,15 @@ int wacomm_b200_set_surrogate(wacomm_b200_context *ctx, const float *parameters,
     return WACOMM_B200_OK;
 }
 
+int wacomm_b200_set_surrogate_error_limit(wacomm_b200_context *ctx, double metres) {
+    if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
+    if (!(metres > 0))
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "error limit %g: must be > 0 (infinity: off)",
+                    metres);
+    ctx->surrMaxError = (float)metres;
+    return WACOMM_B200_OK;
+}
+
 int wacomm_b200_last_surrogate_stats(const wacomm_b200_context *ctx, size_t *run, size_t *fallback,
                                      float *cell_ms, float *step_ms) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
@@ -2116,6 +2127,13 @@ std::vector<uint64_t> layout_of(const wacomm_b200_context *ctx) {
     bytes(ctx->times.data(), ctx->times.size() * sizeof(double));
     bytes(&ctx->cfg, sizeof ctx->cfg);
     bytes(&ctx->opt, sizeof ctx->opt);
+    // the learned form's buffers and its trust limit
+    for (const void *p : {(const void *)ctx->dSurrogate, (const void *)ctx->dZ,
+                          (const void *)ctx->dCorners, (const void *)ctx->dDry,
+                          (const void *)ctx->dFallback, (const void *)ctx->dSurrRows,
+                          (const void *)ctx->dSurrCounts})
+        add(p);
+    bytes(&ctx->surrMaxError, sizeof ctx->surrMaxError);
     return f;
 }
 

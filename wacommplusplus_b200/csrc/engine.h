@@ -1,6 +1,7 @@
 // Host-side declarations of the engine's kernel launchers (defined in the .cu units).
 #pragma once
 
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -224,6 +225,7 @@ struct SurrogateStep {
     const float *depthF = nullptr;
     cudaEvent_t midEvent = nullptr;  // recorded between the step kernel and the post/walk kernel
     const uint32_t *walkOrder = nullptr;  // cell order of the walk kernel's work (null: slot order)
+    float maxError = INFINITY;  // trust limit of the prediction, metres per interval (off: INFINITY)
 };
 
 // Kernel attributes of the tensor-core kernels (once per device; outside stream capture).

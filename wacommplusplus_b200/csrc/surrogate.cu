@@ -89,7 +89,8 @@ struct alignas(16) CellCorners {
     float zeta[2][4];
     float h[4];
     double invXdist, invYdist, depth;  // reciprocal cell metric, depthIntervals(kI)
-    float gate, pad;
+    float gate;   // min(1, sigma / GATE_SIGMA): the weight of the network's correction
+    float sigma;  // RMS deviation (m/s) of the stencil's u, v from the cell's own corner
 };
 static_assert(sizeof(CellCorners) == 208, "corner record layout");
 
@@ -291,8 +292,8 @@ __global__ void __launch_bounds__(128, 1) surrogate_cell_kernel(const CellArgs a
             c.invXdist = 1.0 / m.x;
             c.invYdist = 1.0 / m.y;
             c.depth = a.depthIntervals[kI + a.sW - 2];
-            c.gate = fminf(sqrtf(gsum / 256.f) / GATE_SIGMA, 1.f);
-            c.pad = 0.f;
+            c.sigma = sqrtf(gsum / 256.f);
+            c.gate = fminf(c.sigma / GATE_SIGMA, 1.f);
             a.corners[cl] = c;
         }
         fence_before_sync();
@@ -320,6 +321,7 @@ struct StepArgs {
     double invLength, invDti, invTau0;  // reciprocals: the row epilogue multiplies
     int upper, lower, horizontal;
     int fallbackAll;  // run parameters outside the surrogate: every active particle falls back
+    float maxError;   // metres per interval (INFINITY: off); see surrogate_trusted
     int drift;        // driftModel == 1: drifting objects fall back
     const int *dry;   // inclusive 2-D prefix sums of dry nodes, [(eta+1)][(xi+1)]
     const __half *z;  // [nCL][256]
@@ -385,6 +387,17 @@ __device__ double pinned_axis(double x0, double disp, double d, double nSub, dou
     x = fmin(fmax(x, 0.0), nextafter(maximum, 0.0));
     m = mm;
     return x;
+}
+
+// Whether the one-interval prediction is trusted: an estimate of the start-point method's error
+// over the remaining time, |grad u| |u| t^2 / 2, with the velocity gradient taken as the stencil's
+// RMS deviation sigma over 1.5 cells of the finer axis, must not exceed maxError (metres). A
+// uniform stencil (sigma = 0) is always trusted: there the start-point displacement is exact.
+__device__ __forceinline__ bool surrogate_trusted(float sigma, double invX, double invY, float ub,
+                                                  float vb, double trem, float maxError) {
+    const float grad = sigma * (float)fmax(invX, invY) * (1.f / 1.5f);
+    const float t = (float)trem;
+    return grad * sqrtf(ub * ub + vb * vb) * 0.5f * t * t <= maxError;
 }
 
 __device__ __forceinline__ int dry_in_box(const int *pre, int xi, int ja, int jb, int ia, int ib) {
@@ -759,6 +772,8 @@ __global__ void __launch_bounds__(256, 5) surrogate_post_kernel(const StepArgs a
             const float wb = blend(blend(bil4(cwU0, jF, iF), bil4(cwL0, jF, iF), kF),
                                    blend(bil4(cwU1, jF, iF), bil4(cwL1, jF, iF), kF), am);
             const float hc = bil4(ch, jF, iF) + blend(bil4(cz0, jF, iF), bil4(cz1, jF, iF), am);
+            const float sigma = __ldg(reinterpret_cast<const float *>(cf + 12) + 3);
+            const bool trusted = surrogate_trusted(sigma, inv.x, inv.y, ub, vb, trem, a.maxError);
             const float zdist = hc * (float)depth;
             const double dI = ((double)ub * trem + OUT_H * y0) * inv.x;
             const double dJ = ((double)vb * trem + OUT_H * y1) * inv.y;
@@ -797,7 +812,7 @@ __global__ void __launch_bounds__(256, 5) surrogate_post_kernel(const StepArgs a
             jb = jb < 0 ? 0 : (jb > a.eta - 1 ? a.eta - 1 : jb);
             ia = ia < 0 ? 0 : (ia > a.xi - 1 ? a.xi - 1 : ia);
             ib = ib < 0 ? 0 : (ib > a.xi - 1 ? a.xi - 1 : ib);
-            if (dry_in_box(a.dry, a.xi, ja, jb, ia, ib) > 0) {
+            if (!trusted || dry_in_box(a.dry, a.xi, ja, jb, ia, ib) > 0) {
                 status = ROW_FALLBACK;
             } else {
                 const double age = page + trem;
@@ -1049,7 +1064,7 @@ __global__ void __launch_bounds__(128, WALK_BLOCKS)
         const uint32_t slot = L.order ? L.order[n] : (uint32_t)n;  // cell order of the walk
         const float4 row = a.rows[slot];  // the step kernel's rows follow the slots
         const int code = __float_as_int(row.w);
-        const int status = code >= 0 ? ROW_RUN : (code == ROW_CODE_FALLBACK ? ROW_FALLBACK : ROW_NONE);
+        int status = code >= 0 ? ROW_RUN : (code == ROW_CODE_FALLBACK ? ROW_FALLBACK : ROW_NONE);
         ParticleState p;
         p.j = S.j[slot];
         p.i = S.i[slot];
@@ -1073,19 +1088,26 @@ __global__ void __launch_bounds__(128, WALK_BLOCKS)
             const float vb = blend(bil4(cv0, jF, iF), bil4(cv1, jF, iF), am);
             const float wb = blend(blend(bil4(cwU0, jF, iF), bil4(cwL0, jF, iF), kF),
                                    blend(bil4(cwU1, jF, iF), bil4(cwL1, jF, iF), kF), am);
-            const float rateX = fmaf(OUT_H * row.x * gate, invTrem, ub);
-            const float rateY = fmaf(OUT_H * row.y * gate, invTrem, vb);
-            const float rateZ = fmaf(OUT_V * row.z * gate, invTrem, wb + (float)a.sv);
-            const float *depth = a.sW - 1 <= 64 ? depthS : W.depth;  // deeper grids: global copy
-            steps = walk_particle<SEM, STORE>(cfg, P, W, depth, a.eta, a.xi, a.sW, p, rateX, rateY,
-                                              rateZ);
-            S.j[slot] = p.j;
-            S.i[slot] = p.i;
-            S.k[slot] = p.k;
-            S.age[slot] = p.age;
-            S.health[slot] = p.health;
-            if (L.conc) concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
-            run = true;
+            const double2 inv = __ldg(reinterpret_cast<const double2 *>(cf + 11));
+            const float sigma = __ldg(reinterpret_cast<const float *>(cf + 12) + 3);
+            if (!surrogate_trusted(sigma, inv.x, inv.y, ub, vb, (1.0 - da0) * a.length,
+                                   a.maxError)) {
+                status = ROW_FALLBACK;
+            } else {
+                const float rateX = fmaf(OUT_H * row.x * gate, invTrem, ub);
+                const float rateY = fmaf(OUT_H * row.y * gate, invTrem, vb);
+                const float rateZ = fmaf(OUT_V * row.z * gate, invTrem, wb + (float)a.sv);
+                const float *depth = a.sW - 1 <= 64 ? depthS : W.depth;  // deeper: global copy
+                steps = walk_particle<SEM, STORE>(cfg, P, W, depth, a.eta, a.xi, a.sW, p, rateX,
+                                                  rateY, rateZ);
+                S.j[slot] = p.j;
+                S.i[slot] = p.i;
+                S.k[slot] = p.k;
+                S.age[slot] = p.age;
+                S.health[slot] = p.health;
+                if (L.conc) concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
+                run = true;
+            }
         } else if (status == ROW_NONE && L.conc) {
             concCell = concentration_cell(p, L.concTimeIndex, a.sRho, a.eta, a.xi);
         }
@@ -1251,6 +1273,7 @@ cudaError_t surrogate_step(const SurrogateStep &s, const ParticleSoA &S, const M
     a.lower = s.cfg.lowerClosure;
     a.horizontal = s.cfg.horizontalClosure;
     a.fallbackAll = s.fallbackAll;
+    a.maxError = s.maxError;
     a.drift = s.cfg.driftModel == 1;
     a.dry = s.dry;
     a.z = s.z;

@@ -106,6 +106,11 @@ class Engine:
         self._surrogate = flat
         self._check(self._lib.wacomm_b200_set_surrogate(self._ctx, flat.ctypes.data_as(_fp), len(flat)))
 
+    def set_surrogate_error_limit(self, metres=float("inf")):
+        """Particles whose estimated one-interval surrogate error exceeds `metres` take the FP32
+        step (infinity: every covered particle stays with the surrogate)."""
+        self._check(self._lib.wacomm_b200_set_surrogate_error_limit(self._ctx, float(metres)))
+
     def surrogate_stats(self):
         """dict of the last surrogate interval: particles moved by the surrogate, particles handed
         to the FP32 step, device ms of the per-cell and per-particle kernels."""
