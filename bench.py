@@ -531,6 +531,27 @@ def nonuniform_error(local_rank, hours=24, n=65536):
     out["flow"] = ("streamfunction of 64 Fourier modes, rms 0.3 m/s, wavelengths 2-50 km, "
                    "256x256x12 grid at 0.0015 deg, no land")
     out["plain_fp32_fp16_storage"] = error_stats(win, plain, truth, hours, FP64)
+    # the trust limit: particles whose estimated one-interval error exceeds it take the FP32 step
+    from wacommplusplus_b200.engine import Engine
+    limited = {}
+    for limit in (200.0, 50.0):
+        e = Engine(local_rank, arithmetic="fp32", storage="fp16", surrogate=1)
+        e.set_config(cfg)
+        e.load_window(win)
+        e.set_surrogate()
+        e.set_surrogate_error_limit(limit)
+        e.set_particles(start)
+        run = fallback = 0
+        for t in range(hours):
+            e.move_interval(t)
+            st = e.surrogate_stats()
+            run, fallback = run + st["run"], fallback + st["fallback"]
+        got = e.get_particles()
+        e.close()
+        entry = error_stats(win, got, truth, hours, FP64)
+        entry["surrogate_share"] = run / max(1, run + fallback)
+        limited[f"{limit:g}_m"] = entry
+    out["with_error_limit"] = limited
     return out
 
 
