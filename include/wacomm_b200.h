@@ -461,14 +461,18 @@ int wacomm_b200_cuda_move_particle_noalloc(const wacomm_b200_config *config_devi
 /* Scratch floats of wacomm_b200_mlp_train_step for a batch. */
 size_t wacomm_b200_mlp_train_work_floats(int batch);
 
-/* One training step of the surrogate MLP with the library's own FP32 kernels: forward pass
+/* One training step of the surrogate MLP with the library's own kernels: forward pass
  * (388 -> 256 -> 256 -> 256 -> 3, GELU tanh form, outputs times the gate), mean-squared loss of
  * the gated outputs against the targets (over batch x 3), backward pass of all four layers into
  * grads, then, with update != 0, an Adam step (beta1 0.9, beta2 0.999, eps 1e-8, bias correction
- * at `step` >= 1) of params with moments m, v. Device pointers, asynchronous on `stream`:
- * stencil [batch][384], particle [batch][4], gate [batch], target [batch][3]; params, grads, m, v:
- * the flat parameter layout of wacomm_b200_set_surrogate; work: mlp_train_work_floats(batch);
- * loss: one float. Returns 0, WACOMM_B200_ERR_ARGUMENT or WACOMM_B200_ERR_CUDA. */
+ * at `step` >= 1) of params with moments m, v. The products of layers 1-3 and every weight
+ * gradient run on the tcgen05 tensor cores with BF16 operands and FP32 accumulation; the weight
+ * gradients reduce the batch in a fixed order, so a step is reproducible bit for bit. Device
+ * pointers, asynchronous on `stream`: stencil [batch][384], particle [batch][4], gate [batch],
+ * target [batch][3]; params, grads, m, v: the flat parameter layout of wacomm_b200_set_surrogate;
+ * work: mlp_train_work_floats(batch) floats, whose first 32-bit word is set nonzero when a
+ * tensor-core kernel gave up on a bounded wait (the step's results are then not valid); loss: one
+ * float. Returns 0, WACOMM_B200_ERR_ARGUMENT or WACOMM_B200_ERR_CUDA. */
 int wacomm_b200_mlp_train_step(const float *stencil, const float *particle, const float *gate,
                                const float *target, int batch, float *params, float *grads,
                                float *m, float *v, float *work, float *loss, int step, float lr,

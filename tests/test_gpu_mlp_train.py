@@ -1,6 +1,7 @@
-"""Training of the surrogate MLP with the library's own kernels (wacomm_b200_mlp_train_step):
-gradients and the Adam step against the float64 oracle (oracle/mlp_oracle.py), and what the
-trained network gains over the method without it on held-out segments of the plain kernel."""
+"""Training of the surrogate MLP with the library's own kernels (wacomm_b200_mlp_train_step: BF16
+tcgen05 GEMMs for layers 1-3 and the weight gradients, FP32 elsewhere): gradients and the Adam
+step against the float64 oracle (oracle/mlp_oracle.py), and what the trained network gains over
+the method without it on held-out segments of the plain kernel."""
 import numpy as np
 import pytest
 
@@ -25,23 +26,45 @@ def _cuda(*arrays):
     return [torch.tensor(a, device="cuda") for a in arrays]
 
 
-@pytest.mark.parametrize("n", [37, 300])
+@pytest.mark.parametrize("n", [37, 300, 5000])
 def test_gradients_match_the_oracle(cuda_device, n):
+    """The training GEMMs run on the tensor cores with BF16 operands and FP32 accumulation. Against
+    the float64 backpropagation that rounds the same operands to BF16 (mlp_oracle, bf16_operands)
+    the gradients agree to 2e-3 of each tensor's largest entry (FP32 sums, and a BF16 rounding
+    that the kernel's FP32 activation and the oracle's float64 one may take to different sides);
+    against the unrounded float64 gradients, to 5e-2 (the BF16 roundings themselves)."""
     from wacommplusplus_b200.surrogate_train import KernelTrainer
     weights = sg.random_weights(seed=5)
     data = _batch(n, seed=n)
-    trainer = KernelTrainer(torch, weights, batch=512)
+    trainer = KernelTrainer(torch, weights, batch=max(512, n))
     loss = float(trainer.run(*_cuda(*data), update=False))
-    want_loss, want = mo.loss_and_gradients(weights, *data)
+    assert trainer.error_flag() == 0
+    want_loss, want = mo.loss_and_gradients(weights, *data, bf16_operands=True)
+    exact_loss, exact = mo.loss_and_gradients(weights, *data)
     got = trainer.grads.cpu().numpy().astype(np.float64)
-    assert abs(loss - want_loss) <= 1e-5 * abs(want_loss)
+    assert abs(loss - want_loss) <= 1e-4 * abs(want_loss), (loss, want_loss)
+    assert abs(loss - exact_loss) <= 1e-2 * abs(exact_loss), (loss, exact_loss)
     at = 0
     for name, shape in mo.SHAPES:
         size = int(np.prod(shape))
-        g, w = got[at:at + size], want[at:at + size]
+        g, w, x = got[at:at + size], want[at:at + size], exact[at:at + size]
         rel = np.abs(g - w).max() / max(np.abs(w).max(), 1e-30)
-        assert rel < 1e-4, (name, rel)
+        assert rel < 2e-3, (name, rel)
+        rel = np.abs(g - x).max() / max(np.abs(x).max(), 1e-30)
+        assert rel < 5e-2, (name, rel)
         at += size
+
+
+def test_weight_gradients_are_reproducible(cuda_device):
+    """The weight gradients reduce the batch in a fixed order (per-split partial sums, summed in
+    order): two runs of the same batch give the same bits."""
+    from wacommplusplus_b200.surrogate_train import KernelTrainer
+    data = _cuda(*_batch(20000, seed=3))
+    first = KernelTrainer(torch, sg.random_weights(seed=2), batch=20000)
+    first.run(*data, update=False)
+    second = KernelTrainer(torch, sg.random_weights(seed=2), batch=20000)
+    second.run(*data, update=False)
+    assert torch.equal(first.grads, second.grads)
 
 
 def test_adam_steps_match_the_oracle(cuda_device):

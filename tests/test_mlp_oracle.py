@@ -38,3 +38,13 @@ def test_oracle_adam_first_step_moves_by_the_learning_rate():
     grads = np.array([1e-3, -2.0, 5.0, 0.0])
     new, m, v = mo.adam(flat, grads, np.zeros(4), np.zeros(4), step=1, lr=0.01)
     assert np.allclose(new[:3], -0.01 * np.sign(grads[:3]), rtol=1e-4) and new[3] == 0.0
+
+
+def test_bf16_rounding_matches_torch():
+    """The oracle's bfloat16 rounding (nearest, ties to even) of the tensor-core operands."""
+    import torch
+    rng = np.random.default_rng(4)
+    a = np.concatenate([rng.standard_normal(10000) * 10 ** rng.uniform(-6, 6, 10000),
+                        1 + np.arange(256) * 2.0 ** -9, [0.0, -0.0, 1e-40, 3e38]])
+    want = torch.tensor(a, dtype=torch.float32).bfloat16().double().numpy()
+    assert np.array_equal(mo.bf16(a), want)

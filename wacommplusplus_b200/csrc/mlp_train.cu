@@ -1,16 +1,23 @@
 // Training of the advection surrogate's MLP (388 -> 256 -> 256 -> 256 -> 3, GELU tanh form, the
 // outputs multiplied by the stencil's uniformity gate) with the library's own kernels: the forward
 // pass, the mean-squared loss against the targets, the backward pass through all four layers and
-// an Adam update, in FP32 on the CUDA cores. The parameters use the flat layout of
+// an Adam update. The GEMMs of layers 1-3 (forward, input gradients) and every weight gradient
+// run on the tcgen05 tensor cores with BF16 operands and FP32 accumulation; the three-output layer
+// 4 forward and input gradient, the loss, GELU derivatives, bias sums and Adam are FP32 on the
+// CUDA cores. The parameters use the flat layout of
 // wacomm_b200_set_surrogate (w1 [256][388], b1, w2 [256][256], b2, w3, b3, w4 [3][256], b4), so
 // trained weights go to the inference kernels unchanged.
 //
-// One tiled GEMM kernel covers the three products of a layer: the forward Z = X W^T (bias and
-// GELU fused into its epilogue), the input gradient dX = dZ W, and the weight gradient
-// dW = dZ^T X (the reduction over the batch).
+// The tensor-core GEMM covers the three products of a layer: the forward Z = X W^T (bias and GELU
+// fused into its epilogue), the input gradient dX = dZ W, and the weight gradient dW = dZ^T X (the
+// reduction over the batch, split over the SMs and summed in a fixed order). A tiled FP32 GEMM on
+// the CUDA cores serves layer 4, whose three outputs are too few for a tensor-core tile.
 #include <cmath>
 
+#include <cuda_bf16.h>
+
 #include "engine.h"
+#include "umma.cuh"
 
 namespace wb {
 namespace {
@@ -27,6 +34,236 @@ __device__ __forceinline__ float gelu_exact_tanh(float x, float *derivative) {
     const float t = tanhf(c0 * (x + c1 * x * x * x));
     if (derivative) *derivative = 0.5f * (1.f + t) + 0.5f * x * (1.f - t * t) * c0 * (1.f + 3.f * c1 * x * x);
     return 0.5f * x * (1.f + t);
+}
+
+// ------------------------------------------------------------------ tcgen05 GEMM (layers 1-3)
+//
+// C[M][N] = sum_k a(m, k) b(n, k), a(m, k) = A[m sam + k sak], b(n, k) = B[n sbn + k sbk]: BF16
+// operands, FP32 accumulation in tensor memory. A block owns a 128-row by up to 256-column tile
+// and a range of K; its 256 threads read the FP32 operands (coalesced along whichever index is
+// contiguous in memory, so transposed operands need no separate pass), round them to BF16 and
+// write them into shared memory in the K-major 128-byte-swizzle layout of umma.cuh, two K-blocks
+// of 64 in flight: while one thread issues the four MMAs of block kb, the others fill block kb+1.
+// Epilogues: 0 store; 1 add bias[n]; 2 add bias[n], store Z and GELU(Z); 3 store the block's
+// partial sum of its K range to partial[blockIdx.z] (reduced afterwards in a fixed order, so the
+// weight gradients are reproducible bit for bit).
+constexpr int UM = 128, UK = 64, UN = 256, UTHREADS = 256;
+constexpr uint32_t UA_BYTES = UM * 128, UB_BYTES = UN * 128;
+constexpr size_t USMEM = 2 * ((size_t)UA_BYTES + UB_BYTES) + 1024;
+
+struct UmmaGemm {
+    int M, N, K, kPerSplit;
+    const float *A;
+    long long sam, sak;
+    const float *B;
+    long long sbn, sbk;
+    const float *bias;
+    float *C, *H, *partial;
+    int ldc;
+    int *err;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+// Pairs (row, k..k+1) of a rows x 64 operand block into its swizzled shared-memory image; rows
+// at or past `rows` and k at or past kEnd read as zero.
+__device__ __forceinline__ void stage_block(uint8_t *dst, int rowsInBlock, const float *src,
+                                            long long sRow, long long sK, int row0, int rows,
+                                            int k0, int kEnd, int tid) {
+    const int pairs = rowsInBlock * (UK / 2);
+    for (int e = tid; e < pairs; e += UTHREADS) {
+        int r, kp;
+        if (sK == 1) {
+            r = e / (UK / 2);
+            kp = e % (UK / 2);
+        } else {
+            kp = e / rowsInBlock;
+            r = e % rowsInBlock;
+        }
+        const int gr = row0 + r, gk = k0 + 2 * kp;
+        float v0 = 0.f, v1 = 0.f;
+        if (gr < rows) {
+            const float *p = src + (long long)gr * sRow;
+            if (gk < kEnd) v0 = __ldg(p + (long long)gk * sK);
+            if (gk + 1 < kEnd) v1 = __ldg(p + (long long)(gk + 1) * sK);
+        }
+        *reinterpret_cast<uint32_t *>(dst + umma::sw128_offset(r, 2 * kp)) = pack_bf16x2(v0, v1);
+    }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(UTHREADS, 1) umma_gemm_kernel(const UmmaGemm g) {
+    using namespace umma;
+    extern __shared__ uint8_t dynSmem[];
+    uint8_t *sA = reinterpret_cast<uint8_t *>(((uintptr_t)dynSmem + 1023) & ~(uintptr_t)1023);
+    uint8_t *sB = sA + 2 * UA_BYTES;
+    __shared__ __align__(8) uint64_t freed[2], accFull;
+    __shared__ uint32_t tmemSlot;
+    __shared__ int abortFlag;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * UM, n0 = blockIdx.x * UN;
+    const int nLeft = g.N - n0;
+    const int nTile = nLeft >= UN ? UN : ((nLeft + 15) / 16) * 16;  // MMA N: multiple of 16
+    const int kBegin = blockIdx.z * g.kPerSplit;
+    const int kEnd = min(g.K, kBegin + g.kPerSplit);
+    const int nkb = kEnd > kBegin ? (kEnd - kBegin + UK - 1) / UK : 0;
+    if (tid == 0) {
+        mbar_init(&freed[0], 1);
+        mbar_init(&freed[1], 1);
+        mbar_init(&accFull, 1);
+        abortFlag = 0;
+        fence_barrier_init();
+    }
+    if (warp == 0) tmem_alloc(&tmemSlot, UN);
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = tmemSlot;
+    const uint32_t idesc = idesc_bf16(UM, nTile);
+    bool ok = true;
+    for (int kb = 0; kb < nkb && ok; kb++) {
+        const int s = kb & 1;
+        // the MMAs of block kb-2 read this stage: wait for their commit
+        if (kb >= 2) ok = mbar_wait(&freed[s], (uint32_t)(((kb >> 1) + 1) & 1), &abortFlag);
+        __syncwarp();
+        if (!ok) break;
+        const int k0 = kBegin + kb * UK;
+        stage_block(sA + s * UA_BYTES, UM, g.A, g.sam, g.sak, m0, g.M, k0, kEnd, tid);
+        stage_block(sB + s * UB_BYTES, nTile, g.B, g.sbn, g.sbk, n0, g.N, k0, kEnd, tid);
+        fence_async_shared();
+        fence_before_sync();
+        __syncthreads();
+        fence_after_sync();
+        if (abortFlag) {
+            ok = false;
+            break;
+        }
+        if (tid == 0) {
+#pragma unroll
+            for (int ks = 0; ks < UK / 16; ks++)
+                mma_bf16(tmem, desc_sw128(smem_u32(sA + s * UA_BYTES + ks * 32)),
+                         desc_sw128(smem_u32(sB + s * UB_BYTES + ks * 32)), idesc, (kb | ks) != 0);
+            mma_commit(&freed[s]);
+        }
+    }
+    // every MMA issued so far lands before the accumulator is read (or the block exits)
+    if (tid == 0) mma_commit(&accFull);
+    const bool done = mbar_wait_bounded(&accFull, 0);
+    __syncwarp();
+    fence_after_sync();
+    const bool valid = ok && done && !abortFlag;
+    if (valid) {
+        const int quarter = warp & 3, half = warp >> 2;
+        const int m = m0 + quarter * 32 + lane;
+        for (int c0 = half * (UN / 2); c0 < (half + 1) * (UN / 2) && c0 < nTile; c0 += 32) {
+            float v[32];
+            if (nkb > 0) {
+                tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, v);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 32; c++) v[c] = 0.f;
+            }
+            if (m >= g.M) continue;
+#pragma unroll
+            for (int c = 0; c < 32; c++) {
+                const int n = n0 + c0 + c;
+                if (n >= g.N) break;
+                float z = v[c];
+                if (EPI == 3) {
+                    g.partial[((size_t)blockIdx.z * g.M + m) * g.N + n] = z;
+                    continue;
+                }
+                if (EPI >= 1) z += __ldg(g.bias + n);
+                g.C[(size_t)m * g.ldc + n] = z;
+                if (EPI == 2) g.H[(size_t)m * g.ldc + n] = gelu_exact_tanh(z, nullptr);
+            }
+        }
+    }
+    if (!valid && tid == 0) atomicOr(g.err, 1);
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after_sync();
+        tmem_dealloc(tmem, UN);
+    }
+}
+
+// out[m][n] = sum over the splits z (in order) of partial[z][m][n].
+__global__ void split_sum_kernel(const float *partial, int splits, size_t cells, float *out) {
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < cells;
+         e += (size_t)gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int z = 0; z < splits; z++) s += partial[(size_t)z * cells + e];
+        out[e] = s;
+    }
+}
+
+// Floats of the weight-gradient partial sums: at most 148 / (output tiles) splits of M x N, the
+// most for a 256 x 256 weight (two tiles, 74 splits).
+constexpr size_t UMMA_PARTIAL_FLOATS = (size_t)(148 / 2) * T_HID * T_HID;
+
+cudaError_t umma_prepare() {
+    static bool done[64] = {};
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return e;
+    if (device >= 0 && device < 64 && done[device]) return cudaSuccess;
+    for (auto fn : {umma_gemm_kernel<0>, umma_gemm_kernel<1>, umma_gemm_kernel<2>, umma_gemm_kernel<3>}) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)USMEM);
+        if (e != cudaSuccess) return e;
+    }
+    if (device >= 0 && device < 64) done[device] = true;
+    return cudaSuccess;
+}
+
+// C (M x N, leading dimension ldc) from a(m, k) = A[m sam + k sak] and b(n, k) = B[n sbn + k sbk]
+// on the tensor cores. EPI 3 (a reduction over a long K, the batch) splits K over about one block
+// per SM and sums the splits in order into C (ldc must be N).
+template <int EPI>
+cudaError_t umma_gemm(int M, int N, int K, const float *A, long long sam, long long sak,
+                      const float *B, long long sbn, long long sbk, const float *bias, float *C,
+                      float *H, int ldc, float *partial, int *err, cudaStream_t stream) {
+    cudaError_t e = umma_prepare();
+    if (e != cudaSuccess) return e;
+    UmmaGemm g;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.A = A;
+    g.sam = sam;
+    g.sak = sak;
+    g.B = B;
+    g.sbn = sbn;
+    g.sbk = sbk;
+    g.bias = bias;
+    g.C = C;
+    g.H = H;
+    g.partial = partial;
+    g.ldc = ldc;
+    g.err = err;
+    const int tilesN = (N + UN - 1) / UN, tilesM = (M + UM - 1) / UM;
+    int splits = 1;
+    g.kPerSplit = ((K + UK - 1) / UK) * UK;
+    if (EPI == 3) {
+        splits = 148 / (tilesN * tilesM);
+        if (splits < 1) splits = 1;
+        const int kBlocks = (K + UK - 1) / UK;
+        if (splits > kBlocks) splits = kBlocks > 0 ? kBlocks : 1;
+        g.kPerSplit = ((kBlocks + splits - 1) / splits) * UK;
+        splits = (K + g.kPerSplit - 1) / g.kPerSplit;
+        if (splits < 1) splits = 1;
+        if ((size_t)splits * M * N > UMMA_PARTIAL_FLOATS || ldc != N) return cudaErrorInvalidValue;
+    }
+    dim3 grid(tilesN, tilesM, splits);
+    umma_gemm_kernel<EPI><<<grid, UTHREADS, USMEM, stream>>>(g);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || EPI != 3) return e;
+    const size_t cells = (size_t)M * N;
+    split_sum_kernel<<<(int)((cells + 255) / 256), 256, 0, stream>>>(partial, splits, cells, C);
+    return cudaGetLastError();
 }
 
 // C[M][N] = sum_k a(m, k) b(k, n) with a(m, k) = TA ? A[k lda + m] : A[m lda + k] and
@@ -182,7 +419,9 @@ int blocks_for(size_t n) {
 }  // namespace
 
 size_t mlp_train_work_floats(int batch) {
-    return (size_t)batch * (T_IN + 6 * T_HID + 2 * T_OUT + 2 * T_HID);
+    // an error word (padded to 16 bytes), the weight-gradient partial sums, then the
+    // activations and gradients of the batch
+    return 4 + UMMA_PARTIAL_FLOATS + (size_t)batch * (T_IN + 6 * T_HID + 2 * T_OUT + 2 * T_HID);
 }
 
 cudaError_t mlp_train_step(const float *stencil, const float *particle, const float *gate,
@@ -190,40 +429,58 @@ cudaError_t mlp_train_step(const float *stencil, const float *particle, const fl
                            float *v, float *work, float *loss, int step, float lr, bool update,
                            cudaStream_t stream) {
     const int B = batch;
-    float *X = work, *Z1 = X + (size_t)B * T_IN, *H1 = Z1 + (size_t)B * T_HID,
-          *Z2 = H1 + (size_t)B * T_HID, *H2 = Z2 + (size_t)B * T_HID, *Z3 = H2 + (size_t)B * T_HID,
-          *H3 = Z3 + (size_t)B * T_HID, *O = H3 + (size_t)B * T_HID, *dO = O + (size_t)B * T_OUT,
-          *dA = dO + (size_t)B * T_OUT, *dB = dA + (size_t)B * T_HID;
+    int *err = reinterpret_cast<int *>(work);
+    float *partial = work + 4;
+    float *X = partial + UMMA_PARTIAL_FLOATS, *Z1 = X + (size_t)B * T_IN,
+          *H1 = Z1 + (size_t)B * T_HID, *Z2 = H1 + (size_t)B * T_HID, *H2 = Z2 + (size_t)B * T_HID,
+          *Z3 = H2 + (size_t)B * T_HID, *H3 = Z3 + (size_t)B * T_HID, *O = H3 + (size_t)B * T_HID,
+          *dO = O + (size_t)B * T_OUT, *dA = dO + (size_t)B * T_OUT, *dB = dA + (size_t)B * T_HID;
     const float *W1 = params + OFF_TW1, *W2 = params + OFF_TW2, *W3 = params + OFF_TW3,
                 *W4 = params + OFF_TW4;
     cudaError_t e = cudaMemsetAsync(loss, 0, sizeof(float), stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(grads, 0, T_PARAMS * sizeof(float), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(err, 0, sizeof(int), stream);
     if (e != cudaSuccess) return e;
     concat_kernel<<<blocks_for((size_t)B * T_IN), 256, 0, stream>>>(stencil, particle, B, X);
-    // forward
-    gemm<false, true, 2>(B, T_HID, T_IN, X, T_IN, W1, T_IN, params + OFF_TB1, Z1, H1, T_HID, stream);
-    gemm<false, true, 2>(B, T_HID, T_HID, H1, T_HID, W2, T_HID, params + OFF_TB2, Z2, H2, T_HID, stream);
-    gemm<false, true, 2>(B, T_HID, T_HID, H2, T_HID, W3, T_HID, params + OFF_TB3, Z3, H3, T_HID, stream);
+#define UMMA(call)                              \
+    do {                                        \
+        if ((e = (call)) != cudaSuccess) return e; \
+    } while (0)
+    // forward: layers 1-3 on the tensor cores (BF16 operands, bias and GELU in the epilogue),
+    // layer 4 (three outputs) on the CUDA cores
+    UMMA(umma_gemm<2>(B, T_HID, T_IN, X, T_IN, 1, W1, T_IN, 1, params + OFF_TB1, Z1, H1, T_HID,
+                      partial, err, stream));
+    UMMA(umma_gemm<2>(B, T_HID, T_HID, H1, T_HID, 1, W2, T_HID, 1, params + OFF_TB2, Z2, H2,
+                      T_HID, partial, err, stream));
+    UMMA(umma_gemm<2>(B, T_HID, T_HID, H2, T_HID, 1, W3, T_HID, 1, params + OFF_TB3, Z3, H3,
+                      T_HID, partial, err, stream));
     gemm<false, true, 1>(B, T_OUT, T_HID, H3, T_HID, W4, T_HID, params + OFF_TB4, O, nullptr, T_OUT, stream);
     loss_kernel<<<blocks_for((size_t)B * T_OUT), 256, 0, stream>>>(O, gate, target, B, dO, loss);
-    // backward: layer 4
-    gemm<true, false, 3>(T_OUT, T_HID, B, dO, T_OUT, H3, T_HID, nullptr, grads + OFF_TW4, nullptr, T_HID, stream);
+    // backward, layer 4: dW4 = dO^T H3 (tensor cores, reduction over the batch), dA = dO W4
+    UMMA(umma_gemm<3>(T_OUT, T_HID, B, dO, 1, T_OUT, H3, 1, T_HID, nullptr, grads + OFF_TW4,
+                      nullptr, T_HID, partial, err, stream));
     column_sum_kernel<<<T_OUT, 256, 0, stream>>>(dO, B, T_OUT, grads + OFF_TB4);
     gemm<false, false, 0>(B, T_HID, T_OUT, dO, T_OUT, W4, T_HID, nullptr, dA, nullptr, T_HID, stream);
-    // layer 3
+    // layer 3: dZ3 = dA GELU'(Z3); dW3 = dZ3^T H2; dB = dZ3 W3
     gelu_backward_kernel<<<blocks_for((size_t)B * T_HID), 256, 0, stream>>>(Z3, dA, (size_t)B * T_HID);
-    gemm<true, false, 3>(T_HID, T_HID, B, dA, T_HID, H2, T_HID, nullptr, grads + OFF_TW3, nullptr, T_HID, stream);
+    UMMA(umma_gemm<3>(T_HID, T_HID, B, dA, 1, T_HID, H2, 1, T_HID, nullptr, grads + OFF_TW3,
+                      nullptr, T_HID, partial, err, stream));
     column_sum_kernel<<<T_HID, 256, 0, stream>>>(dA, B, T_HID, grads + OFF_TB3);
-    gemm<false, false, 0>(B, T_HID, T_HID, dA, T_HID, W3, T_HID, nullptr, dB, nullptr, T_HID, stream);
+    UMMA(umma_gemm<0>(B, T_HID, T_HID, dA, T_HID, 1, W3, 1, T_HID, nullptr, dB, nullptr, T_HID,
+                      partial, err, stream));
     // layer 2
     gelu_backward_kernel<<<blocks_for((size_t)B * T_HID), 256, 0, stream>>>(Z2, dB, (size_t)B * T_HID);
-    gemm<true, false, 3>(T_HID, T_HID, B, dB, T_HID, H1, T_HID, nullptr, grads + OFF_TW2, nullptr, T_HID, stream);
+    UMMA(umma_gemm<3>(T_HID, T_HID, B, dB, 1, T_HID, H1, 1, T_HID, nullptr, grads + OFF_TW2,
+                      nullptr, T_HID, partial, err, stream));
     column_sum_kernel<<<T_HID, 256, 0, stream>>>(dB, B, T_HID, grads + OFF_TB2);
-    gemm<false, false, 0>(B, T_HID, T_HID, dB, T_HID, W2, T_HID, nullptr, dA, nullptr, T_HID, stream);
+    UMMA(umma_gemm<0>(B, T_HID, T_HID, dB, T_HID, 1, W2, 1, T_HID, nullptr, dA, nullptr, T_HID,
+                      partial, err, stream));
     // layer 1 (no input gradient)
     gelu_backward_kernel<<<blocks_for((size_t)B * T_HID), 256, 0, stream>>>(Z1, dA, (size_t)B * T_HID);
-    gemm<true, false, 3>(T_HID, T_IN, B, dA, T_HID, X, T_IN, nullptr, grads + OFF_TW1, nullptr, T_IN, stream);
+    UMMA(umma_gemm<3>(T_HID, T_IN, B, dA, 1, T_HID, X, 1, T_IN, nullptr, grads + OFF_TW1,
+                      nullptr, T_IN, partial, err, stream));
     column_sum_kernel<<<T_HID, 256, 0, stream>>>(dA, B, T_HID, grads + OFF_TB1);
+#undef UMMA
     if (update) {
         const float c1 = 1.f - powf(0.9f, (float)step), c2 = 1.f - powf(0.999f, (float)step);
         adam_kernel<<<blocks_for(T_PARAMS), 256, 0, stream>>>(params, grads, m, v, T_PARAMS, lr, c1, c2);

@@ -146,7 +146,8 @@ def initial_weights(seed):
 
 class KernelTrainer:
     """Training of the MLP with the library's own kernels (wacomm_b200_mlp_train_step: forward,
-    loss, backward, Adam, FP32 on the device); torch only holds the device buffers."""
+    loss, backward and Adam on the device, the GEMMs of layers 1-3 and the weight gradients on the
+    tensor cores in BF16 with FP32 accumulation); torch only holds the device buffers."""
 
     def __init__(self, torch, weights, batch):
         self.torch, self.lib, self.batch = torch, _native.lib(), batch
@@ -177,6 +178,11 @@ class KernelTrainer:
         if status != 0:
             raise RuntimeError(f"wacomm_b200_mlp_train_step failed ({status})")
         return self.loss.clone()
+
+    def error_flag(self):
+        """Nonzero when a tensor-core GEMM of the steps so far gave up on a bounded wait (its
+        results are then not valid); waits for the stream."""
+        return int(self.work[:1].view(self.torch.int32).item())
 
     def weights(self):
         flat, out, at = self.params.cpu().numpy(), {}, 0
