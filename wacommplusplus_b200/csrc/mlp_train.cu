@@ -68,11 +68,74 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
     return *reinterpret_cast<uint32_t *>(&v);
 }
 
-// Pairs (row, k..k+1) of a rows x 64 operand block into its swizzled shared-memory image; rows
-// at or past `rows` and k at or past kEnd read as zero.
+__device__ __forceinline__ uint4 pack8(float4 a, float4 b) {
+    return make_uint4(pack_bf16x2(a.x, a.y), pack_bf16x2(a.z, a.w), pack_bf16x2(b.x, b.y),
+                      pack_bf16x2(b.z, b.w));
+}
+
+// One rows x 64 operand block, a(r, k) = src[r sRow + k sK], rounded to BF16 into its swizzled
+// shared-memory image; rows at or past `rows` and k at or past kEnd read as zero. Three ways to
+// read it, chosen per block: with k contiguous, each item is a row's 16-byte chunk of 8 k values
+// (two float4 loads); with rows contiguous, each item is 4 rows x 8 k values (eight float4 loads
+// along the rows, written as four chunks); otherwise scalar pairs. Every thread issues its loads
+// before its stores, so many loads are in flight.
 __device__ __forceinline__ void stage_block(uint8_t *dst, int rowsInBlock, const float *src,
                                             long long sRow, long long sK, int row0, int rows,
                                             int k0, int kEnd, int tid) {
+    const bool aligned = (((uintptr_t)src) & 15) == 0 && k0 + UK <= kEnd;
+    if (aligned && sK == 1 && (sRow & 3) == 0) {
+        const int items = rowsInBlock * 8;
+        for (int base = 0; base < items; base += 4 * UTHREADS) {
+            float4 v[4][2];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int it = base + u * UTHREADS + tid, r = it >> 3, c = it & 7;
+                v[u][0] = v[u][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (it < items && row0 + r < rows) {
+                    const float4 *q =
+                        reinterpret_cast<const float4 *>(src + (long long)(row0 + r) * sRow + k0 + c * 8);
+                    v[u][0] = __ldg(q);
+                    v[u][1] = __ldg(q + 1);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int it = base + u * UTHREADS + tid;
+                if (it < items)
+                    *reinterpret_cast<uint4 *>(dst + umma::sw128_offset(it >> 3, (it & 7) * 8)) =
+                        pack8(v[u][0], v[u][1]);
+            }
+        }
+        return;
+    }
+    if (aligned && sRow == 1 && (sK & 3) == 0 && (row0 & 3) == 0) {
+        const int groups = (rowsInBlock + 3) / 4, items = groups * 8;
+        for (int it = tid; it < items; it += UTHREADS) {
+            const int g = it % groups, c = it / groups, r0 = 4 * g, gr0 = row0 + r0;
+            float4 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const float *col = src + (long long)(k0 + c * 8 + q) * sK;
+                if (gr0 + 3 < rows) {
+                    v[q] = __ldg(reinterpret_cast<const float4 *>(col + gr0));
+                } else {
+                    v[q].x = gr0 < rows ? __ldg(col + gr0) : 0.f;
+                    v[q].y = gr0 + 1 < rows ? __ldg(col + gr0 + 1) : 0.f;
+                    v[q].z = gr0 + 2 < rows ? __ldg(col + gr0 + 2) : 0.f;
+                    v[q].w = 0.f;
+                }
+            }
+            *reinterpret_cast<uint4 *>(dst + umma::sw128_offset(r0 + 0, c * 8)) =
+                pack8(make_float4(v[0].x, v[1].x, v[2].x, v[3].x), make_float4(v[4].x, v[5].x, v[6].x, v[7].x));
+            *reinterpret_cast<uint4 *>(dst + umma::sw128_offset(r0 + 1, c * 8)) =
+                pack8(make_float4(v[0].y, v[1].y, v[2].y, v[3].y), make_float4(v[4].y, v[5].y, v[6].y, v[7].y));
+            *reinterpret_cast<uint4 *>(dst + umma::sw128_offset(r0 + 2, c * 8)) =
+                pack8(make_float4(v[0].z, v[1].z, v[2].z, v[3].z), make_float4(v[4].z, v[5].z, v[6].z, v[7].z));
+            *reinterpret_cast<uint4 *>(dst + umma::sw128_offset(r0 + 3, c * 8)) =
+                pack8(make_float4(v[0].w, v[1].w, v[2].w, v[3].w), make_float4(v[4].w, v[5].w, v[6].w, v[7].w));
+        }
+        return;
+    }
     const int pairs = rowsInBlock * (UK / 2);
     for (int e = tid; e < pairs; e += UTHREADS) {
         int r, kp;
@@ -383,19 +446,41 @@ __global__ void gelu_backward_kernel(const float *Z, float *dH, size_t n) {
     }
 }
 
-// db[n] = sum over the batch of dZ[b][n]; one block per column.
-__global__ void column_sum_kernel(const float *dZ, int batch, int N, float *db) {
-    __shared__ float partial[256];
-    const int n = blockIdx.x;
+// db[n] = sum over the batch of dZ[b][n], in two passes with a fixed order: block (x, y) sums the
+// 32 columns 32x.. over the rows of chunk y (warp w takes rows w, w + 8, ..., its lanes one column
+// each, so every row is read as one 128-byte line), adding its 8 warps' sums in order into
+// partial[y][n]; then the chunks are added in order.
+constexpr int COLUMN_CHUNKS = 64;
+
+__global__ void column_partial_kernel(const float *dZ, int batch, int N, float *partial) {
+    __shared__ float warpSum[8][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n = blockIdx.x * 32 + lane;
+    const int per = (batch + COLUMN_CHUNKS - 1) / COLUMN_CHUNKS;
+    const int b0 = blockIdx.y * per, b1 = min(batch, b0 + per);
     float sum = 0.f;
-    for (int b = threadIdx.x; b < batch; b += blockDim.x) sum += dZ[(size_t)b * N + n];
-    partial[threadIdx.x] = sum;
+    if (n < N)
+        for (int b = b0 + warp; b < b1; b += 8) sum += dZ[(size_t)b * N + n];
+    warpSum[warp][lane] = sum;
     __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if (threadIdx.x < s) partial[threadIdx.x] += partial[threadIdx.x + s];
-        __syncthreads();
+    if (warp == 0 && n < N) {
+        float total = 0.f;
+        for (int w = 0; w < 8; w++) total += warpSum[w][lane];
+        partial[(size_t)blockIdx.y * N + n] = total;
     }
-    if (threadIdx.x == 0) db[n] = partial[0];
+}
+
+__global__ void column_final_kernel(const float *partial, int N, float *db) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    float total = 0.f;
+    for (int c = 0; c < COLUMN_CHUNKS; c++) total += partial[(size_t)c * N + n];
+    db[n] = total;
+}
+
+void column_sum(const float *dZ, int batch, int N, float *partial, float *db, cudaStream_t stream) {
+    column_partial_kernel<<<dim3((N + 31) / 32, COLUMN_CHUNKS), 256, 0, stream>>>(dZ, batch, N, partial);
+    column_final_kernel<<<(N + 255) / 256, 256, 0, stream>>>(partial, N, db);
 }
 
 // Adam (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected at `step`).
@@ -459,27 +544,27 @@ cudaError_t mlp_train_step(const float *stencil, const float *particle, const fl
     // backward, layer 4: dW4 = dO^T H3 (tensor cores, reduction over the batch), dA = dO W4
     UMMA(umma_gemm<3>(T_OUT, T_HID, B, dO, 1, T_OUT, H3, 1, T_HID, nullptr, grads + OFF_TW4,
                       nullptr, T_HID, partial, err, stream));
-    column_sum_kernel<<<T_OUT, 256, 0, stream>>>(dO, B, T_OUT, grads + OFF_TB4);
+    column_sum(dO, B, T_OUT, partial, grads + OFF_TB4, stream);
     gemm<false, false, 0>(B, T_HID, T_OUT, dO, T_OUT, W4, T_HID, nullptr, dA, nullptr, T_HID, stream);
     // layer 3: dZ3 = dA GELU'(Z3); dW3 = dZ3^T H2; dB = dZ3 W3
     gelu_backward_kernel<<<blocks_for((size_t)B * T_HID), 256, 0, stream>>>(Z3, dA, (size_t)B * T_HID);
     UMMA(umma_gemm<3>(T_HID, T_HID, B, dA, 1, T_HID, H2, 1, T_HID, nullptr, grads + OFF_TW3,
                       nullptr, T_HID, partial, err, stream));
-    column_sum_kernel<<<T_HID, 256, 0, stream>>>(dA, B, T_HID, grads + OFF_TB3);
+    column_sum(dA, B, T_HID, partial, grads + OFF_TB3, stream);
     UMMA(umma_gemm<0>(B, T_HID, T_HID, dA, T_HID, 1, W3, 1, T_HID, nullptr, dB, nullptr, T_HID,
                       partial, err, stream));
     // layer 2
     gelu_backward_kernel<<<blocks_for((size_t)B * T_HID), 256, 0, stream>>>(Z2, dB, (size_t)B * T_HID);
     UMMA(umma_gemm<3>(T_HID, T_HID, B, dB, 1, T_HID, H1, 1, T_HID, nullptr, grads + OFF_TW2,
                       nullptr, T_HID, partial, err, stream));
-    column_sum_kernel<<<T_HID, 256, 0, stream>>>(dB, B, T_HID, grads + OFF_TB2);
+    column_sum(dB, B, T_HID, partial, grads + OFF_TB2, stream);
     UMMA(umma_gemm<0>(B, T_HID, T_HID, dB, T_HID, 1, W2, 1, T_HID, nullptr, dA, nullptr, T_HID,
                       partial, err, stream));
     // layer 1 (no input gradient)
     gelu_backward_kernel<<<blocks_for((size_t)B * T_HID), 256, 0, stream>>>(Z1, dA, (size_t)B * T_HID);
     UMMA(umma_gemm<3>(T_HID, T_IN, B, dA, 1, T_HID, X, 1, T_IN, nullptr, grads + OFF_TW1,
                       nullptr, T_IN, partial, err, stream));
-    column_sum_kernel<<<T_HID, 256, 0, stream>>>(dA, B, T_HID, grads + OFF_TB1);
+    column_sum(dA, B, T_HID, partial, grads + OFF_TB1, stream);
 #undef UMMA
     if (update) {
         const float c1 = 1.f - powf(0.9f, (float)step), c2 = 1.f - powf(0.999f, (float)step);
