@@ -141,7 +141,10 @@ __device__ __forceinline__ void philox_normals3(uint64_t key, long long interval
     const float scale = 2.3283064365386963e-10f;  // 2^-32; uniforms in (0,1]
     float u0 = ((float)r.x + 1.0f) * scale, u1 = (float)r.y * scale;
     float u2 = ((float)r.z + 1.0f) * scale, u3 = (float)r.w * scale;
-    float rad0 = sqrtf(-2.0f * __logf(u0)), rad1 = sqrtf(-2.0f * __logf(u2));
+    // radius sqrt(-2 ln u) as x rsqrt(x) (the hardware reciprocal square root, about 2 ulp),
+    // with x kept off zero (u = 1 gives a radius of 1e-15 instead of 0 * inf)
+    const float x0 = fmaxf(-2.0f * __logf(u0), 1e-30f), x2 = fmaxf(-2.0f * __logf(u2), 1e-30f);
+    float rad0 = x0 * rsqrtf(x0), rad1 = x2 * rsqrtf(x2);
     // angles (2u - 1) pi in [-pi, pi), where the hardware sine and cosine are accurate to ~5e-7
     const float pi = 3.14159265358979f;
     float s0, c0, s1, c1;

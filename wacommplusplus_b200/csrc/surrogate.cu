@@ -903,6 +903,9 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
     double jLo = (p.j - fj) - (double)jF, iLo = (p.i - fi) - (double)iF;
     double kLo = (ck - p.k) - (double)kF;
 
+    // surface sums at the particle's position, carried from the previous substep's landing
+    SurfaceSums here{0.f, 0.f};
+    bool carried = false;
     while (elapsed < length) {
         const double stepDt = fmin(cfg.dti, length - elapsed);
         const bool dead = lazy ? (p.age >= P.ageKillHi ||
@@ -913,7 +916,8 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
             lazy = false;
             break;
         }
-        if (!valid_cell(jI, iI, eta, xi) || (SEM == SEM_DEVICE && (kI > 0 || kI <= -sW + 1))) {
+        if (!carried &&
+            (!valid_cell(jI, iI, eta, xi) || (SEM == SEM_DEVICE && (kI > 0 || kI <= -sW + 1)))) {
             p.health = -1;
             lazy = false;
             break;
@@ -921,16 +925,16 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
         steps++;
         const int kM = mem_level(kI, sW);
         const int cell = jI * xi + iI;
-        const CellSurface surf = load_surface(W.surface, cell);
+        if (!carried) here = surface_from(load_surface(W.surface, cell), jF, iF);
         const float2 inv = __ldg(W.invMetric + cell);
         QuadPair aUp, aLo;
         const CellQuad<STORE> *col = W.columns + ((size_t)cell * sW + (size_t)(kM + sW - 1)) * 2;
         load_second<STORE>(col - 1, aLo);  // akt of W level kI-1
         load_second<STORE>(col + 1, aUp);  // akt of W level kI
         const float depth = depthS[kM + sW - 2];
-        const float dt = (float)stepDt;
+        const float dt = stepDt == cfg.dti ? dtiF : (float)stepDt;
         const float alpha = (float)((elapsed + 0.5 * stepDt) * invLength);
-        const float hc = surface_from(surf, jF, iF).height(alpha);
+        const float hc = here.height(alpha);
         if (hc <= shore && cfg.horizontalClosure == CLOSURE_KILL) {
             p.health = -1;
             lazy = false;
@@ -960,21 +964,26 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
         float zleap = fmaf(rateZ, dt, rz);
         if (fabsf(zleap) > zdist) zleap = signf_of(zdist, zleap);
         const float jN = jF + dJ, iN = iF + dI, kN = fmaf(-zleap, rzdist, kF);
-        // the destination's cell and its surface (this cell's, read again, in the common case)
-        const float cj = floorf(jN), ci = floorf(iN);
-        const int nj = jI + (int)cj, ni = iI + (int)ci;
-        const bool inside = valid_cell(nj, ni, eta, xi);
-        const float jD = jN - cj, iD = iN - ci;
-        const CellSurface there = load_surface(W.surface, inside ? nj * xi + ni : cell);
+        // the destination: at most one cell or level away on this path (comparisons, no
+        // float-to-int conversions), and its surface (this cell's, read again, in the common case)
+        const int dj = (jN >= 1.f) - (jN < 0.f), di = (iN >= 1.f) - (iN < 0.f);
+        const int dk = (kN >= 1.f) - (kN < 0.f);
+        const float jD = jN - (float)dj, iD = iN - (float)di, kD = kN - (float)dk;
+        const int nj = jI + dj, ni = iI + di;
+        const bool inside = valid_cell(nj, ni, eta, xi) && jD >= 0.f && jD < 1.f && iD >= 0.f &&
+                            iD < 1.f && kD >= 0.f && kD < 1.f;
+        const SurfaceSums there =
+            surface_from(load_surface(W.surface, inside ? nj * xi + ni : cell), jD, iD);
         const bool vertical = (float)kI - kN > 0.f || (float)kI - kN < kLowerF;
-        if (inside && !vertical && surface_from(there, jD, iD).height(alpha) > shore) {
+        carried = inside && !vertical && there.height(alpha) > shore;
+        if (carried) {
             jI = nj;
             iI = ni;
             jF = jD;
             iF = iD;
-            const float c = floorf(kN);  // level crossing
-            kI -= (int)c;
-            kF = kN - c;
+            kI -= dk;  // level crossing
+            kF = kD;
+            here = there;
         } else {
             // a closure: the plain step's FP64 landing (Particle.cpp:644-791)
             const double pj = (double)jI + (double)jF + jLo, pi = (double)iI + (double)iF + iLo;
