@@ -427,10 +427,12 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
     uint8_t *ring = sA0 + 2 * A_BYTES;
     __shared__ __align__(8) uint64_t full[WRING], empty[WRING], aFull[2], accFull[2];
     __shared__ uint32_t tmemSlot;
-    __shared__ int abortFlag, rowStop;
+    __shared__ int abortFlag;
+    __shared__ int quarterStop[2][4];  // stop decisions per TMEM lane quarter, by tile parity
     __shared__ __align__(16) float w1ps[HID * 4];  // read as float4 per hidden unit
     __shared__ float b2s[HID], b3s[HID], w4s[3 * HID], b4s[4];
-    __shared__ float red[GROUPS - 1][TILE * 3];  // layer-4 partial sums of column groups 1..
+    // layer-4 partial sums of column groups 1.., by tile parity
+    __shared__ float red[2][GROUPS - 1][TILE * 3];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         for (int s = 0; s < WRING; s++) {
@@ -438,11 +440,11 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             mbar_init(&empty[s], 1);
         }
         for (int b = 0; b < 2; b++) {
-            mbar_init(&aFull[b], 1);
+            mbar_init(&aFull[b], ROW_WARPS);  // one arrival per row warp
             mbar_init(&accFull[b], 1);
         }
         abortFlag = 0;
-        rowStop = 0;
+        for (int q = 0; q < 8; q++) quarterStop[q / 4][q % 4] = 0;
         fence_barrier_init();
     }
     {
@@ -526,11 +528,13 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
         const double T0 = a.start, T1 = a.start + a.length;
         const double kLower = -a.sW + 2;
         auto tileOf = [&](int x) { return (long long)blockIdx.x + (long long)x * gridDim.x; };
+        // each row warp signals its own part of an operand buffer (no block-wide barrier): its
+        // lanes' shared-memory writes are fenced for the tensor cores, then lane 0 arrives
         auto arrive = [&](int buf) {
             fence_async_shared();
             fence_before_sync();
-            named_sync(1, ROW_THREADS);
-            if (tid == 0) mbar_arrive(&aFull[buf]);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&aFull[buf]);
         };
 
         // A row's particle state, gathered ahead of the prologue that classifies it.
@@ -671,13 +675,14 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                 }
             }
             if (group > 0) {
-                float *mine = red[group - 1];
+                float *mine = red[x & 1][group - 1];
                 mine[r * 3 + 0] = o0;
                 mine[r * 3 + 1] = o1;
                 mine[r * 3 + 2] = o2;
             }
             fence_before_sync();
-            named_sync(1, ROW_THREADS);
+            // the four warps of this lane quarter (one per column group) meet here
+            named_sync(2 + quarter, 128);
             return ok;
         };
 
@@ -691,6 +696,10 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             if (k + 1 < nT) epilogue2(k + 1);
             float o0, o1, o2;
             epilogue3(k, o0, o1, o2);
+            // the quarter's stop decision, written by its group-0 warp in the previous tile: the
+            // same value for its four warps, which therefore leave the loop together
+            const int stop = quarterStop[k & 1][quarter];
+            if (group == 0 && lane == 0) quarterStop[(k + 1) & 1][quarter] = abortFlag;
             if (group == 0 && cur.status != ROW_EMPTY) {
                 // layer-4 sums and the row tag of the work item, for surrogate_post_kernel
                 const int code = cur.status == ROW_RUN
@@ -699,19 +708,15 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                 float s0 = o0, s1 = o1, s2 = o2;
 #pragma unroll
                 for (int g = 0; g < GROUPS - 1; g++) {
-                    s0 += red[g][r * 3 + 0];
-                    s1 += red[g][r * 3 + 1];
-                    s2 += red[g][r * 3 + 2];
+                    s0 += red[k & 1][g][r * 3 + 0];
+                    s1 += red[k & 1][g][r * 3 + 1];
+                    s2 += red[k & 1][g][r * 3 + 2];
                 }
                 a.rows[tileOf(k) * TILE + r] =
                     make_float4(s0 + b4s[0], s1 + b4s[1], s2 + b4s[2], __int_as_float(code));
             }
             if (k + 2 < nT) after = prologue(k + 2, ahead);
-            // uniform stop decision of the row warps
-            named_sync(1, ROW_THREADS);
-            if (tid == 0) rowStop = abortFlag;
-            named_sync(1, ROW_THREADS);
-            if (rowStop) break;
+            if (stop) break;
             cur = next;
             next = after;
         }
