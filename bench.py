@@ -617,7 +617,7 @@ def surrogate_leg(args, win, particles, local_rank, world, rank, barrier, dist, 
                           "kernel": "surrogate_walk_kernel", "kernel_ms": walk_ms,
                           "algorithmic_bytes_per_particle_step": B_ALG},
     })
-    if rank == 0:
+    if rank == 0 and not args.no_errors:
         n = min(len(particles), 1 << 20)
         sub = particles[:n].copy()
         hours = min(24, n_intervals)
@@ -678,6 +678,8 @@ def main():
     parser.add_argument("--no-cpu", action="store_true")
     parser.add_argument("--no-surrogate", action="store_true")
     parser.add_argument("--no-precision", action="store_true")
+    parser.add_argument("--no-errors", action="store_true",
+                        help="skip the 24-hour position-error runs of the surrogate arm")
     parser.add_argument("--scenarios", type=int, default=256,
                         help="batched workload: number of scenarios")
     parser.add_argument("--workload", default="precision",
@@ -813,7 +815,7 @@ def main():
         surrogate = surrogate_leg(args, win, particles, local_rank, world, rank, barrier, dist,
                                   exchange)
         truth = surrogate.pop("_truth", None)
-        if rank == 0 and not args.no_precision:
+        if rank == 0 and not args.no_precision and truth is not None:
             # rank 0 alone, no collectives: the other ranks wait at the final barrier
             precision = precision_leg(args, win, particles, local_rank, truth,
                                       lambda eng, t: None, lambda: None)

@@ -278,6 +278,32 @@ def evaluate(weights, n_particles=32768, hours=24, seed=1, realistic=False):
     return stats
 
 
+def time_steps(batch, steps=50):
+    """Device time of the library's training step (forward, backward, Adam) on random data, and
+    the rate of its tensor-core GEMMs (layers 1-3 forward, their weight gradients, the input
+    gradients of layers 3 and 2)."""
+    import torch
+    rng = np.random.default_rng(0)
+    S = torch.tensor(rng.standard_normal((batch, 384)).astype(np.float32) * 0.5, device="cuda")
+    P = torch.rand(batch, 4, device="cuda")
+    G = torch.rand(batch, device="cuda")
+    R = torch.randn(batch, 3, device="cuda")
+    trainer = KernelTrainer(torch, initial_weights(1), batch)
+    for _ in range(5):
+        trainer.run(S, P, G, R, lr=1e-4)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        trainer.run(S, P, G, R, lr=1e-4)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    flop = 2 * batch * (2 * 388 * 256 + 6 * 256 * 256)
+    print(f"batch {batch}: {ms:.3f} ms per training step, {flop / ms / 1e9:.1f} TFLOP/s in the "
+          f"tensor-core GEMMs, error flag {trainer.error_flag()}", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=sg.DEFAULT_WEIGHTS)
@@ -290,7 +316,12 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--evaluate-only", action="store_true")
+    ap.add_argument("--time-steps", type=int, default=0, metavar="BATCH",
+                    help="time training steps of this batch on random data and exit")
     args = ap.parse_args()
+    if args.time_steps:
+        time_steps(args.time_steps)
+        return
     if args.evaluate_only:
         evaluate(sg.load_weights(args.out))
         evaluate(sg.load_weights(args.out), realistic=True)
