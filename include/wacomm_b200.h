@@ -130,7 +130,10 @@ typedef struct wacomm_b200_options {
     int rng;                  /* WACOMM_B200_RNG_* */
     int block_size;           /* threads per block of the move kernel: 64..1024, multiple of 32 */
     int substeps_per_launch;  /* 0: one launch per interval; else launches of this many dti */
-    int sort_by_cell;         /* 1: order the work by forcing cell before each launch */
+    int sort_by_cell;         /* N >= 1: order the work by forcing cell, sorting the resident
+                                 population every N-th interval (the intervals between take the
+                                 last sort's order); 1 (the default): every interval; 0: never;
+                                 at most 64; wacomm_b200_autotune chooses 1, 2 or 4 */
     int fuse_concentration;   /* 1: count the concentration in the move kernel's epilogue */
     int launch_shape;         /* FP32 step: 0 = 256 threads, registers unbounded; 1 = 128 threads,
                                  3 blocks/SM; 2 = 256 threads, 2 blocks/SM; 3 = 128 threads,
@@ -259,7 +262,10 @@ int wacomm_b200_graph_release(wacomm_b200_context *ctx);
  * arithmetic: launch_shape 0..3; reference arithmetic: block_size 64, 128, 192, 256), each from
  * the same resident records and concentration after a warm-up pass, keeps the fastest in the
  * options and restores records and concentration: only the options change. Writes the chosen
- * value and its device ms. No reference counterpart. */
+ * value and its device ms. With the cell sort on and four intervals from time_index inside the
+ * forcing window, it then times those four intervals from the same snapshot sorting every 1, 2
+ * or 4 of them and keeps the fastest cadence in options.sort_by_cell. No reference
+ * counterpart. */
 int wacomm_b200_autotune(wacomm_b200_context *ctx, int time_index, int *best, float *best_ms);
 
 /* The same interval through host buffers: uploads n records from `particles` (pinned or

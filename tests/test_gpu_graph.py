@@ -156,6 +156,7 @@ def test_autotune_changes_only_the_launch_shape(cuda_device, setting):
     shape, ms = e.autotune(1)
     assert shape in (0, 1, 2, 3) and ms > 0
     assert e.options().launch_shape == shape
+    assert e.options().sort_by_cell in (1, 2, 4)  # the sort cadence chosen after the shape
     after = e.get_particles()
     for f in before.dtype.names:
         assert before[f].tobytes() == after[f].tobytes(), f
@@ -201,3 +202,35 @@ def test_autotune_block_size_under_reference_arithmetic(cuda_device, setting):
         assert before[f].tobytes() == after[f].tobytes(), f
     assert np.array_equal(conc, e.concentration())
     e.close()
+
+
+@pytest.mark.parametrize("surrogate", [False, True])
+def test_sort_cadence_changes_only_the_work_order(cuda_device, setting, surrogate):
+    """Sorting every N-th interval (options.sort_by_cell = N) only changes the order the work is
+    taken in: every particle is moved on its own, so the records, the concentration and the
+    particle-step count equal those of sorting every interval, bit for bit, for the plain step
+    (leeway drift, random walk) and for the learned form's walk kernel."""
+    win, env, cfg = setting
+    parts = batch(30000, 9, win)
+    if surrogate:
+        parts["driftObjectType"][:] = 0
+    results = []
+    for cadence in (1, 3, 0):
+        if surrogate:
+            e = Engine(0, arithmetic="fp32", storage="fp16", surrogate=1, rng="philox",
+                       sort_by_cell=cadence)
+            e.set_config(default_config(random=True, randomSeed=31))
+            e.load_window(win)
+            e.set_surrogate()
+            e.concentration_reset(win.T)
+            e.set_particles(parts)
+        else:
+            e = engine(win, env, cfg, parts)
+            e.set_options(sort_by_cell=cadence)
+        steps = eager(e)
+        results.append((e.get_particles(), e.concentration(), steps))
+        e.close()
+    for got, conc, steps in results[1:]:
+        for f in got.dtype.names:
+            assert got[f].tobytes() == results[0][0][f].tobytes(), f
+        assert np.array_equal(conc, results[0][1]) and steps == results[0][2]

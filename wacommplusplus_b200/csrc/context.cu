@@ -84,6 +84,11 @@ struct wacomm_b200_context {
     // the previous one keeps the histogram atomics from piling up where particles gather.
     uint32_t *dSeq = nullptr;
     std::vector<size_t> seqBounds;
+    // Intervals since the resident population was last sorted by cell, for a sort cadence
+    // (options.sort_by_cell = N > 1: sort every N-th interval, the others take the last order).
+    // Large after the records were replaced, appended or compacted: the next interval sorts.
+    int sortedAgo = 1 << 30;
+    bool mayReuseOrder = false;  // set around the resident whole-population interval only
     size_t workCap = 0;
     uint32_t *dHist = nullptr, *dOffsets = nullptr;
     size_t binsCap = 0;
@@ -342,6 +347,8 @@ int validate_options(wacomm_b200_context *ctx, const wacomm_b200_options &o) {
     if (o.arithmetic == WACOMM_B200_ARITH_REFERENCE && o.storage != WACOMM_B200_STORAGE_FP32)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT,
                     "reference arithmetic reads the forcing exactly and needs FP32 storage");
+    if (o.sort_by_cell < 0 || o.sort_by_cell > 64)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "sort_by_cell %d out of [0, 64]", o.sort_by_cell);
     if (o.rng != WACOMM_B200_RNG_REFERENCE && o.rng != WACOMM_B200_RNG_PHILOX)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "rng %d out of range", o.rng);
     if (o.block_size < 32 || o.block_size > 256 || o.block_size % 32)
@@ -568,11 +575,19 @@ int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t of
     if (chunk > 0 && base.length > 0) nChunks = (int)std::ceil(base.length / chunk);
     if (nChunks < 1) nChunks = 1;
     for (int c = 0; c < nChunks; c++) {
-        if (ctx->opt.sort_by_cell) {
+        // a sort cadence of N > 1: between sorts the work takes the last sort's order (any
+        // permutation is a valid work order; the cell locality of a recent one is kept)
+        const bool reuse = c == 0 && ctx->mayReuseOrder && seqIn && ctx->opt.sort_by_cell > 1 &&
+                           ctx->sortedAgo + 1 < ctx->opt.sort_by_cell;
+        if (reuse) {
+            L.order = seqIn;
+            ctx->sortedAgo++;
+        } else if (ctx->opt.sort_by_cell) {
             int rc = sort_work(ctx, S, count, keys, order, c == 0 ? seqIn : seqOut, seqOut,
                                launches);
             if (rc) return rc;
             L.order = order;
+            if (c == 0) ctx->sortedAgo = 0;
         }
         if (!ctx->moveTimed && !ctx->capturing) {
             CUDA_TRY(ctx, cudaEventRecord(ctx->evMove0, ctx->stream));
@@ -673,9 +688,10 @@ int enqueue_interval(wacomm_b200_context *ctx, int time_index, int &launches) {
     const std::vector<size_t> whole{0, ctx->n};
     const uint32_t *seqIn = ctx->seqBounds == whole ? ctx->dSeq : nullptr;
     ctx->seqBounds.clear();
-    if ((rc = run_interval(ctx, P, 0, ctx->n, ctx->dKeys, ctx->dOrder, seqIn, ctx->dSeq,
-                           launches)))
-        return rc;
+    ctx->mayReuseOrder = true;
+    rc = run_interval(ctx, P, 0, ctx->n, ctx->dKeys, ctx->dOrder, seqIn, ctx->dSeq, launches);
+    ctx->mayReuseOrder = false;
+    if (rc) return rc;
     if (ctx->opt.sort_by_cell) ctx->seqBounds = whole;
     return WACOMM_B200_OK;
 }
@@ -748,15 +764,22 @@ int run_surrogate(wacomm_b200_context *ctx, const IntervalParams &P, int &launch
     st.invMetric = A.invMetric;
     st.depthF = A.depthIntervalsF;
     if (diffuse && ctx->opt.sort_by_cell) {
-        // the walk takes its particles in cell order; the sort walks the previous order
+        // the walk takes its particles in cell order; the sort walks the previous order (with a
+        // sort cadence N > 1, the intervals between sorts take that order as it is)
         const std::vector<size_t> whole{0, ctx->n};
         const uint32_t *seqIn = ctx->seqBounds == whole ? ctx->dSeq : nullptr;
-        ctx->seqBounds.clear();
-        if ((rc = sort_work(ctx, ctx->S.s, count, ctx->dKeys, ctx->dOrder, seqIn, ctx->dSeq,
-                            launches)))
-            return rc;
-        ctx->seqBounds = whole;
-        st.walkOrder = ctx->dOrder;
+        if (seqIn && ctx->opt.sort_by_cell > 1 && ctx->sortedAgo + 1 < ctx->opt.sort_by_cell) {
+            ctx->sortedAgo++;
+            st.walkOrder = seqIn;
+        } else {
+            ctx->seqBounds.clear();
+            if ((rc = sort_work(ctx, ctx->S.s, count, ctx->dKeys, ctx->dOrder, seqIn, ctx->dSeq,
+                                launches)))
+                return rc;
+            ctx->seqBounds = whole;
+            ctx->sortedAgo = 0;
+            st.walkOrder = ctx->dOrder;
+        }
     }
     st.dry = ctx->dDry;
     st.z = ctx->dZ;
@@ -1184,6 +1207,7 @@ int wacomm_b200_set_particles(wacomm_b200_context *ctx, const wacomm_b200_partic
                               size_t n) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     ctx->n = 0;
+    ctx->sortedAgo = 1 << 30;
     return wacomm_b200_append_particles(ctx, host, n);
 }
 
@@ -1192,6 +1216,7 @@ int wacomm_b200_append_particles(wacomm_b200_context *ctx, const wacomm_b200_par
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     if (n == 0) return WACOMM_B200_OK;
     if (!host) return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "null particles");
+    ctx->sortedAgo = 1 << 30;
     if (ctx->n + n >= MAX_PARTICLES)
         return fail(ctx, WACOMM_B200_ERR_CAPACITY, "more than 2^31 particles");
     cudaSetDevice(ctx->device);
@@ -1375,6 +1400,7 @@ int wacomm_b200_move_interval_host(wacomm_b200_context *ctx, int time_index,
 int wacomm_b200_remove_dead(wacomm_b200_context *ctx) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     if (ctx->n == 0) return WACOMM_B200_OK;
+    ctx->sortedAgo = 1 << 30;
     cudaSetDevice(ctx->device);
     int rc;
     if ((rc = reserve_work(ctx, ctx->n))) return rc;
@@ -1396,6 +1422,7 @@ int wacomm_b200_emit(wacomm_b200_context *ctx, const wacomm_b200_source *sources
                      size_t *emitted) {
     if (!ctx) return WACOMM_B200_ERR_ARGUMENT;
     if (emitted) *emitted = 0;
+    ctx->sortedAgo = 1 << 30;
     if (n_sources < 0 || (n_sources > 0 && !sources))
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "%d sources at %p", n_sources, (const void *)sources);
     if (!ctx->hasConfig) return fail(ctx, WACOMM_B200_ERR_STATE, "set_config has not been called");
@@ -2320,6 +2347,40 @@ int wacomm_b200_autotune(wacomm_b200_context *ctx, int time_index, int *best, fl
     if (!rc) {
         if (fp32) ctx->opt.launch_shape = chosen;
         else ctx->opt.block_size = chosen;
+    }
+    // The sort cadence, with the chosen shape: four intervals from the snapshot sorting every
+    // 1, 2 or 4 of them; the fastest run sets options.sort_by_cell (when sorting is on and the
+    // four intervals lie inside the forcing window).
+    const int dir = ctx->cfg.trackingDirection, T = (int)ctx->times.size();
+    const int runEnd = time_index + 4 * dir;
+    if (!rc && saved.sort_by_cell && runEnd >= 0 && runEnd < T) {
+        int cadence = saved.sort_by_cell;
+        float bestRun = INFINITY;
+        for (int pass = 0; pass < 2 && !rc; pass++)
+            for (int cad : {1, 2, 4}) {
+                ctx->opt.sort_by_cell = cad;
+                cudaError_t e = restore();
+                if (e != cudaSuccess) {
+                    rc = fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e));
+                    break;
+                }
+                ctx->sortedAgo = 1 << 30;  // every run starts with a sort
+                float total = 0;
+                for (int q = 0; q < 4 && !rc; q++) {
+                    if ((rc = wacomm_b200_move_interval(ctx, time_index + q * dir))) break;
+                    float ms = 0;
+                    e = cudaEventSynchronize(ctx->ev1);
+                    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+                    if (e != cudaSuccess) rc = fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e));
+                    total += ms;
+                }
+                if (!rc && pass == 1 && total < bestRun) {
+                    bestRun = total;
+                    cadence = cad;
+                }
+            }
+        ctx->opt.sort_by_cell = cadence;
+        ctx->sortedAgo = 1 << 30;
     }
     cudaError_t e = restore();
     cudaError_t s = cudaStreamSynchronize(ctx->stream);
