@@ -29,6 +29,10 @@ import os
 # core, packed (set before any OpenMP runtime is loaded).
 os.environ.setdefault("OMP_PLACES", "cores")
 os.environ.setdefault("OMP_PROC_BIND", "close")
+# The CPUs this process may run on, read before the first OpenMP region: with OMP_PROC_BIND set,
+# that region binds the calling thread to its own place, after which the thread's affinity mask
+# names one core only.
+CPU_SET = sorted(os.sched_getaffinity(0))
 import statistics
 import subprocess
 import sys
@@ -121,11 +125,11 @@ class ClockSampler:
 
 
 def physical_cores():
-    """(count, how) of the physical cores among the CPUs this process may run on: one per
+    """(count, how) of the physical cores among the CPUs this process could run on at start: one per
     (package, core) pair of the CPU topology. Where the topology is not exposed (a virtual machine
     may report every CPU as core 0, or more than two CPUs per core), the logical CPUs are counted
     and `how` says so."""
-    cpus = sorted(os.sched_getaffinity(0))
+    cpus = CPU_SET
     seen = set()
     for cpu in cpus:
         base = f"/sys/devices/system/cpu/cpu{cpu}/topology/"
@@ -422,7 +426,8 @@ def run_batched(args):
                                "curvilinear hourly and Stokes 0.05-degree 3-hourly regridded on "
                                "the device, Philox random walk, fused concentration, one CUDA "
                                "graph per 48-hour run",
-                   "launch_shape": shape, "autotune_ms": tune_ms, "regrid_s": t_regrid,
+                   "launch_shape": shape, "sort_cadence": engine.options().sort_by_cell,
+                   "autotune_ms": tune_ms, "regrid_s": t_regrid,
                    "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
