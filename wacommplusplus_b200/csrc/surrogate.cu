@@ -405,17 +405,15 @@ __device__ __forceinline__ int dry_in_box(const int *pre, int xi, int ja, int jb
     return pre[(jb + 1) * w + ib + 1] - pre[ja * w + ib + 1] - pre[(jb + 1) * w + ia] + pre[ja * w + ia];
 }
 
-// The MMA jobs of a block in the order the row warps make their operands ready: layer 2 of tiles
-// 0 and 1, layer 3 of tile 0, then for each tile k layer 3 of tile k+1 and layer 2 of tile k+2.
-// fn(tile, layer) returns false to stop.
+// The MMA jobs of a block in the order the row warps make their operands ready: layers 2 and 3 of
+// tile 0, 1, ... (the rows take prologue k+1, epilogue 3 of k, epilogue 2 of k+1, so layer 2 of
+// tile k+1 runs on the tensor cores while the rows finish layer 3 of tile k, and layer 3 of tile
+// k+1 while they build the operand of tile k+2). fn(tile, layer) returns false to stop.
 template <class Fn>
 __device__ __forceinline__ void for_each_job(int nT, Fn fn) {
-    if (nT > 0 && !fn(0, 0)) return;
-    if (nT > 1 && !fn(1, 0)) return;
-    if (nT > 0 && !fn(0, 1)) return;
     for (int k = 0; k < nT; k++) {
-        if (k + 1 < nT && !fn(k + 1, 1)) return;
-        if (k + 2 < nT && !fn(k + 2, 0)) return;
+        if (!fn(k, 0)) return;
+        if (!fn(k, 1)) return;
     }
 }
 
@@ -686,14 +684,15 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             return ok;
         };
 
-        RowTag cur{0u, ROW_EMPTY, 0}, next{0u, ROW_EMPTY, 0}, after{0u, ROW_EMPTY, 0};
+        RowTag cur{0u, ROW_EMPTY, 0}, next{0u, ROW_EMPTY, 0};
         if (nT > 0) cur = prologue(0, fetch(0));
-        if (nT > 1) next = prologue(1, fetch(1));
+        RowState ahead = fetch(1);
         if (nT > 0) epilogue2(0);
         for (int k = 0; k < nT; k++) {
+            // operand of tile k+1 (its layer 2 then runs while the rows finish layer 3 of tile k)
+            if (k + 1 < nT) next = prologue(k + 1, ahead);
             // the state gather of tile k+2 overlaps the epilogues below
-            const RowState ahead = fetch(k + 2);
-            if (k + 1 < nT) epilogue2(k + 1);
+            ahead = fetch(k + 2);
             float o0, o1, o2;
             epilogue3(k, o0, o1, o2);
             // the quarter's stop decision, written by its group-0 warp in the previous tile: the
@@ -715,10 +714,9 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                 a.rows[tileOf(k) * TILE + r] =
                     make_float4(s0 + b4s[0], s1 + b4s[1], s2 + b4s[2], __int_as_float(code));
             }
-            if (k + 2 < nT) after = prologue(k + 2, ahead);
             if (stop) break;
+            if (k + 1 < nT) epilogue2(k + 1);
             cur = next;
-            next = after;
         }
     }
     fence_before_sync();
