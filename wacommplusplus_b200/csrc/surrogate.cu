@@ -61,13 +61,15 @@ constexpr size_t OFF_W4 = OFF_W1P + 4096;
 constexpr size_t OFF_B4 = OFF_W4 + 3072;
 constexpr size_t PACKED_BYTES = OFF_B4 + 1024;
 
-// GELU, tanh form: h = x/2 + (x/2) tanh(x (c0 + c1 x^2)), c0 = sqrt(2/pi), c1 = 0.044715 c0.
-__device__ __forceinline__ float gelu_tanh(float x) {
+// Twice the GELU, tanh form: 2 h = x + x tanh(x (c0 + c1 x^2)), c0 = sqrt(2/pi), c1 = 0.044715 c0.
+// The factor 1/2 of the GELU is carried by the consumer instead: the packed weights of layers 2,
+// 3 and 4 are stored halved. Scaling by a power of two is exact in FP32 and BF16, so the rounded
+// activations and every product are those of the unscaled network, one multiply fewer per unit.
+__device__ __forceinline__ float gelu2_tanh(float x) {
     const float inner = x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f);
     float t;
     asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(inner));
-    const float h = 0.5f * x;
-    return fmaf(h, t, h);
+    return fmaf(x, t, x);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
@@ -607,7 +609,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                         for (int e = 0; e < 8; e++) {
                             const float4 wp =
                                 *reinterpret_cast<const float4 *>(w1ps + (cBase + (q0 + q) * 8 + e) * 4);
-                            h[e] = gelu_tanh(h[e] + wp.x * jF + wp.y * iF + wp.z * kF + wp.w * a0);
+                            h[e] = gelu2_tanh(h[e] + wp.x * jF + wp.y * iF + wp.z * kF + wp.w * a0);
                         }
                         out.x = pack_bf16(h[0], h[1]);
                         out.y = pack_bf16(h[2], h[3]);
@@ -622,7 +624,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             return tag;
         };
 
-        // layer-2 epilogue of tile x: GELU(acc + b2) -> A[x & 1]
+        // layer-2 epilogue of tile x: 2 GELU(acc + b2) -> A[x & 1] (the halved W3 takes the 2 back)
         auto epilogue2 = [&](int x) {
             const int buf = x & 1;
             const bool ok = mbar_wait(&accFull[buf], 0, &abortFlag);
@@ -638,10 +640,10 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     uint4 out;
-                    out.x = pack_bf16(gelu_tanh(v[8 * q + 0] + b2s[c0 + 8 * q + 0]), gelu_tanh(v[8 * q + 1] + b2s[c0 + 8 * q + 1]));
-                    out.y = pack_bf16(gelu_tanh(v[8 * q + 2] + b2s[c0 + 8 * q + 2]), gelu_tanh(v[8 * q + 3] + b2s[c0 + 8 * q + 3]));
-                    out.z = pack_bf16(gelu_tanh(v[8 * q + 4] + b2s[c0 + 8 * q + 4]), gelu_tanh(v[8 * q + 5] + b2s[c0 + 8 * q + 5]));
-                    out.w = pack_bf16(gelu_tanh(v[8 * q + 6] + b2s[c0 + 8 * q + 6]), gelu_tanh(v[8 * q + 7] + b2s[c0 + 8 * q + 7]));
+                    out.x = pack_bf16(gelu2_tanh(v[8 * q + 0] + b2s[c0 + 8 * q + 0]), gelu2_tanh(v[8 * q + 1] + b2s[c0 + 8 * q + 1]));
+                    out.y = pack_bf16(gelu2_tanh(v[8 * q + 2] + b2s[c0 + 8 * q + 2]), gelu2_tanh(v[8 * q + 3] + b2s[c0 + 8 * q + 3]));
+                    out.z = pack_bf16(gelu2_tanh(v[8 * q + 4] + b2s[c0 + 8 * q + 4]), gelu2_tanh(v[8 * q + 5] + b2s[c0 + 8 * q + 5]));
+                    out.w = pack_bf16(gelu2_tanh(v[8 * q + 6] + b2s[c0 + 8 * q + 6]), gelu2_tanh(v[8 * q + 7] + b2s[c0 + 8 * q + 7]));
                     const int col = c0 + 8 * q;
                     *reinterpret_cast<uint4 *>(A + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
                 }
@@ -666,7 +668,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                 tmem_ld32(acc + (uint32_t)c0, v);
 #pragma unroll
                 for (int c = 0; c < 32; c++) {
-                    const float h = gelu_tanh(v[c] + b3s[c0 + c]);
+                    const float h = gelu2_tanh(v[c] + b3s[c0 + c]);
                     o0 = fmaf(h, w4s[c0 + c], o0);
                     o1 = fmaf(h, w4s[HID + c0 + c], o1);
                     o2 = fmaf(h, w4s[2 * HID + c0 + c], o2);
@@ -1209,8 +1211,9 @@ void surrogate_pack(const float *flat, uint8_t *out) {
     for (int n = 0; n < HID; n++) {
         for (int k = 0; k < N_STENCIL; k++) put(OFF_W1, n, k, w1[n * N_INPUT + k]);
         for (int k = 0; k < HID; k++) {
-            put(OFF_W2, n, k, w2[n * HID + k]);
-            put(OFF_W3, n, k, w3[n * HID + k]);
+            // halved: they multiply twice the GELU of the layer below (gelu2_tanh)
+            put(OFF_W2, n, k, 0.5f * w2[n * HID + k]);
+            put(OFF_W3, n, k, 0.5f * w3[n * HID + k]);
         }
     }
     float *fb1 = reinterpret_cast<float *>(out + OFF_B1), *fb2 = reinterpret_cast<float *>(out + OFF_B2);
@@ -1222,7 +1225,7 @@ void surrogate_pack(const float *flat, uint8_t *out) {
         fb3[n] = b3[n];
         for (int e = 0; e < 4; e++) fw1p[n * 4 + e] = w1[n * N_INPUT + N_STENCIL + e];
     }
-    for (int o = 0; o < 3 * HID; o++) fw4[o] = w4[o];
+    for (int o = 0; o < 3 * HID; o++) fw4[o] = 0.5f * w4[o];
     for (int o = 0; o < 3; o++) fb4[o] = b4[o];
 }
 
