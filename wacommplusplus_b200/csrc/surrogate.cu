@@ -10,8 +10,9 @@
 //   read coalesced, and the per-cell z rows and corner records it gathers stay in L2), layer 1 is
 //   finished on the CUDA cores from z and the four particle features, layers 2 and 3 run as two
 //   [128 x 256] x [256 x 256] tcgen05 GEMMs with the weights streamed through a 2-stage
-//   shared-memory ring by bulk copies, and layer 3's epilogue folds in the 3-output layer 4. The
-//   three outputs and a row tag go to rows[] per work item;
+//   shared-memory ring by bulk copies, each accumulating onto its bias (stored into TMEM by the
+//   rows), and layer 3's epilogue folds in the 3-output layer 4. The three outputs and a row tag
+//   go to rows[] per work item;
 // * surrogate_post_kernel: one thread per work item applies the displacement with the closures in
 //   closed form, updates the state and the fused concentration, and appends the particles the
 //   surrogate does not cover to a fallback list for the plain kernel. Run apart from the GEMM
@@ -510,7 +511,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                     for (int ks = 0; ks < 4; ks++)
                         mma_bf16(d, desc_sw128(smem_u32(A + kb * KBLOCK_A + ks * 32)),
                                  desc_sw128(smem_u32(ring + s * KBLOCK_W + ks * 32)), idesc,
-                                 (kb | ks) != 0);
+                                 true);  // onto the bias the rows stored
                     mma_commit(&empty[s]);
                 }
                 mma_commit(&accFull[buf]);
@@ -620,11 +621,17 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                     *reinterpret_cast<uint4 *>(A + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
                 }
             }
+            // layer 2 accumulates onto its bias: this warp's columns of the tile's accumulator
+            // (free since the rows read layer 3 of tile x-2 out of it) start as b2
+            const uint32_t acc = tmem + (uint32_t)((x & 1) * HID) + tlane;
+            for (int t = 0; t < chunks; t++) tmem_st32(acc + (uint32_t)(cBase + 32 * t), b2s + cBase + 32 * t);
+            tmem_wait_st();
             arrive(x & 1);
             return tag;
         };
 
-        // layer-2 epilogue of tile x: 2 GELU(acc + b2) -> A[x & 1] (the halved W3 takes the 2 back)
+        // layer-2 epilogue of tile x: 2 GELU(acc) -> A[x & 1] (the halved W3 takes the 2 back); the
+        // accumulator holds b2 + layer 2 and is reset to b3 for layer 3
         auto epilogue2 = [&](int x) {
             const int buf = x & 1;
             const bool ok = mbar_wait(&accFull[buf], 0, &abortFlag);
@@ -637,17 +644,19 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                 const int c0 = cBase + 32 * t;
                 float v[32];
                 tmem_ld32(acc + (uint32_t)c0, v);
+                tmem_st32(acc + (uint32_t)c0, b3s + c0);  // layer 3 accumulates onto b3
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
                     uint4 out;
-                    out.x = pack_bf16(gelu2_tanh(v[8 * q + 0] + b2s[c0 + 8 * q + 0]), gelu2_tanh(v[8 * q + 1] + b2s[c0 + 8 * q + 1]));
-                    out.y = pack_bf16(gelu2_tanh(v[8 * q + 2] + b2s[c0 + 8 * q + 2]), gelu2_tanh(v[8 * q + 3] + b2s[c0 + 8 * q + 3]));
-                    out.z = pack_bf16(gelu2_tanh(v[8 * q + 4] + b2s[c0 + 8 * q + 4]), gelu2_tanh(v[8 * q + 5] + b2s[c0 + 8 * q + 5]));
-                    out.w = pack_bf16(gelu2_tanh(v[8 * q + 6] + b2s[c0 + 8 * q + 6]), gelu2_tanh(v[8 * q + 7] + b2s[c0 + 8 * q + 7]));
+                    out.x = pack_bf16(gelu2_tanh(v[8 * q + 0]), gelu2_tanh(v[8 * q + 1]));
+                    out.y = pack_bf16(gelu2_tanh(v[8 * q + 2]), gelu2_tanh(v[8 * q + 3]));
+                    out.z = pack_bf16(gelu2_tanh(v[8 * q + 4]), gelu2_tanh(v[8 * q + 5]));
+                    out.w = pack_bf16(gelu2_tanh(v[8 * q + 6]), gelu2_tanh(v[8 * q + 7]));
                     const int col = c0 + 8 * q;
                     *reinterpret_cast<uint4 *>(A + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
                 }
             }
+            tmem_wait_st();
             arrive(buf);
             return ok;
         };
@@ -668,7 +677,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                 tmem_ld32(acc + (uint32_t)c0, v);
 #pragma unroll
                 for (int c = 0; c < 32; c++) {
-                    const float h = gelu2_tanh(v[c] + b3s[c0 + c]);
+                    const float h = gelu2_tanh(v[c]);
                     o0 = fmaf(h, w4s[c0 + c], o0);
                     o1 = fmaf(h, w4s[HID + c0 + c], o1);
                     o2 = fmaf(h, w4s[2 * HID + c0 + c], o2);
