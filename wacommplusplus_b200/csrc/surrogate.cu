@@ -73,6 +73,17 @@ __device__ __forceinline__ float gelu2_tanh(float x) {
     return fmaf(x, t, x);
 }
 
+// Asynchronous 16-byte copy global -> shared (cached in L1), completed by cp_async_wait_all of
+// the issuing thread.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(umma::smem_u32(smem)), "l"(gmem)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
     __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<uint32_t *>(&v);
@@ -560,7 +571,12 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
             }
             return st;
         };
-        auto prologue = [&](int x, const RowState &st) {
+        // A row's classification and layer-1 features, taken from its gathered state.
+        struct Pending {
+            RowTag tag;
+            float jF, iF, kF, a0;
+        };
+        auto classify = [&](const RowState &st) {
             RowTag tag{0u, ROW_EMPTY, 0};
             float jF = 0.f, iF = 0.f, kF = 0.f, a0 = 0.f;
             if (st.valid) {
@@ -586,19 +602,40 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                     }
                 }
             }
+            return Pending{tag, jF, iF, kF, a0};
+        };
+        // The row's per-cell layer-1 sums (FP16) for tile x, copied asynchronously into this
+        // thread's own part of operand buffer A[x & 1]: 16-byte chunk q at the swizzled slot where
+        // chunk q of the row's layer-1 output goes, so that the prologue converts them in place.
+        // Issued once the tensor cores are done with the buffer, they land while the rows work on
+        // the tiles before x.
+        auto stage = [&](int x, const Pending &pd) {
+            if (pd.tag.status == ROW_RUN) {
+                uint8_t *A = sA0 + (x & 1) * A_BYTES;
+                const uint4 *zrow = reinterpret_cast<const uint4 *>(a.z + (size_t)pd.tag.cl * HID + cBase);
+                for (int q = 0; q < chunks * 4; q++) {
+                    const int col = cBase + q * 8;
+                    cp_async16(A + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64), zrow + q);
+                }
+            }
+            cp_async_commit();
+        };
+        // layer 1 of tile x from its staged sums: 2 GELU(z + features) -> A[x & 1], in place
+        auto prologue = [&](int x, const Pending &pd) {
+            const RowTag tag = pd.tag;
+            const float jF = pd.jF, iF = pd.iF, kF = pd.kF, a0 = pd.a0;
             uint8_t *A = sA0 + (x & 1) * A_BYTES;
-            const uint4 *zrow = reinterpret_cast<const uint4 *>(a.z + (size_t)tag.cl * HID + cBase);
+            cp_async_wait_all();
 #pragma unroll 1
             for (int q0 = 0; q0 < chunks * 4; q0 += 4) {
-                uint4 zz[4];
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    zz[q] = tag.status == ROW_RUN ? __ldg(zrow + q0 + q) : make_uint4(0, 0, 0, 0);
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
+                    const int col = cBase + (q0 + q) * 8;
+                    uint4 *slotPtr = reinterpret_cast<uint4 *>(A + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64));
                     uint4 out = make_uint4(0, 0, 0, 0);
                     if (tag.status == ROW_RUN) {
-                        const __half2 *hz = reinterpret_cast<const __half2 *>(&zz[q]);
+                        const uint4 zz = *slotPtr;
+                        const __half2 *hz = reinterpret_cast<const __half2 *>(&zz);
                         float h[8];
 #pragma unroll
                         for (int e = 0; e < 4; e++) {
@@ -617,8 +654,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                         out.z = pack_bf16(h[4], h[5]);
                         out.w = pack_bf16(h[6], h[7]);
                     }
-                    const int col = cBase + (q0 + q) * 8;
-                    *reinterpret_cast<uint4 *>(A + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
+                    *slotPtr = out;
                 }
             }
             // layer 2 accumulates onto its bias: this warp's columns of the tile's accumulator
@@ -696,14 +732,17 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
         };
 
         RowTag cur{0u, ROW_EMPTY, 0}, next{0u, ROW_EMPTY, 0};
-        if (nT > 0) cur = prologue(0, fetch(0));
-        RowState ahead = fetch(1);
+        Pending pend = classify(fetch(0));
+        stage(0, pend);
+        if (nT > 0) cur = prologue(0, pend);
+        pend = classify(fetch(1));
+        stage(1, pend);
         if (nT > 0) epilogue2(0);
         for (int k = 0; k < nT; k++) {
             // operand of tile k+1 (its layer 2 then runs while the rows finish layer 3 of tile k)
-            if (k + 1 < nT) next = prologue(k + 1, ahead);
-            // the state gather of tile k+2 overlaps the epilogues below
-            ahead = fetch(k + 2);
+            if (k + 1 < nT) next = prologue(k + 1, pend);
+            // the state gather of tile k+2 overlaps the layer-3 epilogue below
+            const RowState ahead = fetch(k + 2);
             float o0, o1, o2;
             epilogue3(k, o0, o1, o2);
             // the quarter's stop decision, written by its group-0 warp in the previous tile: the
@@ -726,9 +765,14 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                     make_float4(s0 + b4s[0], s1 + b4s[1], s2 + b4s[2], __int_as_float(code));
             }
             if (stop) break;
+            // tile k+2's sums go to A[k & 1], which layer 3 of tile k no longer reads; they land
+            // during the layer-2 epilogue of tile k+1
+            pend = classify(ahead);
+            stage(k + 2, pend);
             if (k + 1 < nT) epilogue2(k + 1);
             cur = next;
         }
+        cp_async_wait_all();  // no copy into shared memory outlives the block
     }
     fence_before_sync();
     __syncthreads();
