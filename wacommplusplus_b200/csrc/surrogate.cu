@@ -73,6 +73,18 @@ __device__ __forceinline__ float gelu2_tanh(float x) {
     return fmaf(x, t, x);
 }
 
+// gelu2_tanh of two units with the packed FP32x2 multiply and multiply-add of sm_100 (the same
+// operations and roundings, half the instructions).
+__device__ __forceinline__ float2 gelu2_pair(float2 x) {
+    const float2 p = __ffma2_rn(__fmul2_rn(x, x), make_float2(0.035677408136300125f, 0.035677408136300125f),
+                                make_float2(0.7978845608028654f, 0.7978845608028654f));
+    const float2 inner = __fmul2_rn(x, p);
+    float2 t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t.x) : "f"(inner.x));
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t.y) : "f"(inner.y));
+    return __ffma2_rn(x, t, x);
+}
+
 // Asynchronous 16-byte copy global -> shared (cached in L1), completed by cp_async_wait_all of
 // the issuing thread.
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -441,7 +453,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
     __shared__ uint32_t tmemSlot;
     __shared__ int abortFlag;
     __shared__ int quarterStop[2][4];  // stop decisions per TMEM lane quarter, by tile parity
-    __shared__ __align__(16) float w1ps[HID * 4];  // read as float4 per hidden unit
+    __shared__ __align__(16) float w1ps[4 * HID];  // feature-major: pairs of units as float2
     __shared__ float b2s[HID], b3s[HID], w4s[3 * HID], b4s[4];
     // layer-4 partial sums of column groups 1.., by tile parity
     __shared__ float red[2][GROUPS - 1][TILE * 3];
@@ -465,7 +477,7 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
         const float *b3 = reinterpret_cast<const float *>(a.weights + OFF_B3);
         const float *w4 = reinterpret_cast<const float *>(a.weights + OFF_W4);
         const float *b4 = reinterpret_cast<const float *>(a.weights + OFF_B4);
-        for (int c = tid; c < HID * 4; c += STEP_THREADS) w1ps[c] = w1p[c];
+        for (int c = tid; c < HID * 4; c += STEP_THREADS) w1ps[(c & 3) * HID + (c >> 2)] = w1p[c];
         for (int c = tid; c < HID; c += STEP_THREADS) {
             b2s[c] = b2[c];
             b3s[c] = b3[c];
@@ -636,23 +648,22 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                     if (tag.status == ROW_RUN) {
                         const uint4 zz = *slotPtr;
                         const __half2 *hz = reinterpret_cast<const __half2 *>(&zz);
-                        float h[8];
+                        const float2 fj = make_float2(jF, jF), fi = make_float2(iF, iF);
+                        const float2 fk = make_float2(kF, kF), fa = make_float2(a0, a0);
+                        uint32_t o[4];
 #pragma unroll
                         for (int e = 0; e < 4; e++) {
-                            const float2 f2 = __half22float2(hz[e]);
-                            h[2 * e] = f2.x;
-                            h[2 * e + 1] = f2.y;
+                            // units col + 2e, col + 2e + 1: z + w_j jF + w_i iF + w_k kF + w_a a0
+                            const int u = col + 2 * e;
+                            float2 h = __half22float2(hz[e]);
+                            h = __ffma2_rn(*reinterpret_cast<const float2 *>(w1ps + u), fj, h);
+                            h = __ffma2_rn(*reinterpret_cast<const float2 *>(w1ps + HID + u), fi, h);
+                            h = __ffma2_rn(*reinterpret_cast<const float2 *>(w1ps + 2 * HID + u), fk, h);
+                            h = __ffma2_rn(*reinterpret_cast<const float2 *>(w1ps + 3 * HID + u), fa, h);
+                            h = gelu2_pair(h);
+                            o[e] = pack_bf16(h.x, h.y);
                         }
-#pragma unroll
-                        for (int e = 0; e < 8; e++) {
-                            const float4 wp =
-                                *reinterpret_cast<const float4 *>(w1ps + (cBase + (q0 + q) * 8 + e) * 4);
-                            h[e] = gelu2_tanh(h[e] + wp.x * jF + wp.y * iF + wp.z * kF + wp.w * a0);
-                        }
-                        out.x = pack_bf16(h[0], h[1]);
-                        out.y = pack_bf16(h[2], h[3]);
-                        out.z = pack_bf16(h[4], h[5]);
-                        out.w = pack_bf16(h[6], h[7]);
+                        out = make_uint4(o[0], o[1], o[2], o[3]);
                     }
                     *slotPtr = out;
                 }
@@ -683,11 +694,13 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                 tmem_st32(acc + (uint32_t)c0, b3s + c0);  // layer 3 accumulates onto b3
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    uint4 out;
-                    out.x = pack_bf16(gelu2_tanh(v[8 * q + 0]), gelu2_tanh(v[8 * q + 1]));
-                    out.y = pack_bf16(gelu2_tanh(v[8 * q + 2]), gelu2_tanh(v[8 * q + 3]));
-                    out.z = pack_bf16(gelu2_tanh(v[8 * q + 4]), gelu2_tanh(v[8 * q + 5]));
-                    out.w = pack_bf16(gelu2_tanh(v[8 * q + 6]), gelu2_tanh(v[8 * q + 7]));
+                    uint32_t o[4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const float2 h = gelu2_pair(make_float2(v[8 * q + 2 * e], v[8 * q + 2 * e + 1]));
+                        o[e] = pack_bf16(h.x, h.y);
+                    }
+                    const uint4 out = make_uint4(o[0], o[1], o[2], o[3]);
                     const int col = c0 + 8 * q;
                     *reinterpret_cast<uint4 *>(A + (col / 64) * KBLOCK_A + sw128_offset(r, col % 64)) = out;
                 }
@@ -712,11 +725,14 @@ __global__ void __launch_bounds__(STEP_THREADS, 1)
                 float v[32];
                 tmem_ld32(acc + (uint32_t)c0, v);
 #pragma unroll
-                for (int c = 0; c < 32; c++) {
-                    const float h = gelu2_tanh(v[c]);
-                    o0 = fmaf(h, w4s[c0 + c], o0);
-                    o1 = fmaf(h, w4s[HID + c0 + c], o1);
-                    o2 = fmaf(h, w4s[2 * HID + c0 + c], o2);
+                for (int c = 0; c < 32; c += 2) {
+                    const float2 h = gelu2_pair(make_float2(v[c], v[c + 1]));
+                    o0 = fmaf(h.x, w4s[c0 + c], o0);
+                    o1 = fmaf(h.x, w4s[HID + c0 + c], o1);
+                    o2 = fmaf(h.x, w4s[2 * HID + c0 + c], o2);
+                    o0 = fmaf(h.y, w4s[c0 + c + 1], o0);
+                    o1 = fmaf(h.y, w4s[HID + c0 + c + 1], o1);
+                    o2 = fmaf(h.y, w4s[2 * HID + c0 + c + 1], o2);
                 }
             }
             if (group > 0) {
