@@ -62,19 +62,12 @@ constexpr size_t OFF_W4 = OFF_W1P + 4096;
 constexpr size_t OFF_B4 = OFF_W4 + 3072;
 constexpr size_t PACKED_BYTES = OFF_B4 + 1024;
 
-// Twice the GELU, tanh form: 2 h = x + x tanh(x (c0 + c1 x^2)), c0 = sqrt(2/pi), c1 = 0.044715 c0.
-// The factor 1/2 of the GELU is carried by the consumer instead: the packed weights of layers 2,
-// 3 and 4 are stored halved. Scaling by a power of two is exact in FP32 and BF16, so the rounded
-// activations and every product are those of the unscaled network, one multiply fewer per unit.
-__device__ __forceinline__ float gelu2_tanh(float x) {
-    const float inner = x * fmaf(0.035677408136300125f, x * x, 0.7978845608028654f);
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(inner));
-    return fmaf(x, t, x);
-}
-
-// gelu2_tanh of two units with the packed FP32x2 multiply and multiply-add of sm_100 (the same
-// operations and roundings, half the instructions).
+// Twice the GELU, tanh form, of two units: 2 h = x + x tanh(x (c0 + c1 x^2)), c0 = sqrt(2/pi),
+// c1 = 0.044715 c0, with the packed FP32x2 multiply and multiply-add of sm_100 (half the
+// instructions of the scalar form, the same roundings). The factor 1/2 of the GELU is carried by
+// the consumer instead: the packed weights of layers 2, 3 and 4 are stored halved. Scaling by a
+// power of two is exact in FP32 and BF16, so the rounded activations and every product are those
+// of the unscaled network, one multiply fewer per unit.
 __device__ __forceinline__ float2 gelu2_pair(float2 x) {
     const float2 p = __ffma2_rn(__fmul2_rn(x, x), make_float2(0.035677408136300125f, 0.035677408136300125f),
                                 make_float2(0.7978845608028654f, 0.7978845608028654f));
@@ -943,6 +936,31 @@ __device__ __forceinline__ CellSurface load_surface(const CellSurface *s, int ce
     return CellSurface{__ldg(q), __ldg(q + 1)};
 }
 
+// One axis of a destination that may lie one cell beyond the domain, reflected at its edge as
+// reflect_domain does (x -> 2 max - x past the last node, -x before the first): n is the
+// destination cell on the axis, d its fraction there, x the fraction measured from the start cell
+// and last the last valid cell. Returns whether the result is a cell and a fraction in [0, 1)
+// (strictly inside (0, 1) when mirrored: a fraction of exactly 1 is the nextafter case, left to the
+// FP64 landing); flip says whether the axis was mirrored.
+__device__ __forceinline__ bool mirror_axis(int n, float d, float x, int last, int &cell, float &frac,
+                                            bool &flip) {
+    flip = false;
+    cell = n;
+    frac = d;
+    if (n >= 0 && n <= last) return d >= 0.f && d < 1.f;
+    flip = true;
+    if (n == last + 1) {
+        cell = last;
+        frac = 2.f - x;
+    } else if (n == -1) {
+        cell = 0;
+        frac = -x;
+    } else {
+        return false;
+    }
+    return frac > 0.f && frac < 1.f;
+}
+
 // One particle over the rest of a forward interval: the surrogate's deterministic displacement,
 // spread evenly over the substeps as constant rates (m/s), plus the plain stochastic operator and
 // closures of every substep, as the FP32 Euler step applies them (Particle.cpp:505-533,644-814;
@@ -1050,7 +1068,41 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
             surface_from(load_surface(W.surface, inside ? nj * xi + ni : cell), jD, iD);
         const bool vertical = (float)kI - kN > 0.f || (float)kI - kN < kLowerF;
         carried = inside && !vertical && there.height(alpha) > shore;
-        if (carried) {
+        // The domain edge, under the closures that do not look at the land there: the destination
+        // cell lies outside the valid cells and the level stays in range. Constraint drops the
+        // horizontal move (the position and its surface sums stay); reflection mirrors each axis
+        // that left at the edge (NumericalHelpers.hpp:67-74). FP32 work on the fractions, as a
+        // landing in water, whenever the mirrored fraction lies inside (0, 1); otherwise, and for
+        // the other closures, the FP64 landing below. A particle the current keeps pushing against
+        // the edge takes this path every substep.
+        bool edge = false;
+        if (!carried && !vertical && kD >= 0.f && kD < 1.f && !valid_cell(nj, ni, eta, xi)) {
+            if (cfg.horizontalClosure == CLOSURE_CONSTRAINT) {
+                edge = true;
+                carried = true;
+            } else if (cfg.horizontalClosure == CLOSURE_REFLECTION) {
+                int mj, mi;
+                float mjF, miF;
+                bool flipJ, flipI;
+                if (mirror_axis(nj, jD, jN, eta - 2, mj, mjF, flipJ) &&
+                    mirror_axis(ni, iD, iN, xi - 2, mi, miF, flipI)) {
+                    edge = true;  // carried stays false: the next substep reads the new surface
+                    jI = mj;
+                    iI = mi;
+                    jF = mjF;
+                    iF = miF;
+                    if (flipJ) jLo = -jLo;
+                    if (flipI) iLo = -iLo;
+                }
+            }
+            if (edge) {
+                kI -= dk;
+                kF = kD;
+            }
+        }
+        if (edge) {
+            // landed above
+        } else if (carried) {
             jI = nj;
             iI = ni;
             jF = jD;
@@ -1280,7 +1332,7 @@ void surrogate_pack(const float *flat, uint8_t *out) {
     for (int n = 0; n < HID; n++) {
         for (int k = 0; k < N_STENCIL; k++) put(OFF_W1, n, k, w1[n * N_INPUT + k]);
         for (int k = 0; k < HID; k++) {
-            // halved: they multiply twice the GELU of the layer below (gelu2_tanh)
+            // halved: they multiply twice the GELU of the layer below (gelu2_pair)
             put(OFF_W2, n, k, 0.5f * w2[n * HID + k]);
             put(OFF_W3, n, k, 0.5f * w3[n * HID + k]);
         }
