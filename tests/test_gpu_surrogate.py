@@ -318,6 +318,44 @@ def test_diffusive_walk_matches_the_oracle_draw_for_draw(cuda_device, scene, clo
     assert np.allclose(got["health"][both], want["health"][both], rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("closure", [1, 3])
+def test_diffusive_walk_at_the_domain_edges(cuda_device, closure):
+    """Particles started in the outermost cells of the analytic grid, which the current and the
+    walk push against the edges substep after substep: the walk's FP32 edge landings (constraint:
+    the horizontal move dropped; reflection: the axis mirrored) against the oracle's FP64
+    closures, draw for draw."""
+    win = syn.config1_window(n_frames=3)
+    rng = np.random.default_rng(40 + closure)
+    n = 20000
+    p = syn.uniform_particles(n, win.eta, win.xi, time=win.times[0], seed=40 + closure)
+    side = np.arange(n) % 4
+    east, north = win.xi - 1.0, win.eta - 1.0   # the coordinates stay below these
+    p["i"] = np.where(side == 0, rng.uniform(east - 1.5, east - 1e-3, n), p["i"])
+    p["j"] = np.where(side == 1, rng.uniform(north - 1.5, north - 1e-3, n), p["j"])
+    p["i"] = np.where(side == 2, rng.uniform(1e-3, 1.5, n), p["i"])
+    p["j"] = np.where(side == 3, rng.uniform(1e-3, 1.5, n), p["j"])
+    corner = np.arange(n) % 16 == 0                 # the north-east corner
+    p["i"][corner] = rng.uniform(east - 1.0, east - 1e-3, corner.sum())
+    p["j"][corner] = rng.uniform(north - 1.0, north - 1e-3, corner.sum())
+    cfg = default_config(random=True, integrator=1, horizontalClosure=closure,
+                         upperClosure=closure, lowerClosure=3, sigma=12.0)
+    e = walk_engine(win, cfg)
+    e.set_particles(p)
+    want = p.copy()
+    for t in (0, 1):
+        e.move_interval(t)
+        ob.oracle_move(cfg, want, win, t, ob.SEMANTICS_HOST, threads=0)
+    got = e.get_particles()
+    e.close()
+    for f in ("id", "time", "driftObjectType", "driftSide"):
+        assert np.array_equal(got[f], want[f]), f
+    assert near(got, want, WALK_MAX) >= 0.999
+    # the particles did meet the edges: some sit within a tenth of a cell of one
+    edge = ((want["i"] > east - 0.1) | (want["j"] > north - 0.1) | (want["i"] < 0.1) |
+            (want["j"] < 0.1))
+    assert edge.mean() > 0.05, edge.mean()
+
+
 @pytest.mark.parametrize("storage,bound", [("fp32", WALK_MAX), ("fp16", 3e-3)])
 def test_diffusive_walk_matches_the_fp32_step_on_philox_streams(cuda_device, storage, bound):
     """Philox streams keyed on (particle, interval, step time), the same in both kernels. With
