@@ -235,14 +235,18 @@ __device__ __forceinline__ double jibe_step_probability(double hourly, double se
 __device__ __forceinline__ double reflect_cell(double oldCoordinate, int oldCell, double candidate,
                                                int candidateCell) {
     if (candidateCell < oldCell) return oldCell + fabs(oldCoordinate - candidate);
-    if (candidateCell > oldCell) return candidateCell - fmod(candidate, 1.0);
+    // fmod(x, 1) is x - trunc(x) exactly (both are exact for every finite double)
+    if (candidateCell > oldCell) return candidateCell - (candidate - trunc(candidate));
     return candidate;
 }
 
 // NumericalHelpers.hpp:67-74
 __device__ __forceinline__ double reflect_domain(double coordinate, double maximum) {
     if (maximum <= 0) return 0;
-    double reflected = fmod(coordinate, 2.0 * maximum);
+    // fmod returns its argument when |coordinate| < 2 maximum (exact): the library call only for
+    // positions more than a domain away
+    const double period = 2.0 * maximum;
+    double reflected = fabs(coordinate) < period ? coordinate : fmod(coordinate, period);
     if (reflected < 0) reflected += 2.0 * maximum;
     if (reflected >= maximum) reflected = 2.0 * maximum - reflected;
     if (reflected >= maximum) reflected = nextafter(maximum, 0.0);
