@@ -18,8 +18,11 @@ the same random walk and the deterministic surrogate; with the tensor-core roofl
 kernel and its position error after 24 hours against the FP64 reference-arithmetic kernel, on the
 analytic grid (1,048,576-particle subset) and on a non-uniform streamfunction flow. `precision`
 gives the plain step with FP32, FP16 and BF16 forcing storage (throughput and 24-hour error) and
-the FP64 reference-arithmetic kernel's throughput. Kernel times come from per-interval events
-recorded inside the timed loops.
+the FP64 reference-arithmetic kernel's throughput. `realistic` runs the realistic grid
+(1024x1024x30, ~20 % land, records generated on the device, 4,194,304 particles from the device
+emitter, Philox random walk, dt = 15 s) for 5 intervals after 3 warm-up ones, with its own
+roofline and CPU baseline (`--workload realistic` runs it alone, longer). Kernel times come from
+per-interval events recorded inside the timed loops.
 """
 import argparse
 import json
@@ -229,18 +232,26 @@ def run_reference(args):
 
 
 def run_realistic(args):
+    n_total = args.particles if args.particles != 1 << 24 else 1 << 22
+    line = realistic_leg(n_total, max(args.warmup, 3), args.steps, not args.no_cpu)
+    print(json.dumps(line), flush=True)
+
+
+def realistic_leg(n_total, warm, steps, with_cpu):
     """The realistic configuration on one GPU: 1024x1024 rho nodes, 30 Vtransform-2 levels, ~20 %
-    land, 24 hourly FP32 records of a 64-mode streamfunction flow; 4,194,304 particles released
-    by the device emitter from 64 uniform-rate sources during the first hour; dt = 15 s,
-    random walk with Philox streams, fused uint32 concentration, dead-record compaction each
-    interval. One step = emission + cell sort + move + concentration + compaction of one
-    interval, device-timed."""
+    land, hourly FP32 records of a 64-mode streamfunction flow (generated on the device, as many
+    as the run needs, at most 24); n_total particles released by the device emitter from 64
+    uniform-rate sources during the first hour; dt = 15 s, random walk with Philox streams,
+    fused uint32 concentration, dead-record compaction each interval. One step = emission + cell
+    sort + move + concentration + compaction of one interval, device-timed."""
     import torch
     from wacommplusplus_b200 import synthetic as syn
     from wacommplusplus_b200.engine import Engine
     from wacommplusplus_b200.types import PARTICLE_DTYPE, default_config, make_sources
 
-    n_total, n_sources, frames = args.particles if args.particles != 1 << 24 else 1 << 22, 64, 24
+    n_sources = 64
+    n_steps = min(steps, 24 - 1 - warm)
+    frames = warm + n_steps + 1
     forcing = syn.RealisticForcing(eta=1024, xi=1024, s_rho=30, n_frames=frames, seed=2)
     cfg = default_config(random=True, dti=15.0, randomSeed=11)
     engine = Engine(0, arithmetic="fp32", storage="fp32", rng="philox")
@@ -250,10 +261,13 @@ def run_realistic(args):
                     forcing.latRad, forcing.h, forcing.depthIntervals, forcing.mask)
     engine.set_times(forcing.times)
     frame_bytes = 0
+    kept = {}
     for t in range(frames):
-        f = forcing.frame(t)
+        f = forcing.frame_device(t)
         engine.upload_frame(t, f["zeta"], f["u"], f["v"], f["w"], f["akt"])
         frame_bytes = sum(a.nbytes for a in f.values())
+        if t in (warm, warm + 1):
+            kept[t] = f  # the records of the CPU baseline's interval
     t_build = time.perf_counter() - t_build
     engine.concentration_reset(frames)
     pos = forcing.sources(n_sources, seed=3)
@@ -270,7 +284,6 @@ def run_realistic(args):
         engine.remove_dead()
         return st
 
-    warm = max(args.warmup, 3)
     for t in range(warm):
         step(t)
     ext = torch.cuda.ExternalStream(engine.stream)
@@ -281,7 +294,6 @@ def run_realistic(args):
     steps_total, launches, move_ms = 0.0, 0, []
     count = engine.count()
     start.record(ext)
-    n_steps = min(args.steps, frames - 1 - warm)
     for s in range(n_steps):
         st = step(warm + s)
         steps_total += st["particle_steps"]
@@ -292,9 +304,9 @@ def run_realistic(args):
     clocks = sampler.stop()
     elapsed_ms = start.elapsed_time(end)
     cpu = None
-    if not args.no_cpu:
+    if with_cpu:
         # the reference CPU step on a sample of the live particles over one interval
-        win2 = forcing.window(frames=[warm, warm + 1])
+        win2 = forcing.window_of([warm, warm + 1], [kept[warm], kept[warm + 1]])
         live = engine.get_particles()
         sample = live[np.random.default_rng(0).permutation(len(live))[:65536]]
         sample = np.ascontiguousarray(np.sort(sample, order="id"))
@@ -305,22 +317,30 @@ def run_realistic(args):
                "sample": f"{n} live particles x 240 substeps, one interval, Particle::move "
                          "(OpenMP dynamic,64) + Concentration::evaluate, one thread per physical "
                          "core, median of 2 after a warm-up"}
+    peak, peak_src = measured_peaks()
+    achieved = steps_total / n_steps * B_ALG / (statistics.mean(move_ms) * 1e-3) / 1e9
     line = {
         "metric": "particle-steps/s", "value": steps_total / (elapsed_ms / 1000.0),
         "unit": "particle-steps/s", "n_gpus": 1, "steps": n_steps, "warmup": warm,
         "ms_per_step": elapsed_ms / n_steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "realistic: 1024x1024x30 ROMS-shaped grid (Vtransform 2, ~20 % land), "
-                               f"24 hourly FP32 records, {n_total} particles from {n_sources} "
+                               f"{frames} hourly FP32 records (generated on the device), "
+                               f"{n_total} particles from {n_sources} "
                                "uniform-rate sources (device emission, first hour), dt=15 s, "
                                "Philox random walk, fused concentration, compaction each interval",
                    "particles_alive_at_timing": count,
                    "forcing_build_s": t_build, "record_bytes": frame_bytes},
         "move_kernel_ms": statistics.mean(move_ms),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src, "traffic": None,
+                     "kernel": "move_fast_kernel (FP32 step, random-walk form)",
+                     "kernel_ms": statistics.mean(move_ms),
+                     "algorithmic_bytes_per_particle_step": B_ALG},
         "cpu_baseline": cpu, "e2e": None, "gpu_launches": launches, "clocks": clocks,
     }
-    print(json.dumps(line), flush=True)
     engine.close()
+    return line
 
 
 def run_batched(args):
@@ -685,6 +705,8 @@ def main():
     parser.add_argument("--no-precision", action="store_true")
     parser.add_argument("--no-errors", action="store_true",
                         help="skip the 24-hour position-error runs of the surrogate arm")
+    parser.add_argument("--no-realistic", action="store_true",
+                        help="skip the realistic-grid key of the default line")
     parser.add_argument("--scenarios", type=int, default=256,
                         help="batched workload: number of scenarios")
     parser.add_argument("--workload", default="precision",
@@ -824,6 +846,16 @@ def main():
             # rank 0 alone, no collectives: the other ranks wait at the final barrier
             precision = precision_leg(args, win, particles, local_rank, truth,
                                       lambda eng, t: None, lambda: None)
+    realistic = None
+    if rank == 0 and world == 1 and not args.no_realistic:
+        # the realistic grid as a second workload of the default line (4,194,304 particles,
+        # 3 warm-up and 5 timed intervals; records generated on the device)
+        r = realistic_leg(1 << 22, 3, 5, not args.no_cpu)
+        realistic = {key: r[key] for key in ("value", "unit", "steps", "warmup", "ms_per_step",
+                                             "move_kernel_ms", "roofline", "cpu_baseline",
+                                             "gpu_launches", "clocks")}
+        realistic["workload"] = r["config"]["workload"]
+        realistic["particles_alive_at_timing"] = r["config"]["particles_alive_at_timing"]
 
     if rank == 0:
         line = {
@@ -846,6 +878,7 @@ def main():
             "roofline": roofline,
             "surrogate": surrogate,
             "precision": precision,
+            "realistic": realistic,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
