@@ -447,6 +447,7 @@ def run_batched(args):
                                "the device, Philox random walk, fused concentration, one CUDA "
                                "graph per 48-hour run",
                    "launch_shape": shape, "sort_cadence": engine.options().sort_by_cell,
+                   "particles_per_thread": engine.options().particles_per_thread,
                    "autotune_ms": tune_ms, "regrid_s": t_regrid,
                    "l2": "inputs larger than L2"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -142,6 +142,10 @@ typedef struct wacomm_b200_options {
     int surrogate;            /* 1: forward intervals by the learned surrogate
                                  (wacomm_b200_set_surrogate), with the plain stochastic operator
                                  per substep when the random walk is on; the rest by the FP32 step */
+    int particles_per_thread; /* FP32 step: work items per thread, 1..16 (default 1): the grid
+                                 shrinks by this factor and each block strides over it, taking
+                                 consecutive blocks of work items in turn; results do not depend
+                                 on it; wacomm_b200_autotune chooses 1, 2 or 4 */
 } wacomm_b200_options;
 
 /* ------------------------------------------------------------------ context */
@@ -262,9 +266,11 @@ int wacomm_b200_graph_release(wacomm_b200_context *ctx);
  * arithmetic: launch_shape 0..3; reference arithmetic: block_size 64, 128, 192, 256), each from
  * the same resident records and concentration after a warm-up pass, keeps the fastest in the
  * options and restores records and concentration: only the options change. Writes the chosen
- * value and its device ms. With the cell sort on and four intervals from time_index inside the
- * forcing window, it then times those four intervals from the same snapshot sorting every 1, 2
- * or 4 of them and keeps the fastest cadence in options.sort_by_cell. No reference
+ * value and its device ms. With FP32 arithmetic it then times the interval with 1, 2 and 4
+ * work items per thread at the chosen shape and keeps the fastest in
+ * options.particles_per_thread. With the cell sort on and four intervals from time_index inside
+ * the forcing window, it then times those four intervals from the same snapshot sorting every
+ * 1, 2 or 4 of them and keeps the fastest cadence in options.sort_by_cell. No reference
  * counterpart. */
 int wacomm_b200_autotune(wacomm_b200_context *ctx, int time_index, int *best, float *best_ms);
 

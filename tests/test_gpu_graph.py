@@ -156,6 +156,7 @@ def test_autotune_changes_only_the_launch_shape(cuda_device, setting):
     shape, ms = e.autotune(1)
     assert shape in (0, 1, 2, 3) and ms > 0
     assert e.options().launch_shape == shape
+    assert e.options().particles_per_thread in (1, 2, 4)  # chosen after the shape
     assert e.options().sort_by_cell in (1, 2, 4)  # the sort cadence chosen after the shape
     after = e.get_particles()
     for f in before.dtype.names:
@@ -234,3 +235,36 @@ def test_sort_cadence_changes_only_the_work_order(cuda_device, setting, surrogat
         for f in got.dtype.names:
             assert got[f].tobytes() == results[0][0][f].tobytes(), f
         assert np.array_equal(conc, results[0][1]) and steps == results[0][2]
+
+
+def test_particles_per_thread_changes_only_the_grid(cuda_device, setting):
+    """Several work items per thread (options.particles_per_thread) shrink the grid of the FP32
+    step and stride each block over it: every particle is moved on its own, so the records, the
+    concentration and the particle-step count equal one item per thread's, bit for bit, eager and
+    captured; values outside 1..16 are refused."""
+    win, env, cfg = setting
+    parts = batch(30001, 12, win)   # not a multiple of any block
+    results = []
+    for per in (1, 2, 4, 16):
+        e = engine(win, env, cfg, parts)
+        e.set_options(particles_per_thread=per)
+        steps = eager(e)
+        results.append((e.get_particles(), e.concentration(), steps))
+        e.close()
+    for got, conc, steps in results[1:]:
+        for f in got.dtype.names:
+            assert got[f].tobytes() == results[0][0][f].tobytes(), f
+        assert np.array_equal(conc, results[0][1]) and steps == results[0][2]
+    g = engine(win, env, cfg, parts)
+    g.set_options(particles_per_thread=4)
+    g.graph_capture(0, INTERVALS)
+    g.graph_launch()
+    g.synchronize()
+    assert g.stats()["particle_steps"] == results[0][2]
+    pg = g.get_particles()
+    for f in pg.dtype.names:
+        assert pg[f].tobytes() == results[0][0][f].tobytes(), f
+    for bad in (0, 17):
+        with pytest.raises(WacommError):
+            g.set_options(particles_per_thread=bad)
+    g.close()

@@ -35,7 +35,7 @@ class options_t(ctypes.Structure):
         ("rng", ctypes.c_int), ("block_size", ctypes.c_int),
         ("substeps_per_launch", ctypes.c_int), ("sort_by_cell", ctypes.c_int),
         ("fuse_concentration", ctypes.c_int), ("launch_shape", ctypes.c_int),
-        ("surrogate", ctypes.c_int),
+        ("surrogate", ctypes.c_int), ("particles_per_thread", ctypes.c_int),
     ]
 
 

@@ -358,6 +358,9 @@ int validate_options(wacomm_b200_context *ctx, const wacomm_b200_options &o) {
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "substeps_per_launch must be >= 0");
     if (o.launch_shape < WACOMM_B200_LAUNCH_SHAPE_AUTO || o.launch_shape > 3)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "launch_shape %d out of [-1, 3]", o.launch_shape);
+    if (o.particles_per_thread < 1 || o.particles_per_thread > 16)
+        return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "particles_per_thread %d out of [1, 16]",
+                    o.particles_per_thread);
     if (o.surrogate != 0 && o.surrogate != 1)
         return fail(ctx, WACOMM_B200_ERR_ARGUMENT, "surrogate %d: 0 or 1", o.surrogate);
     if (o.surrogate && o.arithmetic != WACOMM_B200_ARITH_FP32)
@@ -561,6 +564,7 @@ int run_interval(wacomm_b200_context *ctx, const IntervalParams &base, size_t of
     MoveLaunch L;
     L.count = (int)count;
     L.order = nullptr;
+    L.perThread = ctx->opt.particles_per_thread;
     int concTime = base.t0 + base.direction;
     bool count_here = ctx->opt.fuse_concentration && ctx->dConc && concTime >= 0 &&
                       concTime < ctx->concTimes;
@@ -860,6 +864,7 @@ int wacomm_b200_default_options(wacomm_b200_options *out) {
     out->fuse_concentration = 1;
     out->launch_shape = WACOMM_B200_LAUNCH_SHAPE_AUTO;
     out->surrogate = 0;
+    out->particles_per_thread = 1;
     return WACOMM_B200_OK;
 }
 
@@ -2347,6 +2352,34 @@ int wacomm_b200_autotune(wacomm_b200_context *ctx, int time_index, int *best, fl
     if (!rc) {
         if (fp32) ctx->opt.launch_shape = chosen;
         else ctx->opt.block_size = chosen;
+    }
+    // Work items per thread of the FP32 step, with the chosen shape: one interval each from the
+    // snapshot, the fastest kept in options.particles_per_thread.
+    if (!rc && fp32) {
+        int per = saved.particles_per_thread;
+        float bestPer = INFINITY;
+        for (int pass = 0; pass < 2 && !rc; pass++)
+            for (int c : {1, 2, 4}) {
+                ctx->opt.particles_per_thread = c;
+                cudaError_t e = restore();
+                if (e != cudaSuccess) {
+                    rc = fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e));
+                    break;
+                }
+                if ((rc = wacomm_b200_move_interval(ctx, time_index))) break;
+                float ms = 0;
+                e = cudaEventSynchronize(ctx->ev1);
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+                if (e != cudaSuccess) {
+                    rc = fail(ctx, WACOMM_B200_ERR_CUDA, "%s", cudaGetErrorString(e));
+                    break;
+                }
+                if (pass == 1 && ms < bestPer) {
+                    bestPer = ms;
+                    per = c;
+                }
+            }
+        ctx->opt.particles_per_thread = per;
     }
     // The sort cadence, with the chosen shape: four intervals from the snapshot sorting every
     // 1, 2 or 4 of them; the fastest run sets options.sort_by_cell (when sorting is on and the

@@ -25,6 +25,9 @@ struct MoveLaunch {
     // When set, the work items are the first min(count, *countDevice): a list whose length a
     // kernel earlier on the stream wrote (the launch covers `count`, blocks past the list exit).
     const uint32_t *countDevice = nullptr;
+    // FP32 step: work items per thread; the grid is that many times smaller and each block
+    // strides over it (results do not depend on it).
+    int perThread = 1;
 };
 
 // Work items of a launch: count, or the device-side length of its list.
@@ -125,36 +128,39 @@ __global__ void __launch_bounds__(LaunchShape<SHAPE>::threads, LaunchShape<SHAPE
                                                         const FastView<STORE> F, ParticleSoA S,
                                                         const MoveLaunch L) {
     const int count = launch_count(L);
-    if ((int)(blockIdx.x * blockDim.x) >= count) return;  // whole blocks past a device-side list
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    long long cell = -1;
-    int steps = 0;
-    if (t < count) {
-        uint32_t slot = L.order ? L.order[t] : (uint32_t)t;
-        ParticleState p;
-        p.id = S.id[slot];
-        p.k = S.k[slot];
-        p.j = S.j[slot];
-        p.i = S.i[slot];
-        p.health = S.health[slot];
-        p.age = S.age[slot];
-        p.time = S.time[slot];
-        p.type = S.type[slot];
-        p.side = S.side[slot];
-        double elapsed = P.firstChunk ? P.elapsed0 : S.elapsed[slot];
-        steps = move_particle_fast<SEM, STORE, VARIANT>(cfg, P, F, p, elapsed, L.err);
-        S.k[slot] = p.k;
-        S.j[slot] = p.j;
-        S.i[slot] = p.i;
-        S.health[slot] = p.health;
-        S.age[slot] = p.age;
-        S.side[slot] = (int8_t)p.side;
-        if (!P.lastChunk) S.elapsed[slot] = elapsed;
-        if (L.conc && P.lastChunk)
-            cell = concentration_cell(p, L.concTimeIndex, F.V.g.sRho, F.V.g.eta, F.V.g.xi);
+    // block-uniform stride loop (blocks past a device-side list take no turn)
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < count;
+         base += (long long)gridDim.x * blockDim.x) {
+        const int t = (int)base + threadIdx.x;
+        long long cell = -1;
+        int steps = 0;
+        if (t < count) {
+            uint32_t slot = L.order ? L.order[t] : (uint32_t)t;
+            ParticleState p;
+            p.id = S.id[slot];
+            p.k = S.k[slot];
+            p.j = S.j[slot];
+            p.i = S.i[slot];
+            p.health = S.health[slot];
+            p.age = S.age[slot];
+            p.time = S.time[slot];
+            p.type = S.type[slot];
+            p.side = S.side[slot];
+            double elapsed = P.firstChunk ? P.elapsed0 : S.elapsed[slot];
+            steps = move_particle_fast<SEM, STORE, VARIANT>(cfg, P, F, p, elapsed, L.err);
+            S.k[slot] = p.k;
+            S.j[slot] = p.j;
+            S.i[slot] = p.i;
+            S.health[slot] = p.health;
+            S.age[slot] = p.age;
+            S.side[slot] = (int8_t)p.side;
+            if (!P.lastChunk) S.elapsed[slot] = elapsed;
+            if (L.conc && P.lastChunk)
+                cell = concentration_cell(p, L.concTimeIndex, F.V.g.sRho, F.V.g.eta, F.V.g.xi);
+        }
+        if (L.steps) warp_sum_steps(L.steps, steps);
+        if (L.conc && P.lastChunk) warp_count(L.conc, cell);
     }
-    if (L.steps) warp_sum_steps(L.steps, steps);
-    if (L.conc && P.lastChunk) warp_count(L.conc, cell);
 }
 
 template <int SEM, int STORE, int SHAPE, int VARIANT>
@@ -163,7 +169,8 @@ cudaError_t launch_move_fast(const wacomm_b200_config &cfg, const IntervalParams
                              cudaStream_t stream) {
     if (L.count <= 0) return cudaSuccess;
     constexpr int threads = LaunchShape<SHAPE>::threads;
-    int blocks = (L.count + threads - 1) / threads;
+    const int per = L.perThread > 1 ? L.perThread : 1;
+    int blocks = (L.count + threads * per - 1) / (threads * per);
     move_fast_kernel<SEM, STORE, SHAPE, VARIANT><<<blocks, threads, 0, stream>>>(cfg, P, F, S, L);
     return cudaGetLastError();
 }

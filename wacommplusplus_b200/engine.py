@@ -230,7 +230,8 @@ class Engine:
 
     def autotune(self, time_index):
         """Times each launch configuration on interval time_index and keeps the fastest;
-        returns (chosen launch_shape or block_size, its device ms)."""
+        returns (chosen launch_shape or block_size, its device ms). The FP32 step's work items
+        per thread and the sort cadence it chooses next are in options()."""
         best, ms = ctypes.c_int(), ctypes.c_float()
         self._check(self._lib.wacomm_b200_autotune(self._ctx, time_index, ctypes.byref(best),
                                                    ctypes.byref(ms)))
