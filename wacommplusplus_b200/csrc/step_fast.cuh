@@ -35,10 +35,15 @@ struct Weights8 {
     float p1, p2, p3, p4, q1, q2, q3, q4;
 };
 
+// The products run in pairs on the packed FP32x2 multiply of sm_100 (the same roundings).
 __device__ __forceinline__ Weights8 weights8(float jF, float iF, float a) {
-    float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
-    float b = 1.f - a;
-    return Weights8{b * w1, b * w2, b * w3, b * w4, a * w1, a * w2, a * w3, a * w4};
+    const float oi = 1.f - iF, oj = 1.f - jF, b = 1.f - a;
+    const float2 w12 = __fmul2_rn(make_float2(oi, oi), make_float2(oj, jF));
+    const float2 w34 = __fmul2_rn(make_float2(iF, iF), make_float2(jF, oj));
+    const float2 bb = make_float2(b, b), aa = make_float2(a, a);
+    const float2 p12 = __fmul2_rn(bb, w12), p34 = __fmul2_rn(bb, w34);
+    const float2 q12 = __fmul2_rn(aa, w12), q34 = __fmul2_rn(aa, w34);
+    return Weights8{p12.x, p12.y, p34.x, p34.y, q12.x, q12.y, q34.x, q34.y};
 }
 
 // Two independent FMA chains (record t0, record t1) keep the dependency depth at four.
@@ -90,9 +95,13 @@ struct StencilAt {
     Quad u, v, wUp, wLo;
 };
 
+// t0 + a (t1 - t0) per corner, two corners per packed FP32x2 add and multiply-add.
 __device__ __forceinline__ Quad at_time(const QuadPair &q, float a) {
-    return Quad{fmaf(a, q.t1.c1 - q.t0.c1, q.t0.c1), fmaf(a, q.t1.c2 - q.t0.c2, q.t0.c2),
-                fmaf(a, q.t1.c3 - q.t0.c3, q.t0.c3), fmaf(a, q.t1.c4 - q.t0.c4, q.t0.c4)};
+    const float2 a2 = make_float2(a, a);
+    const float2 lo0 = make_float2(q.t0.c1, q.t0.c2), hi0 = make_float2(q.t0.c3, q.t0.c4);
+    const float2 lo = __ffma2_rn(a2, __fadd2_rn(make_float2(q.t1.c1, q.t1.c2), make_float2(-lo0.x, -lo0.y)), lo0);
+    const float2 hi = __ffma2_rn(a2, __fadd2_rn(make_float2(q.t1.c3, q.t1.c4), make_float2(-hi0.x, -hi0.y)), hi0);
+    return Quad{lo.x, lo.y, hi.x, hi.y};
 }
 
 __device__ __forceinline__ float bilinear4(const Quad &q, float w1, float w2, float w3, float w4) {
