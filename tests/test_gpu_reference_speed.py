@@ -101,10 +101,11 @@ def test_reference_kernel_against_this_library(cuda_device):
         assert _native.lib().wacomm_b200_cuda_move_particle_noalloc(
             d_cfg.data_ptr(), ours.data_ptr(), INTERVAL, *head, *ptrs, N, 1, 1, stream) == 0
 
-    copy_ms = _timed(lambda: theirs.copy_(start))
-    ref_ms = _timed(reference) - copy_ms
-    noalloc_ms = _timed(noalloc) - copy_ms
-    dropin_ms = _timed(dropin) - copy_ms
+    # three interleaved rounds, the fastest of each: another tenant of a shared GPU slows single
+    # rounds, not all of them
+    copy_ms = min(_timed(lambda: theirs.copy_(start)) for _ in range(3))
+    rounds = [(_timed(reference), _timed(noalloc), _timed(dropin)) for _ in range(3)]
+    ref_ms, noalloc_ms, dropin_ms = (min(r[c] for r in rounds) - copy_ms for c in range(3))
     got = ours.cpu().numpy().view(parts.dtype)
     want = theirs.cpu().numpy().view(parts.dtype)
     assert np.array_equal(got["health"] > 0, want["health"] > 0)

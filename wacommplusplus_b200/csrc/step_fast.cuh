@@ -46,16 +46,15 @@ __device__ __forceinline__ Weights8 weights8(float jF, float iF, float a) {
     return Weights8{p12.x, p12.y, p34.x, p34.y, q12.x, q12.y, q34.x, q34.y};
 }
 
-// Two independent FMA chains (record t0, record t1) keep the dependency depth at four.
+// The 8 products summed as pairs of corners (c1, c2 | c3, c4) with the packed FP32x2 multiply
+// and multiply-add of sm_100, record t0 and record t1 apart, then the four partial sums.
 __device__ __forceinline__ float blend(const QuadPair &q, const Weights8 &w) {
-    float x = q.t0.c1 * w.p1, y = q.t1.c1 * w.q1;
-    x = fmaf(q.t0.c2, w.p2, x);
-    y = fmaf(q.t1.c2, w.q2, y);
-    x = fmaf(q.t0.c3, w.p3, x);
-    y = fmaf(q.t1.c3, w.q3, y);
-    x = fmaf(q.t0.c4, w.p4, x);
-    y = fmaf(q.t1.c4, w.q4, y);
-    return x + y;
+    float2 x = __fmul2_rn(make_float2(q.t0.c1, q.t0.c2), make_float2(w.p1, w.p2));
+    float2 y = __fmul2_rn(make_float2(q.t1.c1, q.t1.c2), make_float2(w.q1, w.q2));
+    x = __ffma2_rn(make_float2(q.t0.c3, q.t0.c4), make_float2(w.p3, w.p4), x);
+    y = __ffma2_rn(make_float2(q.t1.c3, q.t1.c4), make_float2(w.q3, w.q4), y);
+    const float2 t = __fadd2_rn(x, y);
+    return t.x + t.y;
 }
 
 // Bilinear h + zeta@t0 and zeta@t1 - zeta@t0 at a fractional position of a cell (FP32); the water
@@ -65,16 +64,21 @@ struct SurfaceSums {
     __device__ __forceinline__ float height(float a) const { return fmaf(a, d, s); }
 };
 
+// Corner weights in pairs {w1, w2}, {w3, w4} (packed FP32x2 multiplies).
+__device__ __forceinline__ void corner_pairs(float jF, float iF, float2 &w12, float2 &w34) {
+    const float oi = 1.f - iF, oj = 1.f - jF;
+    w12 = __fmul2_rn(make_float2(oi, oi), make_float2(oj, jF));
+    w34 = __fmul2_rn(make_float2(iF, iF), make_float2(jF, oj));
+}
+
 __device__ __forceinline__ SurfaceSums surface_from(const CellSurface &c, float jF, float iF) {
-    float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF, w4 = iF * (1.f - jF);
-    float s = c.s0.x * w1, d = c.dz.x * w1;
-    s = fmaf(c.s0.y, w2, s);
-    d = fmaf(c.dz.y, w2, d);
-    s = fmaf(c.s0.z, w3, s);
-    d = fmaf(c.dz.z, w3, d);
-    s = fmaf(c.s0.w, w4, s);
-    d = fmaf(c.dz.w, w4, d);
-    return SurfaceSums{s, d};
+    float2 w12, w34;
+    corner_pairs(jF, iF, w12, w34);
+    float2 s = __fmul2_rn(make_float2(c.s0.x, c.s0.y), w12);
+    float2 d = __fmul2_rn(make_float2(c.dz.x, c.dz.y), w12);
+    s = __ffma2_rn(make_float2(c.s0.z, c.s0.w), w34, s);
+    d = __ffma2_rn(make_float2(c.dz.z, c.dz.w), w34, d);
+    return SurfaceSums{s.x + s.y, d.x + d.y};
 }
 
 template <int STORE>
@@ -104,8 +108,9 @@ __device__ __forceinline__ Quad at_time(const QuadPair &q, float a) {
     return Quad{lo.x, lo.y, hi.x, hi.y};
 }
 
-__device__ __forceinline__ float bilinear4(const Quad &q, float w1, float w2, float w3, float w4) {
-    return fmaf(q.c4, w4, fmaf(q.c3, w3, fmaf(q.c2, w2, q.c1 * w1)));
+__device__ __forceinline__ float bilinear4(const Quad &q, float2 w12, float2 w34) {
+    const float2 x = __ffma2_rn(make_float2(q.c3, q.c4), w34, __fmul2_rn(make_float2(q.c1, q.c2), w12));
+    return x.x + x.y;
 }
 
 // Current (u, v, w) and, when wanted, AKT at a fractional position: one stencil read. With `keep`
@@ -141,11 +146,11 @@ __device__ __forceinline__ void current_cell(const CellView<STORE> &C, int kI, f
 // Current (u, v, w) from a kept stencil at a fractional position of its cell and level.
 __device__ __forceinline__ void current_kept(const StencilAt &k, float kF, float jF, float iF,
                                              float &uu, float &vv, float &ww) {
-    const float w1 = (1.f - iF) * (1.f - jF), w2 = (1.f - iF) * jF, w3 = iF * jF,
-                w4 = iF * (1.f - jF);
-    uu = bilinear4(k.u, w1, w2, w3, w4);
-    vv = bilinear4(k.v, w1, w2, w3, w4);
-    const float up = bilinear4(k.wUp, w1, w2, w3, w4), lo = bilinear4(k.wLo, w1, w2, w3, w4);
+    float2 w12, w34;
+    corner_pairs(jF, iF, w12, w34);
+    uu = bilinear4(k.u, w12, w34);
+    vv = bilinear4(k.v, w12, w34);
+    const float up = bilinear4(k.wUp, w12, w34), lo = bilinear4(k.wLo, w12, w34);
     ww = fmaf(lo - up, kF, up);
 }
 
