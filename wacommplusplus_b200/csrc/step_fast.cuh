@@ -370,8 +370,11 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 n1 = (float)prefix_normal(stepKey, 1);
                 n2 = (float)prefix_normal(stepKey, 2);
             }
-            rx = sigmaDepth * n0 * scale;
-            ry = sigmaDepth * n1 * scale;
+            const float2 rxy = __fmul2_rn(
+                __fmul2_rn(make_float2(sigmaDepth, sigmaDepth), make_float2(n0, n1)),
+                make_float2(scale, scale));
+            rx = rxy.x;
+            ry = rxy.y;
             rz = sigmaDepth * n2 * aa * (float)cfg.crid * scale;
         }
         const float2 inv = __ldg(F.X.invMetric + (size_t)jI * xi + iI);
@@ -383,8 +386,13 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
         if (midpoint) {
             float kHalf = dirf * (sv + ww) * 0.5f * dt;
             if (fabsf(kHalf) > zdist) kHalf = signf_of(zdist, kHalf);
-            double iMid = p.i + (double)(dirf * uu * 0.5f * dt * inv.x);
-            double jMid = p.j + (double)(dirf * vv * 0.5f * dt * inv.y);
+            // (dirf u 0.5 dt) / dx for i and j as one packed FP32x2 chain (the same roundings)
+            const float2 half = __fmul2_rn(
+                __fmul2_rn(__fmul2_rn(make_float2(dirf * uu, dirf * vv), make_float2(0.5f, 0.5f)),
+                           make_float2(dt, dt)),
+                inv);
+            double iMid = p.i + (double)half.x;
+            double jMid = p.j + (double)half.y;
             double kMid = fmin(0.0, fmax(kLower, p.k + (double)(kHalf * rzdist)));
             double fim = floor(iMid), fjm = floor(jMid);
             int iMI = to_index<SEM>(fim), jMI = to_index<SEM>(fjm);
@@ -418,8 +426,10 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 const float2 im = sameCell ? inv : __ldg(F.X.invMetric + (size_t)jMI * xi + iMI);
                 float zdistMid =
                     hcMid * (kMI == kM ? depthHere : __ldg(F.X.depthIntervals + (kMI + sW - 2)));
-                dI = dirf * um * dt * im.x;
-                dJ = dirf * vm * dt * im.y;
+                const float2 d = __fmul2_rn(
+                    __fmul2_rn(make_float2(dirf * um, dirf * vm), make_float2(dt, dt)), im);
+                dI = d.x;
+                dJ = d.y;
                 detZ = dirf * (sv + wm) * dt * zdist * __frcp_rn(zdistMid);
             } else {
                 float ue, ve, we, unused;
@@ -432,8 +442,10 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                     ue += du;
                     ve += dv;
                 }
-                dI = dirf * ue * dt * inv.x;
-                dJ = dirf * ve * dt * inv.y;
+                const float2 d = __fmul2_rn(
+                    __fmul2_rn(make_float2(dirf * ue, dirf * ve), make_float2(dt, dt)), inv);
+                dI = d.x;
+                dJ = d.y;
                 detZ = dirf * (sv + we) * dt;
             }
             dI += rx * inv.x;

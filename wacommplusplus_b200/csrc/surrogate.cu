@@ -1048,14 +1048,18 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
         const float kNow = (float)kI - kF;
         const float sigmaDepth = sigma * (1.f - kNow * invKLower);
         const float scale = stepDt == cfg.dti ? 1.f : sqrtf(dt / dtiF);
-        const float rx = sigmaDepth * n0 * scale, ry = sigmaDepth * n1 * scale;
+        // the two horizontal components in pairs (packed FP32x2, the same roundings)
+        const float2 rxy = __fmul2_rn(__fmul2_rn(make_float2(sigmaDepth, sigmaDepth), make_float2(n0, n1)),
+                                      make_float2(scale, scale));
         const float rz = sigmaDepth * n2 * aa * crid * scale;
         const float zdist = hc * depth;
         const float rzdist = __frcp_rn(zdist);
-        const float dI = fmaf(rateX, dt, rx) * inv.x, dJ = fmaf(rateY, dt, ry) * inv.y;
+        const float2 dIJ = __fmul2_rn(__ffma2_rn(make_float2(rateX, rateY), make_float2(dt, dt), rxy), inv);
+        const float dI = dIJ.x, dJ = dIJ.y;
         float zleap = fmaf(rateZ, dt, rz);
         if (fabsf(zleap) > zdist) zleap = signf_of(zdist, zleap);
-        const float jN = jF + dJ, iN = iF + dI, kN = fmaf(-zleap, rzdist, kF);
+        const float2 ijN = __fadd2_rn(make_float2(iF, jF), dIJ);
+        const float iN = ijN.x, jN = ijN.y, kN = fmaf(-zleap, rzdist, kF);
         // the destination: at most one cell or level away on this path (comparisons, no
         // float-to-int conversions), and its surface (this cell's, read again, in the common case)
         const int dj = (jN >= 1.f) - (jN < 0.f), di = (iN >= 1.f) - (iN < 0.f);
