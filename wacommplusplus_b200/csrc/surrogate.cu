@@ -988,6 +988,13 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
     bool lazy = false;
     int steps = 0;
     double elapsed = p.time > P.start ? fmin(length, p.time - P.start) : 0.0;  // activation
+    // Substeps left in which the lazy survival tests cannot change their outcome: while
+    // age < min(ageKillLo, ageUnder) a lazily tracked particle is neither dead (age stays below
+    // ageKillLo <= ageKillHi) nor without health (age below ageUnder). Counted when the
+    // particle turns lazy, two substeps short of the bound for rounding; while it lasts and no
+    // closure has ended the lazy tracking, both tests are skipped.
+    const double ageSafe = fmin(P.ageKillLo, P.ageUnder), invDti = 1.0 / cfg.dti;
+    int youngLeft = 0;
 
     const double fj = floor(p.j), fi = floor(p.i), ck = ceil(p.k);
     int jI = to_index<SEM>(fj), iI = to_index<SEM>(fi), kI = to_index<SEM>(ck);
@@ -1000,13 +1007,15 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
     bool carried = false;
     while (elapsed < length) {
         const double stepDt = fmin(cfg.dti, length - elapsed);
-        const bool dead = lazy ? (p.age >= P.ageKillHi ||
-                                  (p.age > P.ageKillLo && exp(-p.age / cfg.tau0) < cfg.survprob))
-                               : p.health < cfg.survprob;
-        if (dead) {
-            p.health = -1;
-            lazy = false;
-            break;
+        if (!(lazy && youngLeft > 0)) {
+            const bool dead = lazy ? (p.age >= P.ageKillHi ||
+                                      (p.age > P.ageKillLo && exp(-p.age / cfg.tau0) < cfg.survprob))
+                                   : p.health < cfg.survprob;
+            if (dead) {
+                p.health = -1;
+                lazy = false;
+                break;
+            }
         }
         if (!carried &&
             (!valid_cell(jI, iI, eta, xi) || (SEM == SEM_DEVICE && (kI > 0 || kI <= -sW + 1)))) {
@@ -1167,10 +1176,19 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
             iLo = (nI - gi) - (double)iF;
             kLo = (gk - nK) - (double)kF;
         }
-        const bool alive = lazy ? (p.age < P.ageUnder || exp(-p.age / cfg.tau0) > 0) : p.health > 0;
-        if (alive) {
+        if (lazy && youngLeft > 0) {  // still lazy: no closure ended the tracking this substep
             p.age = p.age + stepDt;
-            lazy = true;
+            youngLeft--;
+        } else {
+            const bool alive = lazy ? (p.age < P.ageUnder || exp(-p.age / cfg.tau0) > 0) : p.health > 0;
+            if (alive) {
+                if (!lazy) {
+                    const double n = floor((ageSafe - p.age) * invDti) - 2.0;
+                    youngLeft = n > 0.0 ? (n < 1.0e9 ? (int)n : 1000000000) : 0;
+                }
+                p.age = p.age + stepDt;
+                lazy = true;
+            }
         }
         elapsed += stepDt;
     }
