@@ -265,6 +265,12 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
     if (drift && SEM == SEM_HOST && (p.type < 0 || p.type > 22)) atomicOr(err, ERR_DRIFT_OBJECT);
     bool lazy = false;
     int steps = 0;
+    // Substeps left in which the lazy survival tests cannot change their outcome (age below
+    // min(ageKillLo, ageUnder): neither dead nor without health), counted when the particle turns
+    // lazy, two substeps short of the bound for rounding; skipped while it lasts and no closure
+    // has ended the lazy tracking.
+    const double ageSafe = fmin(P.ageKillLo, P.ageUnder);
+    int youngLeft = 0;
 
     if (P.firstChunk) {
         if (p.k > 0) close_upper(cfg, p.k, p.health, lazy);
@@ -288,14 +294,16 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
             elapsed = fmin(length, p.time - P.start);
             continue;
         }
-        bool dead = lazy ? (p.age >= P.ageKillHi ||
-                            (p.age > P.ageKillLo && exp(-p.age / cfg.tau0) < cfg.survprob))
-                         : p.health < cfg.survprob;
-        if (dead) {
-            p.health = -1;
-            lazy = false;
-            elapsed = length;
-            break;
+        if (!(lazy && youngLeft > 0)) {
+            bool dead = lazy ? (p.age >= P.ageKillHi ||
+                                (p.age > P.ageKillLo && exp(-p.age / cfg.tau0) < cfg.survprob))
+                             : p.health < cfg.survprob;
+            if (dead) {
+                p.health = -1;
+                lazy = false;
+                elapsed = length;
+                break;
+            }
         }
         const double kc = ceil(p.k);
         const int kI = to_index<SEM>(kc);
@@ -503,7 +511,18 @@ __device__ int move_particle_fast(const wacomm_b200_config &cfg, const IntervalP
                 p.k = kdet;
             }
         }
-        bool alive = lazy ? (p.age < P.ageUnder || exp(-p.age / cfg.tau0) > 0) : p.health > 0;
+        bool alive;
+        if (lazy && youngLeft > 0) {  // still lazy: no closure ended the tracking this substep
+            alive = true;
+            youngLeft--;
+        } else {
+            alive = lazy ? (p.age < P.ageUnder || exp(-p.age / cfg.tau0) > 0) : p.health > 0;
+            if (alive && !lazy) {
+                // FP32 and an approximate division: the two-substep margin covers their error
+                const float n = floorf(__fdividef((float)(ageSafe - p.age), (float)cfg.dti)) - 2.f;
+                youngLeft = n > 0.f ? (n < 1.0e9f ? (int)n : 1000000000) : 0;
+            }
+        }
         if (alive) {
             p.age = p.age + stepDt;
             lazy = true;

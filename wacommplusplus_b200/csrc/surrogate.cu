@@ -993,7 +993,7 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
     // ageKillLo <= ageKillHi) nor without health (age below ageUnder). Counted when the
     // particle turns lazy, two substeps short of the bound for rounding; while it lasts and no
     // closure has ended the lazy tracking, both tests are skipped.
-    const double ageSafe = fmin(P.ageKillLo, P.ageUnder), invDti = 1.0 / cfg.dti;
+    const double ageSafe = fmin(P.ageKillLo, P.ageUnder);
     int youngLeft = 0;
 
     const double fj = floor(p.j), fi = floor(p.i), ck = ceil(p.k);
@@ -1183,8 +1183,9 @@ __device__ int walk_particle(const wacomm_b200_config &cfg, const IntervalParams
             const bool alive = lazy ? (p.age < P.ageUnder || exp(-p.age / cfg.tau0) > 0) : p.health > 0;
             if (alive) {
                 if (!lazy) {
-                    const double n = floor((ageSafe - p.age) * invDti) - 2.0;
-                    youngLeft = n > 0.0 ? (n < 1.0e9 ? (int)n : 1000000000) : 0;
+                    // FP32 and an approximate division: the two-substep margin covers their error
+                    const float n = floorf(__fdividef((float)(ageSafe - p.age), (float)cfg.dti)) - 2.f;
+                    youngLeft = n > 0.f ? (n < 1.0e9f ? (int)n : 1000000000) : 0;
                 }
                 p.age = p.age + stepDt;
                 lazy = true;
