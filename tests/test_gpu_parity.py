@@ -324,3 +324,40 @@ def test_unknown_drift_object_is_an_error_under_host_rules(cuda_device):
         e.move_interval(0)
         with pytest.raises(RuntimeError, match="catalogue"):
             e.synchronize()
+
+
+@pytest.mark.parametrize("form", ["fp32", "fp32_random_walk", "walk"])
+def test_survival_threshold_crossed_inside_the_interval(cuda_device, form):
+    """Particles whose age crosses the survival threshold (exp(-age/tau0) = survprob) at every
+    substep of the interval: each dies at the substep the oracle's survival test kills it, so
+    alive/dead status, age (which stops at death) and health agree. The FP32 step and the walk
+    kernel skip the lazy survival tests while the outcome cannot change; this holds them to the
+    oracle where it does."""
+    win = syn.config1_window(n_frames=2)
+    cfg = default_config(random=form != "fp32", randomSeed=7, tau0=86400.0, survprob=1e-4)
+    kill = -86400.0 * np.log(1e-4)
+    n = 8192
+    p = syn.uniform_particles(n, win.eta, win.xi, time=win.times[0], seed=31)
+    rng = np.random.default_rng(32)
+    p["age"] = kill - rng.uniform(-60.0, 3900.0, n)   # dies before, during or after the hour
+    p["age"][:64] = rng.uniform(0.0, 1000.0, 64)      # young ones too
+    p["health"] = np.exp(-p["age"] / 86400.0)
+    if form == "walk":
+        e = Engine(0, arithmetic="fp32", storage="fp32", surrogate=1)
+        e.set_config(cfg)
+        e.load_window(win)
+        e.set_surrogate()
+    else:
+        e = Engine(0, arithmetic="fp32", storage="fp32")
+        e.set_config(cfg)
+        e.load_window(win)
+    e.set_particles(p)
+    e.move_interval(0)
+    got = e.get_particles()
+    e.close()
+    want = ob.oracle_move(cfg, p.copy(), win, 0, ob.SEMANTICS_HOST, threads=0)
+    alive = want["health"] > 0
+    assert 0.2 < alive.mean() < 0.9
+    assert np.array_equal(got["health"] > 0, alive)
+    assert np.allclose(got["age"], want["age"], rtol=0, atol=1e-9)
+    assert np.allclose(got["health"][alive], want["health"][alive], rtol=1e-12, atol=0)
